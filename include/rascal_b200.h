@@ -1,0 +1,232 @@
+/*
+ * rascal_b200.h -- C ABI of the B200 descriptor/GAP library.
+ *
+ * One shared library (librascal_b200/_lib/librascal_b200.so) holds the
+ * sm_100a CUDA kernels and the C++ host code that drives them. The entry
+ * points below are the drop-in boundary for librascal's SOAP + sparse-GAP
+ * hot path: each one names the reference interface it replaces (paths are
+ * relative to the librascal source tree). Arguments are plain pointers and
+ * sizes; every array argument is a HOST pointer unless its name ends in
+ * `_dev`.
+ *
+ * Every function returns an rgpu_status (0 = success). On failure the message
+ * of the matching reference exception is available from
+ * rgpu_last_error() (thread-local), and rgpu_error_kind() tells which C++
+ * exception type the reference throws for it (see rgpu_error_kind_t), so a
+ * binding can re-raise the same Python exception class.
+ *
+ * Threading: a handle is used by one host thread at a time; each structure
+ * set owns one CUDA stream. This matches the reference, which is serial and
+ * releases the GIL around compute
+ * (bindings/bind_py_representation_calculator.cc:57-62).
+ */
+#ifndef RASCAL_B200_H_
+#define RASCAL_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int rgpu_status;
+enum {
+  RGPU_OK = 0,
+  RGPU_ERR_INVALID_ARGUMENT = 1, /* bad hypers / sizes: std::logic_error, runtime_error */
+  RGPU_ERR_STRUCTURE = 2,        /* atom outside cell, zero cell, type range: runtime_error */
+  RGPU_ERR_CAPACITY = 3,         /* device buffer too small (retried internally) */
+  RGPU_ERR_TIMEOUT = 4,          /* a bounded device-side wait gave up */
+  RGPU_ERR_CUDA = 5,             /* CUDA runtime error */
+  RGPU_ERR_OVERFLOW = 6,         /* 1F1 overflow: std::overflow_error */
+  RGPU_ERR_NOT_COMPUTED = 7      /* features requested before compute */
+};
+
+/* Which reference exception a status maps to. */
+typedef enum {
+  RGPU_EXC_NONE = 0,
+  RGPU_EXC_RUNTIME_ERROR = 1,
+  RGPU_EXC_LOGIC_ERROR = 2,
+  RGPU_EXC_OVERFLOW_ERROR = 3
+} rgpu_error_kind_t;
+
+const char * rgpu_last_error(void);
+int rgpu_error_kind(void);
+int rgpu_version(void);
+
+/* Opaque handles. */
+typedef struct rgpu_calculator rgpu_calculator;
+typedef struct rgpu_structures rgpu_structures;
+typedef struct rgpu_gap_model rgpu_gap_model;
+
+/* Arithmetic of a compute call. */
+enum {
+  RGPU_PRECISION_FP64 = 0, /* plain path: FP64 everywhere, reference data flow */
+  RGPU_PRECISION_FP32 = 1  /* fast path: FP32 expansion, TF32 tensor-core GEMMs */
+};
+
+/* ---------------------------------------------------------------------- */
+/* Calculators.
+ * Replaces CalculatorSphericalInvariants(hypers) / CalculatorSphericalExpansion
+ * (hypers) constructed from JSON:
+ *   bindings/bind_py_representation_calculator.cc:43-47 (py::init from dict)
+ *   src/rascal/representations/calculator_spherical_invariants.hh:171-176,257-292
+ *   src/rascal/representations/calculator_spherical_expansion.hh:1596-1742
+ * `kind` is "sphericalinvariants" or "sphericalexpansion"; `hypers_json` is the
+ * hypers dict the reference's Python wrapper builds
+ * (bindings/rascal/representations/spherical_invariants.py:209-294). The GTO
+ * radial spline is built here in FP64 on the host and uploaded. */
+rgpu_status rgpu_calculator_create(const char * kind, const char * hypers_json,
+                                   rgpu_calculator ** out);
+rgpu_status rgpu_calculator_destroy(rgpu_calculator * calc);
+/* Name used by the reference to register results: prefix + hypers dump
+ * (src/rascal/representations/calculator_base.hh:105-112). */
+rgpu_status rgpu_calculator_name(const rgpu_calculator * calc, char * buf,
+                                 size_t buflen);
+/* Shape of the radial spline (grid points, values per point). */
+rgpu_status rgpu_calculator_spline_shape(const rgpu_calculator * calc,
+                                         int32_t * grid_size, int32_t * width);
+/* Copy out the FP64 spline (grid, values y, y''h^2/6), each grid_size x width,
+ * for parity checks of the host spline builder
+ * (src/rascal/math/interpolator.hh:976-1287). */
+rgpu_status rgpu_calculator_spline_table(const rgpu_calculator * calc,
+                                         double * grid, double * y,
+                                         double * y2h);
+
+/* ---------------------------------------------------------------------- */
+/* Structure sets.
+ * Replaces ManagerCollection(adaptors) + add_structures(AtomicStructureList)
+ * (src/rascal/structure_managers/structure_manager_collection.hh:178-184,
+ *  bindings/bind_py_structure_manager.cc:472-560). Structures are flat arrays:
+ *   atom_offsets  int64  [n_structures + 1]
+ *   positions     double [n_atoms * 3]
+ *   numbers       int32  [n_atoms]   atomic numbers in [0, 130)
+ *   cells         double [n_structures * 9], row-major, ROWS are lattice
+ *                 vectors (ASE convention; the reference transposes,
+ *                 src/rascal/structure_managers/atomic_structure.hh:413-449)
+ *   pbc           int32  [n_structures * 3]
+ *   center_mask   uint8  [n_atoms] or NULL (all atoms are centres)
+ * Input validation follows StructureManagerCenters::build
+ * (structure_manager_centers.cc:39-94): positions must be inside the cell
+ * (scaled coordinates in [-1e-10, 1+1e-10]), the cell must not be zero and
+ * types must be in [0, 130). */
+rgpu_status rgpu_structures_create(rgpu_structures ** out);
+rgpu_status rgpu_structures_destroy(rgpu_structures * s);
+rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures,
+                                const int64_t * atom_offsets,
+                                const double * positions,
+                                const int32_t * numbers, const double * cells,
+                                const int32_t * pbc,
+                                const uint8_t * center_mask);
+/* Replace positions only (same atoms, same cells): an MD-style update. */
+rgpu_status rgpu_structures_update_positions(rgpu_structures * s,
+                                             const double * positions);
+/* Mark the neighbour list and the features out of date without touching the
+ * inputs already on the device, so that the next call recomputes them (the
+ * reference's per-manager update flags, updateable_base.hh:91). */
+rgpu_status rgpu_structures_invalidate(rgpu_structures * s);
+/* The CUDA stream (cudaStream_t) this structure set's work runs on. */
+rgpu_status rgpu_structures_stream(const rgpu_structures * s, void ** stream);
+
+/* ---------------------------------------------------------------------- */
+/* Neighbour list.
+ * Replaces the adaptor stack centers -> neighbourlist(cutoff) ->
+ * centercontribution -> strict(cutoff)
+ * (bindings/rascal/representations/spherical_invariants.py:285-290;
+ *  src/rascal/structure_managers/adaptor_neighbour_list.hh:903-1118,
+ *  adaptor_center_contribution.hh:333-406, adaptor_strict.hh:373-455).
+ * Pairs are grouped by centre, self pair first, then the linked-cell stencil
+ * order of the reference. */
+rgpu_status rgpu_neighbour_list_build(rgpu_structures * s, double cutoff);
+rgpu_status rgpu_neighbour_list_size(const rgpu_structures * s,
+                                     int64_t * n_centers, int64_t * n_pairs);
+/* Export. centers: center_atom [n_centers] (global atom index),
+ * pair_offsets [n_centers + 1]; pairs: j_atom [n_pairs] (global index of the
+ * real atom), shift [n_pairs * 3] (periodic image), distance [n_pairs],
+ * direction [n_pairs * 3]. Any pointer may be NULL.
+ * Replaces ManagerCollection.get_distances / get_direction_vectors /
+ * get_gradients_info (bindings/bind_py_structure_manager.cc:708-905). */
+rgpu_status rgpu_neighbour_list_get(const rgpu_structures * s,
+                                    int32_t * center_atom,
+                                    int64_t * pair_offsets, int32_t * j_atom,
+                                    int32_t * shift, double * distance,
+                                    double * direction);
+
+/* ---------------------------------------------------------------------- */
+/* Representations.
+ * Replaces calculator.compute(managers)
+ * (bind_py_representation_calculator.cc:57-62 ->
+ *  calculator_spherical_invariants.hh:674-931 /
+ *  calculator_spherical_expansion.hh:2139-2411). Builds the neighbour list
+ * with the calculator's cutoff when needed. `gradients` follows the
+ * compute_gradients hyper unless forced to 1 here. */
+rgpu_status rgpu_compute(rgpu_calculator * calc, rgpu_structures * s,
+                         int precision, int gradients);
+/* Dense features (rows = centres, columns = sorted keys x inner block):
+ * get_features (bindings/bind_py_structure_manager.cc:573-614;
+ * property_block_sparse.hh:911-931). The species list of the dense layout is
+ * returned by rgpu_get_species; rgpu_get_feature_keys gives the keys present
+ * in the batch (keys[k*2+0..1]; expansion keys use only keys[k*2]).
+ * `out` is n_centers x (n_keys * inner) FP64. */
+rgpu_status rgpu_get_species(const rgpu_structures * s, int32_t * n_species,
+                             int32_t * species /* >= 130 entries */);
+rgpu_status rgpu_get_feature_keys(const rgpu_calculator * calc,
+                                  const rgpu_structures * s, int32_t * n_keys,
+                                  int32_t * keys /* >= 2 * n_keys */);
+rgpu_status rgpu_get_features(const rgpu_calculator * calc,
+                              const rgpu_structures * s, int32_t n_keys,
+                              const int32_t * keys, double * out);
+/* Dense gradients, 3 rows (x, y, z) per pair including self pairs:
+ * get_features_gradient (bind_py_structure_manager.cc:621-668;
+ * property_block_sparse.hh:961-987). `out` is 3*n_pairs x (n_keys * inner).
+ * Needs a compute with gradients at RGPU_PRECISION_FP64. */
+rgpu_status rgpu_get_features_gradient(const rgpu_calculator * calc,
+                                       const rgpu_structures * s,
+                                       int32_t n_keys, const int32_t * keys,
+                                       double * out);
+
+/* ---------------------------------------------------------------------- */
+/* Sparse GAP model.
+ * Replaces KRR(weights, Kernel(GAP, zeta), SparsePoints) prediction:
+ *   models/krr.py:92-166, models/sparse_kernels.hh:104-131,
+ *   models/sparse_kernel_predict.hh:70-266, models/sparse_points.hh:179-338.
+ * Sparse points are given dense: T [n_sparse x D] FP64 in the power-spectrum
+ * layout of `species` (sorted, n_species entries; D = n_species*(n_species+1)/2
+ * * n^2 * (l+1)), one row per sparse environment, with its central species in
+ * sparse_species [n_sparse]; weights [n_sparse]; self_contributions
+ * [n_species] (energy baseline per species, models/krr.py:68-90). */
+rgpu_status rgpu_gap_model_create(rgpu_calculator * calc, int32_t n_species,
+                                  const int32_t * species, int32_t n_sparse,
+                                  const int32_t * sparse_species,
+                                  const double * T, const double * weights,
+                                  int32_t zeta,
+                                  const double * self_contributions,
+                                  rgpu_gap_model ** out);
+rgpu_status rgpu_gap_model_destroy(rgpu_gap_model * m);
+/* Energies (n_structures, baseline included) and forces (n_atoms x 3, FP64,
+ * = -dE/dr). RGPU_PRECISION_FP64 runs the reference's own algorithm on the
+ * GPU (materialised dX/dr contracted with the scaled sparse points);
+ * RGPU_PRECISION_FP32 runs the adjoint path (dE/dC contracted with dC/dr
+ * recomputed per pair). Either output may be NULL. */
+rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s,
+                             int precision, double * energies,
+                             double * forces);
+
+/* ---------------------------------------------------------------------- */
+/* Timing support: synchronise the structure set's stream; number of kernels
+ * this library launched since the counter was last reset. */
+rgpu_status rgpu_synchronize(rgpu_structures * s);
+int64_t rgpu_kernel_launches(int reset);
+/* Device time (ms) of the stages of the last rgpu_gap_predict call, from
+ * CUDA events on the structure set's stream: 0 = whole call, 1 = neighbour
+ * list, 2 = expansion, 3 = power spectrum, 4 = forward GEMMs, 5 = backward
+ * GEMMs, 6 = power-spectrum backward (plain path: the materialised gradient
+ * chunks and their contraction), 7 = pair adjoint. */
+rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out,
+                             int32_t n_stages);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RASCAL_B200_H_ */

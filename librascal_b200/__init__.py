@@ -1,0 +1,20 @@
+"""librascal_b200: B200-native SOAP power spectrum and sparse-GAP energies and
+forces, a drop-in for librascal's descriptor hot path.
+
+Public API (same names and arguments as the reference's Python package):
+  SphericalInvariants, SphericalExpansion   representations/
+  AtomsList                                 neighbourlist/
+  SparsePoints, Kernel, KRR,
+  compute_sparse_kernel_gradients           models/
+plus StructureSet / GAPModel (direct handles on the C ABI) and gap_energy
+(torch.autograd.Function over the adjoint force path).
+"""
+from ._native import LIB_PATH, lib  # noqa: F401
+from .models import (KRR, GAPModel, Kernel, SparsePoints, compute_sparse_kernel_gradients,  # noqa: F401
+                     gap_energy)
+from .neighbourlist import AtomsList, StructureSet, frames_to_batch  # noqa: F401
+from .representations import SphericalExpansion, SphericalInvariants  # noqa: F401
+
+__all__ = ["SphericalInvariants", "SphericalExpansion", "AtomsList", "StructureSet", "SparsePoints",
+           "Kernel", "KRR", "GAPModel", "compute_sparse_kernel_gradients", "gap_energy",
+           "frames_to_batch"]

@@ -1,0 +1,1101 @@
+// C ABI and host orchestration of the B200 descriptor / GAP path.
+//
+// Host objects mirror the reference's: a calculator owns its hypers and the
+// radial spline (calculator_spherical_expansion.hh:1019-1156), a structure set
+// owns the structures, their neighbour list and the computed features
+// (ManagerCollection + Properties, structure_manager_collection.hh), a GAP
+// model owns the sparse points and weights (models/krr.py, sparse_points.hh).
+// Every device buffer is owned by one of these handles and reused across
+// calls; kernels run on the structure set's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "json_lite.h"
+
+namespace rgpu {
+int64_t launches(bool reset);
+extern bool g_tf32_split;
+}  // namespace rgpu
+
+using namespace rgpu;
+
+namespace {
+
+thread_local std::string t_err;
+thread_local int t_kind = RGPU_EXC_NONE;
+
+int fail(const Error & e) {
+  t_err = e.what();
+  t_kind = e.kind;
+  return e.code;
+}
+
+template <class F>
+int guard(F && f) {
+  try {
+    t_err.clear();
+    t_kind = RGPU_EXC_NONE;
+    f();
+    return RGPU_OK;
+  } catch (const Error & e) {
+    return fail(e);
+  } catch (const std::bad_alloc &) {
+    return fail(Error(RGPU_ERR_CUDA, "host allocation failed"));
+  } catch (const std::exception & e) {
+    return fail(Error(RGPU_ERR_INVALID_ARGUMENT, e.what()));
+  }
+}
+
+const double kPi = 3.14159265358979323846264338327950288;
+
+}  // namespace
+
+// ------------------------------------------------------------------- hypers
+namespace rgpu {
+void parse_hypers(const std::string & kind, const std::string & text, Hypers & h) {
+  Json j = Json::parse(text);
+  if (j.type != Json::Object) throw Error(RGPU_ERR_INVALID_ARGUMENT, "hypers must be a JSON object");
+  h.kind = kind;
+  if (kind != "sphericalinvariants" && kind != "sphericalexpansion")
+    throw Error(RGPU_ERR_INVALID_ARGUMENT,
+                "The representations factory " + kind +
+                    " has not been registered. The available combinations are: "
+                    "['sphericalexpansion', 'sphericalinvariants']");
+  h.max_radial = j.at("max_radial").as_int();
+  h.max_angular = j.at("max_angular").as_int();
+  if (h.max_radial < 1) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial must be >= 1");
+  if (h.max_angular < 0 || h.max_angular > kMaxL)
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular must be in [0, 12] on the GPU path");
+  h.compute_gradients = j.has("compute_gradients") ? j.at("compute_gradients").as_bool() : false;
+  if (kind == "sphericalinvariants") {
+    h.normalize = j.at("normalize").as_bool();
+    h.soap_type = j.at("soap_type").as_string();
+    if (h.soap_type != "PowerSpectrum") {
+      if (h.soap_type == "RadialSpectrum" || h.soap_type == "BiSpectrum")
+        throw Error(RGPU_ERR_INVALID_ARGUMENT,
+                    "Requested SphericalInvariants type '" + h.soap_type +
+                        "' is not on the B200 path. Supported: 'PowerSpectrum'.");
+      throw Error(RGPU_ERR_INVALID_ARGUMENT,
+                  "Requested SphericalInvariants type '" + h.soap_type +
+                      "' has not been implemented.  Must be one of: 'PowerSpectrum', "
+                      "'RadialSpectrum', or 'BiSpectrum'.");
+    }
+    if (j.has("coefficient_subselection"))
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "coefficient_subselection is not on the B200 path");
+  }
+  if (j.has("expansion_by_species_method")) {
+    std::string m = j.at("expansion_by_species_method").as_string();
+    if (m != "environment wise" && m != "user defined" && m != "structure wise")
+      throw Error(RGPU_ERR_INVALID_ARGUMENT,
+                  "expansion_by_species_method provided:'" + m +
+                      "' is not part of the implemented methods: 'environment wise', "
+                      "'structure wise', 'user defined', ");
+  }
+  const Json & fc = j.at("cutoff_function");
+  std::string fct = fc.at("type").as_string();
+  if (fct != "ShiftedCosine")
+    throw Error(RGPU_ERR_INVALID_ARGUMENT,
+                "Requested cutoff function type '" + fct + "' is not on the B200 path. Supported: "
+                                                          "'ShiftedCosine'.");
+  h.cutoff = fc.at("cutoff").at("value").as_number();
+  h.smooth_width = fc.at("smooth_width").at("value").as_number();
+  const Json & gd = j.at("gaussian_density");
+  std::string gt = gd.at("type").as_string();
+  if (gt != "Constant")
+    throw Error(RGPU_ERR_INVALID_ARGUMENT,
+                "Requested Smearing type '" + gt + "' has not been implemented.  Must be one of: 'Constant'.");
+  h.sigma = gd.at("gaussian_sigma").at("value").as_number();
+  const Json & rc = j.at("radial_contribution");
+  std::string rt = rc.at("type").as_string();
+  if (rt != "GTO")
+    throw Error(RGPU_ERR_INVALID_ARGUMENT,
+                "Requested Radial contribution type '" + rt + "' is not on the B200 path. Supported: 'GTO'.");
+  h.spline = false;
+  h.spline_accuracy = 1e-13;  // direct 1F1 evaluation is served by a spline this fine
+  if (rc.has("optimization")) {
+    const Json & o = rc.at("optimization");
+    if (o.has("RadialDimReduction"))
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "RadialDimReduction is not on the B200 path");
+    if (o.has("Spline")) {
+      h.spline = true;
+      const Json & sp = o.at("Spline");
+      if (!sp.has("accuracy")) throw Error(RGPU_ERR_INVALID_ARGUMENT, "No Spline accuracy was given.");
+      h.spline_accuracy = sp.at("accuracy").as_number();
+      if (!(h.spline_accuracy > 0)) throw Error(RGPU_ERR_INVALID_ARGUMENT, "Error bound must be > 0");
+    }
+  }
+  if (!(h.cutoff > 0)) throw Error(RGPU_ERR_INVALID_ARGUMENT, "cutoff must be > 0");
+  h.name = kind + "_" + j.dump();
+}
+}  // namespace rgpu
+
+// ------------------------------------------------------------------ handles
+struct rgpu_calculator {
+  Hypers hy;
+  RadialSpline spline;
+  DevBuf grid, y, y2h, yf, y2hf, center;
+  SplineDev dev{};
+};
+
+struct GapLayout;
+
+struct rgpu_structures {
+  cudaStream_t st{nullptr};
+  int n_struct{0};
+  int64_t n_atoms{0};
+  std::vector<int64_t> atom_off;
+  std::vector<int32_t> types;
+  std::vector<uint8_t> mask;
+  bool has_mask{false};
+  std::vector<int64_t> center_off_h;
+  DevBuf atom_off_d, pos_d, types_d, cells_d, pbc_d, tag2idx_d, ncent_d, center_off_d, atom_struct_d;
+  // staging (pinned) for host inputs
+  void * pinned{nullptr};
+  size_t pinned_cap{0};
+  // neighbour list
+  bool nl_valid{false};
+  double nl_cutoff{-1};
+  NlWork nlw;
+  NlOutputs nl;
+  std::vector<int64_t> pair_off_h;
+  // layout and features
+  std::vector<int> species;  // dense layout (sorted)
+  DevBuf lut;
+  FeatureDims fd{};
+  std::vector<int64_t> species_count;
+  DevBuf row_of_center, center_of_row, species_count_d, sort_tmp, present;
+  DevBuf C64, X64, invn64, C32, X32, norm32;
+  int feat_precision{-1};
+  const rgpu_calculator * feat_calc{nullptr};
+  bool feat_gradients{false};
+  bool feat_valid{false};
+  // GAP work
+  DevBuf E_d, F_d, K64, t64, erow64, W32, dX32, dC32, epart;
+  DevBuf dCp, dCs, dXp;
+  // status and timing
+  DevStatus * status_d{nullptr};
+  DevStatus * status_h{nullptr};
+  cudaEvent_t ev[10]{};
+  double stage_ms[10]{};
+  bool timed{false};
+};
+
+struct rgpu_gap_model {
+  rgpu_calculator * calc{nullptr};
+  std::vector<int> species;  // model layout species (sorted)
+  int M{0};
+  std::vector<int32_t> sp_species;
+  std::vector<double> T;  // M x D_model
+  std::vector<double> alpha;
+  int zeta{2};
+  std::vector<double> self_contrib;  // per model species
+  // device copies for a batch layout
+  std::vector<int> layout_species;
+  int layout_D{0};
+  std::vector<GapSpecies> segs;  // per batch species
+  DevBuf T64, alpha64, T32, Tt32, alpha32;
+  std::vector<int64_t> tt_off;  // per batch species offset into Tt32
+};
+
+namespace {
+
+void ensure_stream(rgpu_structures * s) {
+  if (!s->st) {
+    RGPU_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+    RGPU_CUDA(cudaMalloc(&s->status_d, sizeof(DevStatus)));
+    RGPU_CUDA(cudaMemset(s->status_d, 0, sizeof(DevStatus)));
+    RGPU_CUDA(cudaMallocHost(&s->status_h, sizeof(DevStatus)));
+    for (auto & e : s->ev) RGPU_CUDA(cudaEventCreate(&e));
+  }
+}
+
+void * staging(rgpu_structures * s, size_t bytes) {
+  if (bytes > s->pinned_cap) {
+    if (s->pinned) cudaFreeHost(s->pinned);
+    s->pinned = nullptr;
+    RGPU_CUDA(cudaMallocHost(&s->pinned, bytes));
+    s->pinned_cap = bytes;
+  }
+  return s->pinned;
+}
+
+// Host -> device through the pinned staging buffer, in order on the stream.
+void upload(rgpu_structures * s, DevBuf & dst, const void * src, size_t bytes) {
+  dst.ensure(bytes);
+  if (bytes == 0) return;
+  RGPU_CUDA(cudaStreamSynchronize(s->st));  // staging buffer reuse
+  void * p = staging(s, bytes);
+  std::memcpy(p, src, bytes);
+  RGPU_CUDA(cudaMemcpyAsync(dst.p, p, bytes, cudaMemcpyHostToDevice, s->st));
+}
+
+void mark(rgpu_structures * s, int i) {
+  if (s->timed) RGPU_CUDA(cudaEventRecord(s->ev[i], s->st));
+}
+
+FeatureDims make_dims(const Hypers & hy, int S) {
+  FeatureDims f;
+  f.S = S;
+  f.n = hy.max_radial;
+  f.L = hy.max_angular;
+  f.K = (f.L + 1) * (f.L + 1);
+  f.W = f.n * (f.L + 1);
+  f.nK = f.n * f.K;
+  f.P = S * (S + 1) / 2;
+  f.D = f.P * f.n * f.n * (f.L + 1);
+  f.Dpad = (f.D + 31) / 32 * 32;
+  return f;
+}
+
+// Choose the dense species layout: batch species plus `extra`.
+void set_layout(rgpu_structures * s, const Hypers & hy, const std::vector<int> & extra) {
+  std::set<int> sp(s->types.begin(), s->types.end());
+  sp.insert(extra.begin(), extra.end());
+  std::vector<int> species(sp.begin(), sp.end());
+  if (int(species.size()) > kMaxSpecies)
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, "more than 16 species in one batch is not supported on the GPU");
+  FeatureDims fd = make_dims(hy, int(species.size()));
+  bool same = species == s->species && fd.n == s->fd.n && fd.L == s->fd.L;
+  s->fd = fd;
+  if (same) return;
+  s->species = species;
+  std::vector<int8_t> lut(130, -1);
+  for (size_t i = 0; i < species.size(); ++i) lut[species[i]] = int8_t(i);
+  upload(s, s->lut, lut.data(), lut.size());
+  s->feat_valid = false;
+}
+
+void build_nl(rgpu_structures * s, double cutoff) {
+  if (s->nl_valid && s->nl_cutoff == cutoff) return;
+  NlInputs in;
+  in.n_struct = s->n_struct;
+  in.n_atoms = s->n_atoms;
+  in.atom_off = s->atom_off_d.as<int64_t>();
+  in.pos = s->pos_d.as<double>();
+  in.types = s->types_d.as<int32_t>();
+  in.cells = s->cells_d.as<double>();
+  in.pbc = s->pbc_d.as<int32_t>();
+  in.tag2idx = s->has_mask ? s->tag2idx_d.as<int32_t>() : nullptr;
+  in.n_centers = s->ncent_d.as<int32_t>();
+  in.center_off = s->center_off_d.as<int64_t>();
+  in.atom_struct = s->atom_struct_d.as<int32_t>();
+  build_neighbour_list(in, cutoff, s->nlw, s->nl, s->status_d, s->status_h, s->st);
+  s->pair_off_h.resize(s->nl.n_centers + 1);
+  RGPU_CUDA(cudaMemcpyAsync(s->pair_off_h.data(), s->nl.pair_off, sizeof(int64_t) * (s->nl.n_centers + 1),
+                            cudaMemcpyDeviceToHost, s->st));
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  s->nl_valid = true;
+  s->nl_cutoff = cutoff;
+  s->feat_valid = false;
+}
+
+ExpansionArgs exp_args(const rgpu_calculator * c, const rgpu_structures * s) {
+  ExpansionArgs a;
+  a.fd = s->fd;
+  a.sp = c->dev;
+  a.center_contrib = c->center.as<double>();
+  a.species_lut = s->lut.as<int8_t>();
+  a.rc = c->hy.cutoff;
+  a.sw = c->hy.smooth_width;
+  a.n_centers = s->nl.n_centers;
+  a.center_atom = s->nl.center_atom;
+  a.pair_off = s->nl.pair_off;
+  a.pair_j = s->nl.pair_j;
+  a.pair_dist = s->nl.pair_dist;
+  a.pair_dir = s->nl.pair_dir;
+  a.types = s->types_d.as<int32_t>();
+  return a;
+}
+
+// Species sort of the centres: row order of X (grouped by central species).
+void sort_rows(rgpu_structures * s) {
+  const int64_t nc = s->nl.n_centers;
+  s->row_of_center.ensure(sizeof(int32_t) * (nc + 1));
+  s->center_of_row.ensure(sizeof(int32_t) * (nc + 1));
+  s->species_count_d.ensure(sizeof(int64_t) * kMaxSpecies);
+  launch_species_sort(nc, s->types_d.as<int32_t>(), s->nl.center_atom, s->lut.as<int8_t>(), s->fd.S,
+                      s->species_count_d.as<int64_t>(), s->row_of_center.as<int32_t>(),
+                      s->center_of_row.as<int32_t>(), s->sort_tmp, s->st);
+  s->species_count.assign(s->fd.S, 0);
+  RGPU_CUDA(cudaMemcpyAsync(s->species_count.data(), s->species_count_d.p, sizeof(int64_t) * s->fd.S,
+                            cudaMemcpyDeviceToHost, s->st));
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+}
+
+void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, bool grads,
+                      const std::vector<int> & extra_species) {
+  build_nl(s, c->hy.cutoff);
+  set_layout(s, c->hy, extra_species);
+  if (s->feat_valid && s->feat_calc == c && s->feat_precision == precision) {
+    s->feat_gradients = s->feat_gradients || grads;
+    return;
+  }
+  mark(s, 2);
+  sort_rows(s);
+  const int64_t nc = s->nl.n_centers;
+  const FeatureDims & fd = s->fd;
+  ExpansionArgs ea = exp_args(c, s);
+  s->present.ensure(sizeof(uint32_t) * (nc + 1));
+  PsArgs pa;
+  pa.fd = fd;
+  pa.n_centers = nc;
+  pa.normalize = c->hy.normalize;
+  pa.row_of_center = s->row_of_center.as<int32_t>();
+  if (precision == RGPU_PRECISION_FP64) {
+    s->C64.ensure(sizeof(double) * size_t(nc) * fd.S * fd.nK + 64);
+    launch_expansion_fp64(ea, s->C64.as<double>(), s->present.as<uint32_t>(), s->st);
+    mark(s, 3);
+    if (c->hy.kind == "sphericalinvariants") {
+      s->X64.ensure(sizeof(double) * size_t(nc) * fd.Dpad + 64);
+      s->invn64.ensure(sizeof(double) * (nc + 1));
+      launch_ps_fwd_fp64(pa, s->C64.as<double>(), s->X64.as<double>(), s->invn64.as<double>(), s->st);
+    }
+  } else {
+    s->C32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.nK + 64);
+    launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), s->st);
+    mark(s, 3);
+    if (c->hy.kind == "sphericalinvariants") {
+      s->X32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
+      s->norm32.ensure(sizeof(float) * (nc + 1));
+      launch_ps_fwd_fp32(pa, s->C32.as<float>(), s->X32.as<float>(), s->norm32.as<float>(), s->st);
+    }
+  }
+  s->feat_valid = true;
+  s->feat_calc = c;
+  s->feat_precision = precision;
+  s->feat_gradients = grads;
+}
+
+// Keys present in the batch, as the reference's union of per-centre keys.
+std::vector<std::pair<int, int>> present_keys(const rgpu_calculator * c, const rgpu_structures * s) {
+  const int64_t nc = s->nl.n_centers;
+  std::vector<uint32_t> pres(nc);
+  RGPU_CUDA(cudaMemcpyAsync(pres.data(), s->present.p, sizeof(uint32_t) * nc, cudaMemcpyDeviceToHost, s->st));
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  std::set<uint32_t> masks(pres.begin(), pres.end());
+  std::set<std::pair<int, int>> keys;
+  for (uint32_t m : masks) {
+    for (int a = 0; a < s->fd.S; ++a) {
+      if (!(m >> a & 1)) continue;
+      if (c->hy.kind == "sphericalexpansion") {
+        keys.insert({s->species[a], s->species[a]});
+        continue;
+      }
+      for (int b = a; b < s->fd.S; ++b)
+        if (m >> b & 1) keys.insert({s->species[a], s->species[b]});
+    }
+  }
+  return std::vector<std::pair<int, int>>(keys.begin(), keys.end());
+}
+
+// Column blocks of the dense layout for the requested keys (-1 = absent).
+std::vector<int> key_blocks(const rgpu_calculator * c, const rgpu_structures * s, int n_keys,
+                            const int32_t * keys) {
+  std::vector<int> blocks(n_keys, -1);
+  std::map<int, int> sidx;
+  for (int i = 0; i < s->fd.S; ++i) sidx[s->species[i]] = i;
+  std::map<std::pair<int, int>, int> kid;
+  int k = 0;
+  for (int a = 0; a < s->fd.S; ++a)
+    for (int b = a; b < s->fd.S; ++b) kid[{a, b}] = k++;
+  for (int i = 0; i < n_keys; ++i) {
+    int ka = keys[2 * i], kb = keys[2 * i + 1];
+    if (!sidx.count(ka)) continue;
+    if (c->hy.kind == "sphericalexpansion") {
+      blocks[i] = sidx[ka];
+      continue;
+    }
+    if (!sidx.count(kb)) continue;
+    int a = sidx[ka], b = sidx[kb];
+    if (a > b) std::swap(a, b);
+    blocks[i] = kid[{a, b}];
+  }
+  return blocks;
+}
+
+// Device copies of a model's sparse points in the batch's layout.
+void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
+  const FeatureDims & fd = s->fd;
+  if (m->layout_species == s->species && m->layout_D == fd.D) return;
+  const int Sm = int(m->species.size());
+  FeatureDims fm = make_dims(m->calc->hy, Sm);
+  std::map<int, int> bidx;
+  for (int i = 0; i < fd.S; ++i) bidx[s->species[i]] = i;
+  std::vector<std::vector<int>> kb(fd.S, std::vector<int>(fd.S, -1));
+  int k = 0;
+  for (int a = 0; a < fd.S; ++a)
+    for (int b = a; b < fd.S; ++b) kb[a][b] = k++;
+  const int blk = fd.n * fd.n * (fd.L + 1);
+  // group sparse points by batch species, keep their order inside a species
+  std::vector<std::vector<int>> rows(fd.S);
+  for (int i = 0; i < m->M; ++i) rows[bidx.at(m->sp_species[i])].push_back(i);
+  m->segs.assign(fd.S, GapSpecies{});
+  std::vector<double> T(size_t(m->M) * fd.Dpad, 0.), al(m->M);
+  int pos = 0;
+  int64_t tt_total = 0;
+  m->tt_off.assign(fd.S, 0);
+  for (int sI = 0; sI < fd.S; ++sI) {
+    GapSpecies & g = m->segs[sI];
+    g.m0 = pos;
+    g.M = int(rows[sI].size());
+    g.Mpad = (g.M + 31) / 32 * 32;
+    m->tt_off[sI] = tt_total;
+    tt_total += int64_t(g.Mpad) * fd.Dpad;
+    for (int r : rows[sI]) {
+      al[pos] = m->alpha[r];
+      const double * src = &m->T[size_t(r) * fm.D];
+      double * dst = &T[size_t(pos) * fd.Dpad];
+      int km = 0;
+      for (int a = 0; a < Sm; ++a)
+        for (int b = a; b < Sm; ++b, ++km) {
+          int A = bidx.at(m->species[a]), B = bidx.at(m->species[b]);
+          int kk = kb[std::min(A, B)][std::max(A, B)];
+          std::memcpy(dst + size_t(kk) * blk, src + size_t(km) * blk, sizeof(double) * blk);
+        }
+      ++pos;
+    }
+  }
+  std::vector<float> T32(T.size()), al32(al.size());
+  for (size_t i = 0; i < T.size(); ++i) T32[i] = float(T[i]);
+  for (size_t i = 0; i < al.size(); ++i) al32[i] = float(al[i]);
+  std::vector<float> Tt(size_t(std::max<int64_t>(tt_total, 1)), 0.f);
+  for (int sI = 0; sI < fd.S; ++sI) {
+    const GapSpecies & g = m->segs[sI];
+    float * dst = &Tt[m->tt_off[sI]];
+    for (int mm = 0; mm < g.M; ++mm)
+      for (int d = 0; d < fd.D; ++d) dst[size_t(d) * g.Mpad + mm] = T32[size_t(g.m0 + mm) * fd.Dpad + d];
+  }
+  upload(s, m->T64, T.data(), sizeof(double) * T.size());
+  upload(s, m->alpha64, al.data(), sizeof(double) * al.size());
+  upload(s, m->T32, T32.data(), sizeof(float) * T32.size());
+  upload(s, m->alpha32, al32.data(), sizeof(float) * al32.size());
+  upload(s, m->Tt32, Tt.data(), sizeof(float) * Tt.size());
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  m->layout_species = s->species;
+  m->layout_D = fd.D;
+}
+
+size_t plain_budget_bytes() { return size_t(24) << 30; }
+
+void gap_plain(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * grad_d, bool forces) {
+  rgpu_calculator * c = m->calc;
+  const FeatureDims & fd = s->fd;
+  const int64_t nc = s->nl.n_centers;
+  cudaStream_t st = s->st;
+  mark(s, 4);
+  // forward GEMMs per species: k = X T^T, pointwise, t = W T
+  int Mmax = 0;
+  for (auto & g : m->segs) Mmax = std::max(Mmax, g.M);
+  s->K64.ensure(sizeof(double) * size_t(nc) * std::max(Mmax, 1) + 64);
+  s->erow64.ensure(sizeof(double) * (nc + 1));
+  s->t64.ensure(sizeof(double) * size_t(nc) * fd.Dpad + 64);
+  launch_fill_f64(s->erow64.as<double>(), nc, 0., st);
+  int64_t row0 = 0;
+  for (int sI = 0; sI < fd.S; ++sI) {
+    const int64_t rows = s->species_count[sI];
+    const GapSpecies & g = m->segs[sI];
+    if (rows > 0 && g.M > 0) {
+      const double * Xs = s->X64.as<double>() + size_t(row0) * fd.Dpad;
+      const double * Ts = m->T64.as<double>() + size_t(g.m0) * fd.Dpad;
+      double * Kb = s->K64.as<double>();
+      gemm_nt_fp64(rows, g.M, fd.D, Xs, fd.Dpad, Ts, fd.Dpad, Kb, g.M, st);
+      launch_gap_pointwise_fp64(rows, g.M, Kb, g.M, m->alpha64.as<double>() + g.m0, m->zeta, Kb, g.M,
+                                s->erow64.as<double>() + row0, st);
+      if (forces)
+        gemm_nn_fp64(rows, fd.D, g.M, Kb, g.M, Ts, fd.Dpad, s->t64.as<double>() + size_t(row0) * fd.Dpad,
+                     fd.Dpad, st);
+    } else if (forces && rows > 0) {
+      launch_fill_f64(s->t64.as<double>() + size_t(row0) * fd.Dpad, rows * fd.Dpad, 0., st);
+    }
+    row0 += rows;
+  }
+  // struct of each sorted row
+  launch_energy_reduce(nc, 0, nullptr, 0, s->erow64.as<double>(), 0, s->center_of_row.as<int32_t>(),
+                       s->nl.center_struct, E_d, st);
+  mark(s, 5);
+  mark(s, 6);
+  if (!forces) return;
+  // gradients, chunked by a memory budget: materialised d c/d r and d x/d r
+  const size_t per_pair = sizeof(double) * (3 * size_t(fd.D) + 3 * size_t(fd.nK));
+  const size_t per_center = sizeof(double) * size_t(fd.S) * 3 * fd.nK;
+  const size_t budget = plain_budget_bytes();
+  ExpansionArgs ea = exp_args(c, s);
+  PsArgs pa;
+  pa.fd = fd;
+  pa.n_centers = nc;
+  pa.normalize = c->hy.normalize;
+  pa.row_of_center = s->row_of_center.as<int32_t>();
+  int64_t c0 = 0;
+  while (c0 < nc) {
+    int64_t c1 = c0;
+    size_t bytes = 0;
+    while (c1 < nc) {
+      size_t add = per_pair * size_t(s->pair_off_h[c1 + 1] - s->pair_off_h[c1]) + per_center;
+      if (c1 > c0 && bytes + add > budget) break;
+      bytes += add;
+      ++c1;
+    }
+    const int64_t p_base = s->pair_off_h[c0];
+    const int64_t np = s->pair_off_h[c1] - p_base;
+    s->dCp.ensure(sizeof(double) * size_t(np) * 3 * fd.nK + 64);
+    s->dCs.ensure(per_center * size_t(c1 - c0) + 64);
+    s->dXp.ensure(sizeof(double) * size_t(np) * 3 * fd.D + 64);
+    launch_expansion_grad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), st);
+    launch_expansion_selfgrad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), s->dCs.as<double>(), st);
+    launch_ps_grad_fp64(pa, ea, c0, c1, p_base, s->C64.as<double>(), s->X64.as<double>(),
+                        s->invn64.as<double>(), s->dCp.as<double>(), s->dCs.as<double>(),
+                        s->dXp.as<double>(), st);
+    launch_force_contract_fp64(fd, c0, c1, p_base, s->nl.pair_off, s->nl.pair_j,
+                               s->row_of_center.as<int32_t>(), s->dXp.as<double>(), s->t64.as<double>(),
+                               fd.Dpad, grad_d, st);
+    c0 = c1;
+  }
+  mark(s, 7);
+}
+
+void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_d, bool forces) {
+  rgpu_calculator * c = m->calc;
+  const FeatureDims & fd = s->fd;
+  const int64_t nc = s->nl.n_centers;
+  cudaStream_t st = s->st;
+  mark(s, 4);
+  // per-species W and energy partial buffers
+  int64_t wtot = 0, eparts = 0;
+  for (int sI = 0; sI < fd.S; ++sI) {
+    wtot += s->species_count[sI] * m->segs[sI].Mpad;
+    eparts = std::max<int64_t>(eparts, s->species_count[sI] * ((m->segs[sI].M + 127) / 128));
+  }
+  s->W32.ensure(sizeof(float) * size_t(std::max<int64_t>(wtot, 1)) + 64);
+  s->epart.ensure(sizeof(float) * size_t(std::max<int64_t>(eparts, 1)) + 64);
+  s->dX32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
+  int64_t row0 = 0, woff = 0;
+  std::vector<int64_t> wofs(fd.S);
+  for (int sI = 0; sI < fd.S; ++sI) {
+    const int64_t rows = s->species_count[sI];
+    const GapSpecies & g = m->segs[sI];
+    wofs[sI] = woff;
+    if (rows > 0 && g.M > 0) {
+      Tf32GemmArgs a{};
+      a.M = rows;
+      a.N = g.M;
+      a.K = fd.Dpad;
+      a.A = s->X32.as<float>() + size_t(row0) * fd.Dpad;
+      a.lda = fd.Dpad;
+      a.B = m->T32.as<float>() + size_t(g.m0) * fd.Dpad;
+      a.ldb = fd.Dpad;
+      a.C = s->W32.as<float>() + woff;
+      a.ldc = g.Mpad;
+      a.epilogue = 1;
+      a.alpha = m->alpha32.as<float>() + g.m0;
+      a.zeta = m->zeta;
+      a.e_part = s->epart.as<float>();
+      gemm_tf32(a, st);
+      const int nparts = (g.M + 127) / 128;
+      launch_energy_reduce(rows, nparts, s->epart.as<float>(), rows, nullptr, row0,
+                           s->center_of_row.as<int32_t>(), s->nl.center_struct, E_d, st);
+    }
+    row0 += rows;
+    woff += rows * g.Mpad;
+  }
+  mark(s, 5);
+  if (!forces) return;
+  row0 = 0;
+  for (int sI = 0; sI < fd.S; ++sI) {
+    const int64_t rows = s->species_count[sI];
+    const GapSpecies & g = m->segs[sI];
+    if (rows > 0 && g.M > 0) {
+      Tf32GemmArgs a{};
+      a.M = rows;
+      a.N = fd.Dpad;
+      a.K = g.Mpad;
+      a.A = s->W32.as<float>() + wofs[sI];
+      a.lda = g.Mpad;
+      a.B = m->Tt32.as<float>() + m->tt_off[sI];
+      a.ldb = g.Mpad;
+      a.C = s->dX32.as<float>() + size_t(row0) * fd.Dpad;
+      a.ldc = fd.Dpad;
+      a.epilogue = 0;
+      gemm_tf32(a, st);
+    } else if (rows > 0) {
+      launch_fill_f32(s->dX32.as<float>() + size_t(row0) * fd.Dpad, rows * fd.Dpad, 0.f, st);
+    }
+    row0 += rows;
+  }
+  mark(s, 6);
+  PsArgs pa;
+  pa.fd = fd;
+  pa.n_centers = nc;
+  pa.normalize = c->hy.normalize;
+  pa.row_of_center = s->row_of_center.as<int32_t>();
+  s->dC32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.nK + 64);
+  launch_ps_bwd_fp32(pa, s->C32.as<float>(), s->X32.as<float>(), s->norm32.as<float>(),
+                     s->dX32.as<float>(), s->dC32.as<float>(), st);
+  mark(s, 7);
+  ExpansionArgs ea = exp_args(c, s);
+  launch_pair_adjoint_fp32(ea, s->dC32.as<float>(), F_d, st);
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+extern "C" {
+
+const char * rgpu_last_error(void) { return t_err.c_str(); }
+int rgpu_error_kind(void) { return t_kind; }
+int rgpu_version(void) { return 1; }
+
+rgpu_status rgpu_calculator_create(const char * kind, const char * hypers_json, rgpu_calculator ** out) {
+  return guard([&] {
+    if (!kind || !hypers_json || !out) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    auto c = std::make_unique<rgpu_calculator>();
+    parse_hypers(kind, hypers_json, c->hy);
+    build_radial_spline(c->hy, c->spline);
+    *out = c.release();
+  });
+}
+
+rgpu_status rgpu_calculator_destroy(rgpu_calculator * calc) {
+  return guard([&] { delete calc; });
+}
+
+// Device copies of the radial table, made on first use so that a calculator
+// can be built (and its FP64 table inspected) on a host without a GPU.
+static void calculator_to_device(rgpu_calculator * c) {
+  if (c->dev.y) return;
+  {
+    const RadialSpline & sp = c->spline;
+    const size_t GW = size_t(sp.grid_size) * sp.width;
+    std::vector<float> yf(GW), y2hf(GW);
+    for (size_t i = 0; i < GW; ++i) {
+      yf[i] = float(sp.y[i]);
+      y2hf[i] = float(sp.y2h[i]);
+    }
+    std::vector<double> center(sp.center.size());
+    for (size_t i = 0; i < center.size(); ++i) center[i] = sp.center[i] / std::sqrt(4.0 * kPi);
+    auto put = [](DevBuf & b, const void * src, size_t bytes) {
+      b.ensure(bytes);
+      RGPU_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+    };
+    put(c->grid, sp.grid.data(), sizeof(double) * sp.grid.size());
+    put(c->y, sp.y.data(), sizeof(double) * GW);
+    put(c->y2h, sp.y2h.data(), sizeof(double) * GW);
+    put(c->yf, yf.data(), sizeof(float) * GW);
+    put(c->y2hf, y2hf.data(), sizeof(float) * GW);
+    put(c->center, center.data(), sizeof(double) * center.size());
+    c->dev.grid = c->grid.as<double>();
+    c->dev.y = c->y.as<double>();
+    c->dev.y2h = c->y2h.as<double>();
+    c->dev.yf = c->yf.as<float>();
+    c->dev.y2hf = c->y2hf.as<float>();
+    c->dev.x1 = sp.x1;
+    c->dev.h = sp.h;
+    c->dev.inv_h = 1.0 / sp.h;
+    c->dev.ppu = sp.points_per_unit;
+    c->dev.search_size = sp.search_size;
+    c->dev.W = sp.width;
+  }
+}
+
+rgpu_status rgpu_calculator_name(const rgpu_calculator * calc, char * buf, size_t buflen) {
+  return guard([&] {
+    if (!calc || !buf) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    std::snprintf(buf, buflen, "%s", calc->hy.name.c_str());
+  });
+}
+
+rgpu_status rgpu_calculator_spline_shape(const rgpu_calculator * calc, int32_t * grid_size, int32_t * width) {
+  return guard([&] {
+    *grid_size = calc->spline.grid_size;
+    *width = calc->spline.width;
+  });
+}
+
+rgpu_status rgpu_calculator_spline_table(const rgpu_calculator * calc, double * grid, double * y, double * y2h) {
+  return guard([&] {
+    const RadialSpline & s = calc->spline;
+    if (grid) std::memcpy(grid, s.grid.data(), sizeof(double) * s.grid.size());
+    if (y) std::memcpy(y, s.y.data(), sizeof(double) * s.y.size());
+    if (y2h) std::memcpy(y2h, s.y2h.data(), sizeof(double) * s.y2h.size());
+  });
+}
+
+rgpu_status rgpu_structures_create(rgpu_structures ** out) {
+  return guard([&] {
+    auto s = std::make_unique<rgpu_structures>();
+    ensure_stream(s.get());
+    *out = s.release();
+  });
+}
+
+rgpu_status rgpu_structures_destroy(rgpu_structures * s) {
+  return guard([&] {
+    if (!s) return;
+    if (s->st) cudaStreamSynchronize(s->st);
+    if (s->pinned) cudaFreeHost(s->pinned);
+    if (s->status_h) cudaFreeHost(s->status_h);
+    if (s->status_d) cudaFree(s->status_d);
+    for (auto & e : s->ev)
+      if (e) cudaEventDestroy(e);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+  });
+}
+
+rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const int64_t * atom_offsets,
+                                const double * positions, const int32_t * numbers, const double * cells,
+                                const int32_t * pbc, const uint8_t * center_mask) {
+  return guard([&] {
+    if (!s || n_structures < 0 || !atom_offsets) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    ensure_stream(s);
+    s->n_struct = n_structures;
+    s->atom_off.assign(atom_offsets, atom_offsets + n_structures + 1);
+    if (s->atom_off[0] != 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "atom_offsets must start at 0");
+    for (int i = 0; i < n_structures; ++i)
+      if (s->atom_off[i + 1] < s->atom_off[i]) throw Error(RGPU_ERR_INVALID_ARGUMENT, "atom_offsets must be non-decreasing");
+    s->n_atoms = s->atom_off[n_structures];
+    if (s->n_atoms > (int64_t(1) << 31) - 1) throw Error(RGPU_ERR_INVALID_ARGUMENT, "too many atoms");
+    s->types.assign(numbers, numbers + s->n_atoms);
+    for (int64_t a = 0; a < s->n_atoms; ++a)
+      if (s->types[a] < 0 || s->types[a] >= 130)
+        throw Error(RGPU_ERR_STRUCTURE, "atom types (or atomic numbers) should be in the range [0, 130].");
+    s->has_mask = false;
+    if (center_mask)
+      for (int64_t a = 0; a < s->n_atoms; ++a)
+        if (!center_mask[a]) s->has_mask = true;
+    std::vector<int32_t> ncent(n_structures), astruct(s->n_atoms);
+    s->center_off_h.assign(n_structures + 1, 0);
+    std::vector<int32_t> tag2idx;
+    if (s->has_mask) tag2idx.resize(s->n_atoms);
+    for (int i = 0; i < n_structures; ++i) {
+      int64_t a0 = s->atom_off[i], a1 = s->atom_off[i + 1];
+      int nc = 0;
+      for (int64_t a = a0; a < a1; ++a) {
+        astruct[a] = i;
+        if (!center_mask || center_mask[a]) ++nc;
+      }
+      ncent[i] = nc;
+      s->center_off_h[i + 1] = s->center_off_h[i] + nc;
+      if (s->has_mask) {
+        int64_t t = a0;
+        for (int64_t a = a0; a < a1; ++a)
+          if (center_mask[a]) tag2idx[t++] = int32_t(a);
+        for (int64_t a = a0; a < a1; ++a)
+          if (!center_mask[a]) tag2idx[t++] = int32_t(a);
+      }
+    }
+    upload(s, s->atom_off_d, s->atom_off.data(), sizeof(int64_t) * (n_structures + 1));
+    upload(s, s->pos_d, positions, sizeof(double) * 3 * s->n_atoms);
+    upload(s, s->types_d, numbers, sizeof(int32_t) * s->n_atoms);
+    upload(s, s->cells_d, cells, sizeof(double) * 9 * n_structures);
+    upload(s, s->pbc_d, pbc, sizeof(int32_t) * 3 * n_structures);
+    upload(s, s->ncent_d, ncent.data(), sizeof(int32_t) * n_structures);
+    upload(s, s->center_off_d, s->center_off_h.data(), sizeof(int64_t) * (n_structures + 1));
+    upload(s, s->atom_struct_d, astruct.data(), sizeof(int32_t) * s->n_atoms);
+    if (s->has_mask) upload(s, s->tag2idx_d, tag2idx.data(), sizeof(int32_t) * s->n_atoms);
+    s->nl_valid = false;
+    s->feat_valid = false;
+  });
+}
+
+rgpu_status rgpu_structures_update_positions(rgpu_structures * s, const double * positions) {
+  return guard([&] {
+    upload(s, s->pos_d, positions, sizeof(double) * 3 * s->n_atoms);
+    s->nl_valid = false;
+    s->feat_valid = false;
+  });
+}
+
+rgpu_status rgpu_structures_invalidate(rgpu_structures * s) {
+  return guard([&] {
+    s->nl_valid = false;
+    s->feat_valid = false;
+  });
+}
+
+rgpu_status rgpu_structures_stream(const rgpu_structures * s, void ** stream) {
+  return guard([&] { *stream = static_cast<void *>(s->st); });
+}
+
+rgpu_status rgpu_neighbour_list_build(rgpu_structures * s, double cutoff) {
+  return guard([&] {
+    if (!(cutoff > 0)) throw Error(RGPU_ERR_INVALID_ARGUMENT, "cutoff must be > 0");
+    build_nl(s, cutoff);
+  });
+}
+
+rgpu_status rgpu_neighbour_list_size(const rgpu_structures * s, int64_t * n_centers, int64_t * n_pairs) {
+  return guard([&] {
+    if (!s->nl_valid) throw Error(RGPU_ERR_NOT_COMPUTED, "the neighbour list has not been built");
+    *n_centers = s->nl.n_centers;
+    *n_pairs = s->nl.n_pairs;
+  });
+}
+
+rgpu_status rgpu_neighbour_list_get(const rgpu_structures * s, int32_t * center_atom, int64_t * pair_offsets,
+                                    int32_t * j_atom, int32_t * shift, double * distance, double * direction) {
+  return guard([&] {
+    if (!s->nl_valid) throw Error(RGPU_ERR_NOT_COMPUTED, "the neighbour list has not been built");
+    const int64_t nc = s->nl.n_centers, np = s->nl.n_pairs;
+    auto get = [&](void * dst, const void * src, size_t bytes) {
+      if (dst && bytes) RGPU_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->st));
+    };
+    get(center_atom, s->nl.center_atom, sizeof(int32_t) * nc);
+    get(pair_offsets, s->nl.pair_off, sizeof(int64_t) * (nc + 1));
+    get(j_atom, s->nl.pair_j, sizeof(int32_t) * np);
+    get(shift, s->nl.pair_shift, sizeof(int32_t) * 3 * np);
+    get(distance, s->nl.pair_dist, sizeof(double) * np);
+    get(direction, s->nl.pair_dir, sizeof(double) * 3 * np);
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+  });
+}
+
+rgpu_status rgpu_compute(rgpu_calculator * calc, rgpu_structures * s, int precision, int gradients) {
+  return guard([&] {
+    if (!calc || !s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    if (precision != RGPU_PRECISION_FP64 && precision != RGPU_PRECISION_FP32)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+    bool g = gradients || calc->hy.compute_gradients;
+    if (g && s->has_mask)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "Can't compute spherical expansion gradients with masked center atoms",
+                  RGPU_EXC_LOGIC_ERROR);
+    calculator_to_device(calc);
+    s->timed = false;
+    compute_features(calc, s, precision, g, {});
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+  });
+}
+
+rgpu_status rgpu_get_species(const rgpu_structures * s, int32_t * n_species, int32_t * species) {
+  return guard([&] {
+    *n_species = int32_t(s->species.size());
+    for (size_t i = 0; i < s->species.size(); ++i) species[i] = s->species[i];
+  });
+}
+
+rgpu_status rgpu_get_feature_keys(const rgpu_calculator * calc, const rgpu_structures * s, int32_t * n_keys,
+                                  int32_t * keys) {
+  return guard([&] {
+    if (!s->feat_valid || s->feat_calc != calc) throw Error(RGPU_ERR_NOT_COMPUTED, "features have not been computed");
+    auto k = present_keys(calc, s);
+    *n_keys = int32_t(k.size());
+    if (keys)
+      for (size_t i = 0; i < k.size(); ++i) {
+        keys[2 * i] = k[i].first;
+        keys[2 * i + 1] = k[i].second;
+      }
+  });
+}
+
+rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structures * s, int32_t n_keys,
+                              const int32_t * keys, double * out) {
+  return guard([&] {
+    if (!s->feat_valid || s->feat_calc != calc) throw Error(RGPU_ERR_NOT_COMPUTED, "features have not been computed");
+    const FeatureDims & fd = s->fd;
+    const int64_t nc = s->nl.n_centers;
+    const bool ps = calc->hy.kind == "sphericalinvariants";
+    const int inner = ps ? fd.n * fd.n * (fd.L + 1) : fd.nK;
+    const int row_len = ps ? fd.Dpad : fd.S * fd.nK;
+    std::vector<int32_t> row_of(nc);
+    RGPU_CUDA(cudaMemcpyAsync(row_of.data(), s->row_of_center.p, sizeof(int32_t) * nc, cudaMemcpyDeviceToHost, s->st));
+    std::vector<double> dense(size_t(nc) * row_len);
+    if (s->feat_precision == RGPU_PRECISION_FP64) {
+      const void * src = ps ? s->X64.p : s->C64.p;
+      RGPU_CUDA(cudaMemcpyAsync(dense.data(), src, sizeof(double) * dense.size(), cudaMemcpyDeviceToHost, s->st));
+      RGPU_CUDA(cudaStreamSynchronize(s->st));
+    } else {
+      std::vector<float> tmp(dense.size());
+      const void * src = ps ? s->X32.p : s->C32.p;
+      RGPU_CUDA(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, s->st));
+      RGPU_CUDA(cudaStreamSynchronize(s->st));
+      for (size_t i = 0; i < tmp.size(); ++i) dense[i] = tmp[i];
+    }
+    auto blocks = key_blocks(calc, s, n_keys, keys);
+    for (int64_t ci = 0; ci < nc; ++ci) {
+      const double * src = &dense[size_t(ps ? row_of[ci] : ci) * row_len];
+      double * dst = out + size_t(ci) * n_keys * inner;
+      for (int k = 0; k < n_keys; ++k) {
+        if (blocks[k] < 0)
+          std::memset(dst + size_t(k) * inner, 0, sizeof(double) * inner);
+        else
+          std::memcpy(dst + size_t(k) * inner, src + size_t(blocks[k]) * inner, sizeof(double) * inner);
+      }
+    }
+  });
+}
+
+rgpu_status rgpu_get_features_gradient(const rgpu_calculator * calc, const rgpu_structures * s_in, int32_t n_keys,
+                                       const int32_t * keys, double * out) {
+  return guard([&] {
+    rgpu_structures * s = const_cast<rgpu_structures *>(s_in);
+    if (!s->feat_valid || s->feat_calc != calc) throw Error(RGPU_ERR_NOT_COMPUTED, "features have not been computed");
+    if (!s->feat_gradients) throw Error(RGPU_ERR_NOT_COMPUTED, "gradients were not requested (compute_gradients)");
+    if (s->feat_precision != RGPU_PRECISION_FP64 || calc->hy.kind != "sphericalinvariants")
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "dense gradients are exported from the FP64 power spectrum");
+    const FeatureDims & fd = s->fd;
+    const int64_t nc = s->nl.n_centers;
+    const int inner = fd.n * fd.n * (fd.L + 1);
+    auto blocks = key_blocks(calc, s, n_keys, keys);
+    ExpansionArgs ea = exp_args(calc, s);
+    PsArgs pa;
+    pa.fd = fd;
+    pa.n_centers = nc;
+    pa.normalize = calc->hy.normalize;
+    pa.row_of_center = s->row_of_center.as<int32_t>();
+    const size_t per_pair = sizeof(double) * (3 * size_t(fd.D) + 3 * size_t(fd.nK));
+    const size_t per_center = sizeof(double) * size_t(fd.S) * 3 * fd.nK;
+    const size_t budget = size_t(4) << 30;
+    std::vector<double> host;
+    int64_t c0 = 0;
+    while (c0 < nc) {
+      int64_t c1 = c0;
+      size_t bytes = 0;
+      while (c1 < nc) {
+        size_t add = per_pair * size_t(s->pair_off_h[c1 + 1] - s->pair_off_h[c1]) + per_center;
+        if (c1 > c0 && bytes + add > budget) break;
+        bytes += add;
+        ++c1;
+      }
+      const int64_t p_base = s->pair_off_h[c0];
+      const int64_t np = s->pair_off_h[c1] - p_base;
+      s->dCp.ensure(sizeof(double) * size_t(np) * 3 * fd.nK + 64);
+      s->dCs.ensure(per_center * size_t(c1 - c0) + 64);
+      s->dXp.ensure(sizeof(double) * size_t(np) * 3 * fd.D + 64);
+      launch_expansion_grad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), s->st);
+      launch_expansion_selfgrad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), s->dCs.as<double>(), s->st);
+      launch_ps_grad_fp64(pa, ea, c0, c1, p_base, s->C64.as<double>(), s->X64.as<double>(), s->invn64.as<double>(),
+                          s->dCp.as<double>(), s->dCs.as<double>(), s->dXp.as<double>(), s->st);
+      host.resize(size_t(np) * 3 * fd.D);
+      RGPU_CUDA(cudaMemcpyAsync(host.data(), s->dXp.p, sizeof(double) * host.size(), cudaMemcpyDeviceToHost, s->st));
+      RGPU_CUDA(cudaStreamSynchronize(s->st));
+      for (int64_t p = 0; p < np; ++p)
+        for (int c = 0; c < 3; ++c) {
+          const double * src = &host[(size_t(p) * 3 + c) * fd.D];
+          double * dst = out + (size_t(p_base + p) * 3 + c) * size_t(n_keys) * inner;
+          for (int k = 0; k < n_keys; ++k) {
+            if (blocks[k] < 0)
+              std::memset(dst + size_t(k) * inner, 0, sizeof(double) * inner);
+            else
+              std::memcpy(dst + size_t(k) * inner, src + size_t(blocks[k]) * inner, sizeof(double) * inner);
+          }
+        }
+      c0 = c1;
+    }
+  });
+}
+
+rgpu_status rgpu_gap_model_create(rgpu_calculator * calc, int32_t n_species, const int32_t * species,
+                                  int32_t n_sparse, const int32_t * sparse_species, const double * T,
+                                  const double * weights, int32_t zeta, const double * self_contributions,
+                                  rgpu_gap_model ** out) {
+  return guard([&] {
+    if (!calc || !out || n_species <= 0 || n_sparse < 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (calc->hy.kind != "sphericalinvariants")
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "the GAP model needs a SphericalInvariants calculator");
+    if (zeta < 1) throw Error(RGPU_ERR_INVALID_ARGUMENT, "zeta must be >= 1");
+    auto m = std::make_unique<rgpu_gap_model>();
+    m->calc = calc;
+    m->species.assign(species, species + n_species);
+    if (!std::is_sorted(m->species.begin(), m->species.end()))
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "model species must be sorted");
+    m->M = n_sparse;
+    m->sp_species.assign(sparse_species, sparse_species + n_sparse);
+    for (int sp : m->sp_species)
+      if (!std::binary_search(m->species.begin(), m->species.end(), sp))
+        throw Error(RGPU_ERR_INVALID_ARGUMENT, "sparse point species missing from the model species");
+    FeatureDims fm = make_dims(calc->hy, n_species);
+    m->T.assign(T, T + size_t(n_sparse) * fm.D);
+    m->alpha.assign(weights, weights + n_sparse);
+    m->zeta = zeta;
+    m->self_contrib.assign(n_species, 0.);
+    if (self_contributions) m->self_contrib.assign(self_contributions, self_contributions + n_species);
+    *out = m.release();
+  });
+}
+
+rgpu_status rgpu_gap_model_destroy(rgpu_gap_model * m) {
+  return guard([&] { delete m; });
+}
+
+rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precision, double * energies,
+                             double * forces) {
+  return guard([&] {
+    if (!m || !s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    if (s->has_mask)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "Can't compute spherical expansion gradients with masked center atoms",
+                  RGPU_EXC_LOGIC_ERROR);
+    calculator_to_device(m->calc);
+    s->timed = true;
+    mark(s, 0);
+    const bool want_forces = true;
+    // neighbour list, layout, features
+    build_nl(s, m->calc->hy.cutoff);
+    mark(s, 1);
+    compute_features(m->calc, s, precision, want_forces, m->species);
+    model_layout(m, s);
+    const int64_t na = s->n_atoms;
+    s->E_d.ensure(sizeof(double) * (s->n_struct + 1));
+    s->F_d.ensure(sizeof(double) * 3 * (na + 1));
+    RGPU_CUDA(cudaMemsetAsync(s->E_d.p, 0, sizeof(double) * s->n_struct, s->st));
+    RGPU_CUDA(cudaMemsetAsync(s->F_d.p, 0, sizeof(double) * 3 * na, s->st));
+    if (precision == RGPU_PRECISION_FP64)
+      gap_plain(m, s, s->E_d.as<double>(), s->F_d.as<double>(), want_forces);
+    else
+      gap_fast(m, s, s->E_d.as<double>(), s->F_d.as<double>(), want_forces);
+    mark(s, 8);
+    if (energies) {
+      RGPU_CUDA(cudaMemcpyAsync(energies, s->E_d.p, sizeof(double) * s->n_struct, cudaMemcpyDeviceToHost, s->st));
+    }
+    if (forces) {
+      RGPU_CUDA(cudaMemcpyAsync(forces, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s->st));
+    }
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    if (energies) {
+      // baseline (models/krr.py:68-90) on the host, FP64
+      std::map<int, double> sc;
+      for (size_t i = 0; i < m->species.size(); ++i) sc[m->species[i]] = m->self_contrib[i];
+      for (int st = 0; st < s->n_struct; ++st) {
+        double y0 = 0.;
+        for (int64_t a = s->atom_off[st]; a < s->atom_off[st + 1]; ++a) {
+          auto it = sc.find(s->types[a]);
+          if (it != sc.end()) y0 += it->second;
+        }
+        energies[st] += y0;
+      }
+    }
+    if (forces && precision == RGPU_PRECISION_FP64)
+      for (int64_t i = 0; i < 3 * na; ++i) forces[i] = -forces[i];
+  });
+}
+
+rgpu_status rgpu_synchronize(rgpu_structures * s) {
+  return guard([&] { RGPU_CUDA(cudaStreamSynchronize(s->st)); });
+}
+
+int64_t rgpu_kernel_launches(int reset) { return rgpu::launches(reset != 0); }
+
+rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out, int32_t n_stages) {
+  return guard([&] {
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    // 0 whole call, 1 neighbour list, 2 expansion, 3 power spectrum,
+    // 4 forward GEMMs, 5 backward GEMMs, 6 power-spectrum backward (plain:
+    // gradient chunks), 7 pair adjoint
+    const int pairs[8][2] = {{0, 8}, {0, 1}, {2, 3}, {3, 4}, {4, 5}, {5, 6}, {6, 7}, {7, 8}};
+    for (int i = 0; i < n_stages && i < 8; ++i) {
+      float ms = 0.f;
+      cudaError_t e = cudaEventElapsedTime(&ms, s->ev[pairs[i][0]], s->ev[pairs[i][1]]);
+      ms_out[i] = (e == cudaSuccess) ? ms : -1.0;
+    }
+  });
+}
+
+}  // extern "C"

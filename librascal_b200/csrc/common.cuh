@@ -1,0 +1,221 @@
+// Device helpers shared by the kernel files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "rgpu_internal.h"
+
+namespace rgpu {
+
+constexpr int kMaxL = 12;        // largest max_angular the GPU kernels support
+constexpr int kMaxSpecies = 16;  // largest species count of a dense layout
+
+__device__ __forceinline__ void set_status(DevStatus * st, int code, int where, int detail) {
+  if (atomicCAS(&st->code, 0, code) == 0) {
+    st->where = where;
+    st->detail = detail;
+  }
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+inline int div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }
+
+// Spherical-harmonics constants per (l, m), double and float copies:
+// coeff_a, coeff_b (math/spherical_harmonics.cc:54-64), sqrt(2l+1) and
+// -sqrt(1 + 1/(2l)) (:67-71), and the ladder factors sqrt((l-m)(l+m+1))
+// (:86-91). Index l*(kMaxL+2)+m.
+struct SphConst {
+  double a[(kMaxL + 1) * (kMaxL + 2)];
+  double b[(kMaxL + 1) * (kMaxL + 2)];
+  double plm[(kMaxL + 1) * (kMaxL + 2)];
+  double c1[kMaxL + 1];
+  double c2[kMaxL + 1];
+  float af[(kMaxL + 1) * (kMaxL + 2)];
+  float bf[(kMaxL + 1) * (kMaxL + 2)];
+  float plmf[(kMaxL + 1) * (kMaxL + 2)];
+  float c1f[kMaxL + 1];
+  float c2f[kMaxL + 1];
+};
+// Each translation unit that evaluates spherical harmonics holds its own copy
+// (no relocatable device code); sph_constants_tu() fills it once.
+static __constant__ SphConst c_sph;
+SphConst make_sph_constants();
+static inline void sph_constants_tu() {
+  static bool done = false;
+  if (done) return;
+  SphConst h = make_sph_constants();
+  cuda_check(cudaMemcpyToSymbol(c_sph, &h, sizeof(h)), "cudaMemcpyToSymbol(c_sph)");
+  done = true;
+}
+
+template <typename T>
+struct SphC;
+template <>
+struct SphC<double> {
+  static __device__ __forceinline__ double a(int i) { return c_sph.a[i]; }
+  static __device__ __forceinline__ double b(int i) { return c_sph.b[i]; }
+  static __device__ __forceinline__ double plm(int i) { return c_sph.plm[i]; }
+  static __device__ __forceinline__ double c1(int l) { return c_sph.c1[l]; }
+  static __device__ __forceinline__ double c2(int l) { return c_sph.c2[l]; }
+};
+template <>
+struct SphC<float> {
+  static __device__ __forceinline__ float a(int i) { return c_sph.af[i]; }
+  static __device__ __forceinline__ float b(int i) { return c_sph.bf[i]; }
+  static __device__ __forceinline__ float plm(int i) { return c_sph.plmf[i]; }
+  static __device__ __forceinline__ float c1(int l) { return c_sph.c1f[l]; }
+  static __device__ __forceinline__ float c2(int l) { return c_sph.c2f[l]; }
+};
+
+// Real spherical harmonics of a unit vector and (optionally) their Cartesian
+// gradients, following math/spherical_harmonics.cc:97-363: associated
+// Legendre functions by the l-recurrence, cos/sin(m phi) by the Chebyshev
+// recurrence, storage order (l, m = -l..l), pole branch at sin(theta) <= 0.1.
+// The callback receives (lm, Y, dY/dx, dY/dy, dY/dz) for every lm in order.
+template <int L, bool DER, typename T, typename Emit>
+__device__ __forceinline__ void spherical_harmonics(T x, T y, T z, Emit && emit) {
+  constexpr int S = kMaxL + 2;
+  const T nrm2 = x * x + y * y + z * z;
+  if (fabs(double(nrm2) - 1.0) > (sizeof(T) == 8 ? 100.0 * 2.220446049250313e-16 : 1e-5)) {
+    T inv = T(1) / sqrt(nrm2);
+    x *= inv;
+    y *= inv;
+    z *= inv;
+  }
+  const T cos_t = z;
+  const T sxy = hypot(x, y);
+  T cos_p = T(1), sin_p = T(0);
+  if (sxy >= T(100.0 * 2.220446049250313e-16)) {
+    cos_p = x / sxy;
+    sin_p = y / sxy;
+  }
+  const T sin_t = sqrt(T(1) - cos_t * cos_t);
+  const T sin_td = sxy;  // sin(theta) used by the derivative formulas
+  T cm[L + 2], sm[L + 2];
+#pragma unroll
+  for (int m = 0; m < L + 2; ++m) {
+    if (m == 0) {
+      cm[0] = T(1);
+      sm[0] = T(0);
+    } else if (m == 1) {
+      cm[1] = cos_p;
+      sm[1] = sin_p;
+    } else {
+      cm[m] = T(2) * cos_p * cm[m - 1] - cm[m - 2];
+      sm[m] = T(2) * cos_p * sm[m - 1] - sm[m - 2];
+    }
+  }
+  const T inv_sqrt2 = T(0.707106781186547524400844362104849039);
+  const T sqrt_inv_2pi = T(0.398942280401432677939946059934381868);  // sqrt(1/(2 pi))
+  T p2[L + 2], p1[L + 2], p0[L + 2];  // rows l-2, l-1, l
+#pragma unroll
+  for (int m = 0; m < L + 2; ++m) p2[m] = p1[m] = p0[m] = T(0);
+  T l_accum = sqrt_inv_2pi;
+#pragma unroll
+  for (int l = 0; l <= L; ++l) {
+    if (l == 0) {
+      p0[0] = sqrt_inv_2pi;
+    } else if (l == 1) {
+      p0[0] = cos_t * T(1.7320508075688772935274463415058723) * sqrt_inv_2pi;
+      l_accum = l_accum * -T(1.2247448713915890491) * sin_t;  // -sqrt(3/2)
+      p0[1] = l_accum;
+    } else {
+#pragma unroll
+      for (int m = 0; m < l - 1; ++m) {
+        T v = cos_t * p1[m];
+        v += SphC<T>::b(l * S + m) * p2[m];
+        v *= SphC<T>::a(l * S + m);
+        p0[m] = v;
+      }
+      p0[l - 1] = l_accum * cos_t * SphC<T>::c1(l);
+      l_accum = l_accum * sin_t * SphC<T>::c2(l);
+      p0[l] = l_accum;
+    }
+#pragma unroll
+    for (int m = l + 1; m < L + 2; ++m) p0[m] = T(0);
+    const int base = l * l + l;
+    // Y values
+    T Yv[2 * L + 1];
+#pragma unroll
+    for (int m = 0; m <= l; ++m) {
+      Yv[l + m] = p0[m] * cm[m];
+      Yv[l - m] = p0[m] * sm[m];
+    }
+    Yv[l] = p0[0] * inv_sqrt2;
+    if (!DER || l == 0) {
+#pragma unroll
+      for (int k = 0; k < 2 * l + 1; ++k) emit(base - l + k, Yv[k], T(0), T(0), T(0));
+    } else {
+      const T pl0 = SphC<T>::plm(l * S + 0);
+      emit(base, Yv[l], cos_t * cos_p * pl0 * inv_sqrt2 * p0[1],
+           cos_t * sin_p * pl0 * inv_sqrt2 * p0[1], T(-1) * sin_td * pl0 * inv_sqrt2 * p0[1]);
+#pragma unroll
+      for (int k = 0; k < l; ++k) {
+        const int m = k + 1;
+        const T pk = SphC<T>::plm(l * S + k), pk1 = SphC<T>::plm(l * S + k + 1);
+        const T lpd = pk * p0[k] - pk1 * p0[k + 2];
+        T pdf;
+        if (sin_td > T(0.1))
+          pdf = T(k + 1) / sin_td * p0[k + 1];
+        else
+          pdf = T(-0.5) / cos_t * (pk * p0[k] + pk1 * p0[k + 2]);
+        T dxp = sin_p * pdf * sm[m];
+        dxp += T(-0.5) * cos_t * cos_p * cm[m] * lpd;
+        T dxn = T(-1) * sin_p * pdf * cm[m];
+        dxn += T(-0.5) * cos_t * cos_p * sm[m] * lpd;
+        T dyp = T(-1) * cos_p * pdf * sm[m];
+        dyp += T(-0.5) * cos_t * sin_p * cm[m] * lpd;
+        T dyn = cos_p * pdf * cm[m];
+        dyn += T(-0.5) * cos_t * sin_p * sm[m] * lpd;
+        T dzp = T(0.5) * sin_td * cm[m] * lpd;
+        T dzn = T(0.5) * sin_td * sm[m] * lpd;
+        emit(base + m, Yv[l + m], dxp, dyp, dzp);
+        emit(base - m, Yv[l - m], dxn, dyn, dzn);
+      }
+    }
+#pragma unroll
+    for (int m = 0; m < L + 2; ++m) {
+      p2[m] = p1[m];
+      p1[m] = p0[m];
+    }
+  }
+}
+
+// Cubic-spline evaluation of the radial table at r: index search with the
+// reference's points-per-unit quirk (math/interpolator.cc:214-230), value and
+// derivative formulas of math/interpolator.cc:177-212.
+struct SplinePos {
+  int k;
+  double a, b;
+};
+__device__ __forceinline__ SplinePos spline_pos(const SplineDev & s, double r) {
+  SplinePos p;
+  int k = static_cast<int>((r - s.x1) * s.ppu) - 1;
+  k = max(0, min(s.search_size, k));
+  p.k = k;
+  p.a = (s.grid[k + 1] - r) / s.h;
+  p.b = 1 - p.a;
+  return p;
+}
+
+}  // namespace rgpu

@@ -1,0 +1,324 @@
+// Spherical expansion of the neighbour density: coefficients and (plain path)
+// their position gradients.
+//
+// c^i_{a n lm} = [a == type_i] center_n / sqrt(4 pi) delta_{lm,00}
+//              + sum_{j != i, type_j = a} f_c(r_ij) RI_nl(r_ij) Y_lm(r^_ij)
+// grad_j c^i   = (dRI f_c + RI df_c) Y dir + RI f_c / r grad Y
+// grad_i c^i   = - sum_j grad_j c^i over j that are not images of i
+// (src/rascal/representations/calculator_spherical_expansion.hh:2234-2366;
+// the orthonormalised RI comes from the cubic spline, :1019-1156).
+//
+// Work decomposition: one warp per centre. Lanes first evaluate one pair each
+// (spline row fetch, spherical harmonics by recurrence) into shared memory,
+// then each lane owns output elements (n, lm) and accumulates the pairs of
+// each neighbour species in turn.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace rgpu {
+namespace {
+
+constexpr int kWarps = 4;
+
+template <typename T>
+struct Tab;
+template <>
+struct Tab<double> {
+  static __device__ __forceinline__ const double * y(const SplineDev & s) { return s.y; }
+  static __device__ __forceinline__ const double * d(const SplineDev & s) { return s.y2h; }
+};
+template <>
+struct Tab<float> {
+  static __device__ __forceinline__ const float * y(const SplineDev & s) { return s.yf; }
+  static __device__ __forceinline__ const float * d(const SplineDev & s) { return s.y2hf; }
+};
+
+__device__ __forceinline__ double fc_cos(double r, double rc, double sw) {
+  if (r <= (rc - sw)) return 1.0;
+  if (r > rc) return 0.0;
+  double rs = 3.14159265358979323846264338327950288 * (r - rc + sw) / sw;
+  return 0.5 * (1. + cos(rs));
+}
+__device__ __forceinline__ double dfc_cos(double r, double rc, double sw) {
+  if (r <= (rc - sw)) return 0.0;
+  if (r > rc) return 0.0;
+  double rs = 3.14159265358979323846264338327950288 * (r - rc + sw) / sw;
+  return -0.5 * 3.14159265358979323846264338327950288 / sw * sin(rs);
+}
+
+// Evaluate RI (and optionally dRI) of all W channels at r into smem columns.
+template <typename T, bool DER>
+__device__ __forceinline__ void spline_eval(const SplineDev & sp, double r, T * RI, T * dRI,
+                                            int stride) {
+  SplinePos q = spline_pos(sp, r);
+  const T a = T(q.a), b = T(q.b);
+  const T * y0 = Tab<T>::y(sp) + size_t(q.k) * sp.W;
+  const T * d0 = Tab<T>::d(sp) + size_t(q.k) * sp.W;
+  const T * y1 = y0 + sp.W;
+  const T * d1 = d0 + sp.W;
+  const T ca = a * a - T(1), cb = b * b - T(1);
+  const T ea = T(3) * a * a - T(1), eb = T(3) * b * b - T(1);
+  const T ih = T(sp.inv_h);
+  for (int c = 0; c < sp.W; ++c) {
+    T yy0 = __ldg(y0 + c), yy1 = __ldg(y1 + c), dd0 = __ldg(d0 + c), dd1 = __ldg(d1 + c);
+    RI[c * stride] = a * (yy0 + ca * dd0) + b * (yy1 + cb * dd1);
+    if (DER) {
+      if (sizeof(T) == 8)
+        dRI[c * stride] = (yy1 - yy0 - ea * dd0 + eb * dd1) / T(sp.h);
+      else
+        dRI[c * stride] = (yy1 - yy0 - ea * dd0 + eb * dd1) * ih;
+    }
+  }
+}
+
+template <typename T, int L>
+__global__ void __launch_bounds__(kWarps * 32)
+expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ present) {
+  constexpr int K = (L + 1) * (L + 1);
+  constexpr int L1 = L + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int W = a.fd.W, nK = a.fd.nK, S = a.fd.S, n = a.fd.n;
+  T * RI = reinterpret_cast<T *>(smem_raw) + size_t(wid) * (W + K + 1) * 32;
+  T * Y = RI + W * 32;
+  T * FC = Y + K * 32;
+  __shared__ int8_t sp_s[kWarps][32];
+  __shared__ uint8_t order_s[kWarps][32];
+  __shared__ uint8_t lofk[K];
+  for (int lm = threadIdx.x; lm < K; lm += blockDim.x) {
+    int l = 0;
+    while ((l + 1) * (l + 1) <= lm) ++l;
+    lofk[lm] = uint8_t(l);
+  }
+  __syncthreads();
+  for (int64_t ci = int64_t(blockIdx.x) * kWarps + wid; ci < a.n_centers;
+       ci += int64_t(gridDim.x) * kWarps) {
+    T * Ci = C + size_t(ci) * S * nK;
+    for (int e = lane; e < S * nK; e += 32) Ci[e] = T(0);
+    __syncwarp();
+    const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
+    const int ti = a.species_lut[a.types[a.center_atom[ci]]];
+    uint32_t mask_all = 1u << ti;
+    for (int64_t p0 = p_lo; p0 < p_hi; p0 += 32) {
+      const int np = int(min(int64_t(32), p_hi - p0));
+      int my_sp = 31;
+      if (lane < np) {
+        const int64_t p = p0 + lane;
+        const double r = a.pair_dist[p];
+        my_sp = a.species_lut[a.types[a.pair_j[p]]];
+        FC[lane] = T(fc_cos(r, a.rc, a.sw));
+        spline_eval<T, false>(a.sp, r, RI + lane, nullptr, 32);
+        const T dx = T(a.pair_dir[3 * p]), dy = T(a.pair_dir[3 * p + 1]),
+                dz = T(a.pair_dir[3 * p + 2]);
+        spherical_harmonics<L, false, T>(dx, dy, dz, [&](int lm, T y, T, T, T) {
+          Y[lm * 32 + lane] = y;
+        });
+      }
+      // stable order of the chunk's pairs by species
+      int before = 0, cnt_sp[kMaxSpecies];
+      unsigned my_mask = 0;
+      for (int s = 0; s < S; ++s) {
+        unsigned m = __ballot_sync(0xffffffffu, my_sp == s);
+        cnt_sp[s] = __popc(m);
+        if (my_sp == s) my_mask = m;
+        if (s < my_sp) before += __popc(m);
+        if (m) mask_all |= 1u << s;
+      }
+      if (lane < np) {
+        order_s[wid][before + __popc(my_mask & lanemask_lt())] = uint8_t(lane);
+        sp_s[wid][lane] = int8_t(my_sp);
+      }
+      __syncwarp();
+      int start = 0;
+      for (int s = 0; s < S; ++s) {
+        const int cnt = cnt_sp[s];
+        if (cnt == 0) continue;
+        T * Cs = Ci + size_t(s) * nK;
+        for (int e = lane; e < nK; e += 32) {
+          const int nn = e / K, lm = e - nn * K;
+          const int l = lofk[lm];
+          const T * ri = RI + (nn * L1 + l) * 32;
+          const T * yy = Y + lm * 32;
+          T acc = T(0);
+          for (int q = 0; q < cnt; ++q) {
+            const int pl = order_s[wid][start + q];
+            acc += (ri[pl] * yy[pl]) * FC[pl];
+          }
+          Cs[e] += acc;
+        }
+        start += cnt;
+      }
+      __syncwarp();
+    }
+    // centre contribution, orthonormalised (calculator_spherical_expansion.hh:2244-2247)
+    for (int nn = lane; nn < n; nn += 32) Ci[size_t(ti) * nK + nn * K] += T(a.center_contrib[nn]);
+    if (lane == 0) present[ci] = mask_all;
+    __syncwarp();
+  }
+}
+
+// Plain path: grad_j c^i for every non-self pair of centres [c0, c1); each
+// lane streams its pair's 3 x n x K block.
+template <int L>
+__global__ void __launch_bounds__(kWarps * 32)
+expansion_grad_kernel(ExpansionArgs a, int64_t c0, int64_t c1, int64_t p_base,
+                      double * __restrict__ dCp) {
+  constexpr int K = (L + 1) * (L + 1);
+  constexpr int L1 = L + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int W = a.fd.W, n = a.fd.n, nK = a.fd.nK;
+  double * RI = reinterpret_cast<double *>(smem_raw) + size_t(wid) * 2 * W * 32;
+  double * P1 = RI + W * 32;
+  for (int64_t ci = c0 + int64_t(blockIdx.x) * kWarps + wid; ci < c1;
+       ci += int64_t(gridDim.x) * kWarps) {
+    const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
+    for (int64_t p = p_lo + lane; p < p_hi; p += 32) {
+      const double r = a.pair_dist[p];
+      const double fc = fc_cos(r, a.rc, a.sw), dfc = dfc_cos(r, a.rc, a.sw);
+      spline_eval<double, true>(a.sp, r, RI + lane, P1 + lane, 32);
+      for (int c = 0; c < W; ++c) {
+        // p1 = dRI f_c + RI df_c
+        P1[c * 32 + lane] = (P1[c * 32 + lane] * fc) + (RI[c * 32 + lane] * dfc);
+      }
+      const double dir[3] = {a.pair_dir[3 * p], a.pair_dir[3 * p + 1], a.pair_dir[3 * p + 2]};
+      double * out = dCp + size_t(p - p_base) * 3 * nK;
+      spherical_harmonics<L, true, double>(dir[0], dir[1], dir[2],
+                                           [&](int lm, double y, double gx, double gy, double gz) {
+        int l = 0;
+#pragma unroll
+        for (int ll = 1; ll <= L; ++ll) l += (lm >= ll * ll);
+        const double g[3] = {gx, gy, gz};
+        for (int nn = 0; nn < n; ++nn) {
+          const double p1 = P1[(nn * L1 + l) * 32 + lane];
+          const double ri = RI[(nn * L1 + l) * 32 + lane];
+#pragma unroll
+          for (int cc = 0; cc < 3; ++cc)
+            out[cc * nK + nn * K + lm] = (p1 * y) * dir[cc] + ((ri * g[cc]) * fc) / r;
+        }
+      });
+    }
+  }
+}
+
+// Plain path: grad_i c^i = - sum over non-image neighbours, per species block.
+__global__ void expansion_selfgrad_kernel(ExpansionArgs a, int64_t c0, int64_t p_base,
+                                          const double * __restrict__ dCp,
+                                          double * __restrict__ dCs) {
+  const int64_t ci = c0 + blockIdx.x;
+  const int nK3 = 3 * a.fd.nK, S = a.fd.S;
+  const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
+  const int32_t self_atom = a.center_atom[ci];
+  double * out = dCs + size_t(blockIdx.x) * S * nK3;
+  for (int s = 0; s < S; ++s) {
+    for (int e = threadIdx.x; e < nK3; e += blockDim.x) {
+      double acc = 0.;
+      for (int64_t p = p_lo; p < p_hi; ++p) {
+        const int32_t j = a.pair_j[p];
+        if (j == self_atom) continue;  // periodic image of the centre
+        if (a.species_lut[a.types[j]] != s) continue;
+        acc -= dCp[size_t(p - p_base) * nK3 + e];
+      }
+      out[size_t(s) * nK3 + e] = acc;
+    }
+  }
+}
+
+template <typename T>
+size_t exp_smem(const FeatureDims & fd) {
+  return size_t(kWarps) * (fd.W + fd.K + 1) * 32 * sizeof(T);
+}
+
+template <typename T>
+void launch_exp(const ExpansionArgs & a, T * C, uint32_t * present, cudaStream_t st) {
+  if (a.n_centers == 0) return;
+  sph_constants_tu();
+  const size_t smem = exp_smem<T>(a.fd);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int grid = int(std::min<int64_t>((a.n_centers + kWarps - 1) / kWarps, int64_t(sms) * 16));
+#define RGPU_EXP_CASE(LL)                                                                   \
+  case LL:                                                                                  \
+    RGPU_CUDA(cudaFuncSetAttribute(expansion_kernel<T, LL>,                                 \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    expansion_kernel<T, LL><<<grid, kWarps * 32, smem, st>>>(a, C, present);                \
+    break;
+  switch (a.fd.L) {
+    RGPU_EXP_CASE(0)
+    RGPU_EXP_CASE(1)
+    RGPU_EXP_CASE(2)
+    RGPU_EXP_CASE(3)
+    RGPU_EXP_CASE(4)
+    RGPU_EXP_CASE(5)
+    RGPU_EXP_CASE(6)
+    RGPU_EXP_CASE(7)
+    RGPU_EXP_CASE(8)
+    RGPU_EXP_CASE(9)
+    RGPU_EXP_CASE(10)
+    RGPU_EXP_CASE(11)
+    RGPU_EXP_CASE(12)
+    default:
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
+  }
+#undef RGPU_EXP_CASE
+  RGPU_LAUNCHED();
+  RGPU_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+void launch_expansion_fp64(const ExpansionArgs & a, double * C, uint32_t * present,
+                           cudaStream_t st) {
+  launch_exp<double>(a, C, present, st);
+}
+void launch_expansion_fp32(const ExpansionArgs & a, float * C, uint32_t * present,
+                           cudaStream_t st) {
+  launch_exp<float>(a, C, present, st);
+}
+
+void launch_expansion_grad_fp64(const ExpansionArgs & a, int64_t c0, int64_t c1, int64_t p_base,
+                                double * dCp, cudaStream_t st) {
+  if (c1 <= c0) return;
+  sph_constants_tu();
+  const size_t smem = size_t(kWarps) * 2 * a.fd.W * 32 * sizeof(double);
+  int grid = int(std::min<int64_t>((c1 - c0 + kWarps - 1) / kWarps, 148 * 16));
+#define RGPU_GRAD_CASE(LL)                                                                  \
+  case LL:                                                                                  \
+    RGPU_CUDA(cudaFuncSetAttribute(expansion_grad_kernel<LL>,                               \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+    expansion_grad_kernel<LL><<<grid, kWarps * 32, smem, st>>>(a, c0, c1, p_base, dCp);     \
+    break;
+  switch (a.fd.L) {
+    RGPU_GRAD_CASE(0)
+    RGPU_GRAD_CASE(1)
+    RGPU_GRAD_CASE(2)
+    RGPU_GRAD_CASE(3)
+    RGPU_GRAD_CASE(4)
+    RGPU_GRAD_CASE(5)
+    RGPU_GRAD_CASE(6)
+    RGPU_GRAD_CASE(7)
+    RGPU_GRAD_CASE(8)
+    RGPU_GRAD_CASE(9)
+    RGPU_GRAD_CASE(10)
+    RGPU_GRAD_CASE(11)
+    RGPU_GRAD_CASE(12)
+    default:
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
+  }
+#undef RGPU_GRAD_CASE
+  RGPU_LAUNCHED();
+  RGPU_CUDA(cudaGetLastError());
+}
+
+void launch_expansion_selfgrad_fp64(const ExpansionArgs & a, int64_t c0, int64_t c1,
+                                    int64_t p_base, const double * dCp, double * dCs,
+                                    cudaStream_t st) {
+  if (c1 <= c0) return;
+  expansion_selfgrad_kernel<<<int(c1 - c0), 256, 0, st>>>(a, c0, p_base, dCp, dCs);
+  RGPU_LAUNCHED();
+  RGPU_CUDA(cudaGetLastError());
+}
+
+}  // namespace rgpu

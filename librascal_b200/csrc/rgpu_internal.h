@@ -1,0 +1,257 @@
+// Internal declarations shared by the host orchestration (api.cu) and the
+// kernel files. Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/rascal_b200.h"
+
+namespace rgpu {
+
+// Library error carrying an rgpu_status and the reference exception kind.
+struct Error : std::runtime_error {
+  int code;
+  int kind;
+  Error(int c, const std::string & m, int k = -1)
+      : std::runtime_error(m), code(c),
+        kind(k >= 0 ? k
+                    : (c == RGPU_ERR_OVERFLOW
+                           ? RGPU_EXC_OVERFLOW_ERROR
+                           : (c == RGPU_ERR_INVALID_ARGUMENT ? RGPU_EXC_LOGIC_ERROR
+                                                             : RGPU_EXC_RUNTIME_ERROR))) {}
+};
+
+void cuda_check(cudaError_t e, const char * what);
+#define RGPU_CUDA(x) ::rgpu::cuda_check((x), #x)
+// Counts launches of this library's kernels (reported by the bench).
+void count_launch(int n = 1);
+#define RGPU_LAUNCHED() ::rgpu::count_launch(1)
+
+// Parsed calculator hypers (the subset the GPU path supports).
+struct Hypers {
+  std::string kind;  // "sphericalinvariants" | "sphericalexpansion"
+  std::string name;  // registry name: prefix + canonical JSON dump
+  std::string soap_type{"PowerSpectrum"};
+  int max_radial{0}, max_angular{0};
+  double cutoff{0}, smooth_width{0}, sigma{0};
+  bool spline{true};
+  double spline_accuracy{1e-8};
+  bool normalize{true};
+  bool compute_gradients{false};
+};
+void parse_hypers(const std::string & kind, const std::string & json, Hypers & out);
+
+// FP64 natural cubic spline of the orthonormalised GTO radial integral,
+// grid_size x width values (width = n_max * (l_max + 1), index n*(l+1)+l).
+struct RadialSpline {
+  int grid_size{0}, width{0}, search_size{0};
+  double x1{0}, h{0}, points_per_unit{0};
+  std::vector<double> grid, y, y2h, center;
+  void interpolate(double x, double * out) const;
+};
+void build_radial_spline(const Hypers & hy, RadialSpline & out);
+
+// Growable device buffer (reused across calls; never shrinks).
+struct DevBuf {
+  void * p{nullptr};
+  size_t cap{0};
+  void ensure(size_t bytes);
+  void release();
+  template <class T>
+  T * as() const {
+    return static_cast<T *>(p);
+  }
+  ~DevBuf() { release(); }
+};
+
+// Device view of the radial spline (both precisions).
+struct SplineDev {
+  const double * grid;
+  const double * y;    // [G][W]
+  const double * y2h;  // [G][W]
+  const float * yf;
+  const float * y2hf;
+  double x1, h, inv_h, ppu;
+  int search_size, W;
+};
+
+// Per-structure cell-list geometry (device POD), written by nl_setup.
+struct NlGeom {
+  double cell[9];  // reference layout: cell[i*3+j] = component i of lattice vector j
+  double cinv[9];
+  double mesh_min[3], ghost_min[3], ghost_max[3];
+  double bound_tol;
+  int nboxes[3], pmin[3], reps[3];
+  int n_atoms, n_centers;
+};
+
+// Status word written by kernels (first error wins).
+struct DevStatus {
+  int code;
+  int where;  // structure or item index
+  int detail;
+  int pad;
+};
+
+// ------------------------------------------------------------------ scans
+// Exclusive prefix sum of n int64 values, out[n] = total. `tmp` scratch.
+void scan_exclusive_i64(const int64_t * in, int64_t * out, int64_t n, DevBuf & tmp,
+                        cudaStream_t st);
+void scan_exclusive_i32to64(const int32_t * in, int64_t * out, int64_t n, DevBuf & tmp,
+                            cudaStream_t st);
+
+// ------------------------------------------------------------------ NL
+struct NlBuffers;  // defined in nl.cu
+struct NlInputs {
+  int n_struct;
+  int64_t n_atoms;
+  const int64_t * atom_off;    // [n_struct+1]
+  const double * pos;          // [n_atoms*3] original order
+  const int32_t * types;       // [n_atoms]
+  const double * cells;        // [n_struct*9] ASE rows
+  const int32_t * pbc;         // [n_struct*3]
+  const int32_t * tag2idx;     // [n_atoms] global original index of each tag, or null
+  const int32_t * n_centers;   // [n_struct]
+  const int64_t * center_off;  // [n_struct+1]
+  const int32_t * atom_struct; // [n_atoms]
+};
+struct NlOutputs {
+  int64_t n_centers{0}, n_pairs{0};
+  int32_t * center_atom{nullptr};   // [n_centers] global original index
+  int32_t * center_struct{nullptr}; // [n_centers]
+  int64_t * pair_off{nullptr};      // [n_centers+1]
+  int32_t * pair_j{nullptr};        // [n_pairs] global original index of the real atom
+  int32_t * pair_shift{nullptr};    // [n_pairs*3]
+  double * pair_dist{nullptr};      // [n_pairs]
+  double * pair_dir{nullptr};       // [n_pairs*3]
+};
+struct NlWork {
+  DevBuf geom, counts64, scan_tmp, ghost_off, site_x, site_type, site_real, site_shift,
+      site_box, box_base, box_count, box_ptr, box_fill, sorted, sorted_x, sorted_info,
+      pair_count;
+  DevBuf center_atom, center_struct, pair_off, pair_j, pair_shift, pair_dist, pair_dir;
+};
+// Builds the full list with self pairs and the strict cutoff. Synchronises
+// the stream a few times to size buffers. Throws Error on invalid input.
+void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutputs & out,
+                          DevStatus * status_dev, DevStatus * status_host, cudaStream_t st);
+
+// ------------------------------------------------------------------ features
+struct FeatureDims {
+  int S;  // species in the dense layout
+  int n, L, K, W;
+  int nK;     // n*K
+  int P;      // species pairs S(S+1)/2
+  int D;      // P*n*n*(L+1)
+  int Dpad;   // D rounded up to 32
+};
+
+struct ExpansionArgs {
+  FeatureDims fd;
+  SplineDev sp;
+  const double * center_contrib;  // [n] / sqrt(4 pi) already applied
+  const int8_t * species_lut;     // [130] -> species index or -1
+  double rc, sw;
+  int64_t n_centers;
+  const int32_t * center_atom;
+  const int64_t * pair_off;
+  const int32_t * pair_j;
+  const double * pair_dist;
+  const double * pair_dir;
+  const int32_t * types;
+};
+// C[i][S][n][K] and the per-centre species presence bitmask.
+void launch_expansion_fp64(const ExpansionArgs & a, double * C, uint32_t * present,
+                           cudaStream_t st);
+void launch_expansion_fp32(const ExpansionArgs & a, float * C, uint32_t * present,
+                           cudaStream_t st);
+// Plain-path pair gradients for centres [c0,c1): dCp[p - p_base][3][n][K]
+// (non-self pairs only; the self slot is left untouched).
+void launch_expansion_grad_fp64(const ExpansionArgs & a, int64_t c0, int64_t c1,
+                                int64_t p_base, double * dCp, cudaStream_t st);
+// Self-pair gradients: dCs[i - c0][S][3][n][K] = -sum_j (j not an image of i).
+void launch_expansion_selfgrad_fp64(const ExpansionArgs & a, int64_t c0, int64_t c1,
+                                    int64_t p_base, const double * dCp, double * dCs,
+                                    cudaStream_t st);
+
+struct PsArgs {
+  FeatureDims fd;
+  int64_t n_centers;
+  bool normalize;
+  const int32_t * row_of_center;  // output row for each centre (species-sorted)
+};
+// X rows (normalised) and inverse norms.
+void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double * inv_norm,
+                        cudaStream_t st);
+void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, float * norm,
+                        cudaStream_t st);
+// Plain-path gradients of the normalised power spectrum for pairs of centres
+// [c0,c1): dX[p - p_base][3][D].
+void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, int64_t c1,
+                         int64_t p_base, const double * C, const double * X,
+                         const double * inv_norm, const double * dCp, const double * dCs,
+                         double * dX, cudaStream_t st);
+// Adjoint: dE/dC[i][S][n][K] from dE/dX rows (species-sorted) for all centres.
+void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const float * X,
+                        const float * norm, const float * dX, float * dC, cudaStream_t st);
+
+// ------------------------------------------------------------------ GAP
+struct GapSpecies {
+  int64_t row0, rows;  // species segment in the sorted row order
+  int m0, M, Mpad;     // sparse points of this species (global index m0..m0+M)
+};
+// FP64 plain GEMMs: K = X T^T (per species), energies, W, t = W T.
+void gemm_nt_fp64(int64_t M, int64_t N, int64_t K, const double * A, int64_t lda,
+                  const double * B, int64_t ldb, double * C, int64_t ldc, cudaStream_t st);
+void gemm_nn_fp64(int64_t M, int64_t N, int64_t K, const double * A, int64_t lda,
+                  const double * B, int64_t ldb, double * C, int64_t ldc, cudaStream_t st);
+// k -> (e_row += alpha k^zeta, W = alpha zeta k^(zeta-1)) for FP64.
+void launch_gap_pointwise_fp64(int64_t rows, int M, const double * Kmat, int64_t ldk,
+                               const double * alpha, int zeta, double * W, int64_t ldw,
+                               double * e_row, cudaStream_t st);
+// TF32 tensor-core GEMM C = A B^T (both K-major) with optional GAP epilogue.
+struct Tf32GemmArgs {
+  int64_t M, N, K;  // rows of A, rows of B, reduction length (multiple of 32)
+  const float * A;
+  int64_t lda;
+  const float * B;
+  int64_t ldb;
+  float * C;  // plain store (epilogue 0) or W (epilogue 1)
+  int64_t ldc;
+  // GAP epilogue
+  int epilogue;          // 0: store C; 1: GAP forward
+  const float * alpha;   // [N]
+  int zeta;
+  float * e_part;        // [n_tiles_N][M] row partial energies
+};
+void gemm_tf32(const Tf32GemmArgs & g, cudaStream_t st);
+// energies[structure of centre(center_of_row[row0 + r])] += e(r), where e(r)
+// is e_row_fp64[r] or the sum of the n_parts FP32 partials e_part[t*ld + r].
+void launch_energy_reduce(int64_t rows, int n_parts, const float * e_part, int64_t ld,
+                          const double * e_row_fp64, int64_t row0, const int32_t * center_of_row,
+                          const int32_t * center_struct, double * energies, cudaStream_t st);
+
+// Plain force contraction: grad[j] += dX[p] . t_i for pairs of centres [c0,c1).
+void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, int64_t p_base,
+                                const int64_t * pair_off, const int32_t * pair_j,
+                                const int32_t * row_of_center, const double * dX,
+                                const double * t, int64_t ldt, double * grad, cudaStream_t st);
+// Adjoint pair kernel: forces from dE/dC (FP32) and recomputed dC/dr.
+void launch_pair_adjoint_fp32(const ExpansionArgs & a, const float * dC, double * forces,
+                              cudaStream_t st);
+
+// ------------------------------------------------------------------ helpers
+void launch_species_sort(int64_t n, const int32_t * types, const int32_t * center_atom,
+                         const int8_t * lut, int S, int64_t * species_count /*[S]*/,
+                         int32_t * row_of_center, int32_t * center_of_row, DevBuf & tmp,
+                         cudaStream_t st);
+void launch_round_tf32(float * x, int64_t n, cudaStream_t st);
+void launch_fill_f64(double * p, int64_t n, double v, cudaStream_t st);
+void launch_fill_f32(float * p, int64_t n, float v, cudaStream_t st);
+
+}  // namespace rgpu

@@ -1,0 +1,265 @@
+// Scans, the stable species sort of centres, fills and small utilities.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+
+#include "common.cuh"
+
+namespace rgpu {
+
+namespace {
+std::atomic<int64_t> g_launches{0};
+}
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launches(bool reset) {
+  return reset ? g_launches.exchange(0) : g_launches.load();
+}
+
+void cuda_check(cudaError_t e, const char * what) {
+  if (e != cudaSuccess) {
+    throw Error(RGPU_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e) + " in " + what);
+  }
+}
+
+void DevBuf::ensure(size_t bytes) {
+  if (bytes <= cap && p) return;
+  release();
+  size_t want = bytes < 256 ? 256 : bytes;
+  // grow geometrically so repeated calls with slowly growing sizes do not
+  // reallocate every time
+  if (want < cap * 5 / 4) want = cap * 5 / 4;
+  cuda_check(cudaMalloc(&p, want), "cudaMalloc");
+  cap = want;
+}
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+}
+
+SphConst make_sph_constants() {
+  SphConst h{};
+  const int S = kMaxL + 2;
+  for (int l = 0; l <= kMaxL; ++l) {
+    double lsq = double(l) * l, lm1sq = double(l - 1) * (l - 1);
+    for (int m = 0; m <= l; ++m) {
+      double msq = double(m) * m;
+      h.a[l * S + m] = std::sqrt((4 * lsq - 1.0) / (lsq - msq));
+      h.b[l * S + m] = -1.0 * std::sqrt((lm1sq - msq) / (4 * lm1sq - 1.0));
+      h.plm[l * S + m] = std::sqrt(double((l - m) * (l + m + 1)));
+    }
+    h.c1[l] = std::sqrt(2 * l + 1);
+    h.c2[l] = -std::sqrt(1.0 + 0.5 / l);
+  }
+  for (int i = 0; i < (kMaxL + 1) * S; ++i) {
+    h.af[i] = float(h.a[i]);
+    h.bf[i] = float(h.b[i]);
+    h.plmf[i] = float(h.plm[i]);
+  }
+  for (int l = 0; l <= kMaxL; ++l) {
+    h.c1f[l] = float(h.c1[l]);
+    h.c2f[l] = float(h.c2[l]);
+  }
+  return h;
+}
+
+namespace {
+
+constexpr int kScanBlock = 1024;
+
+template <typename Tin>
+__global__ void scan_block_kernel(const Tin * __restrict__ in, int64_t * __restrict__ out, int64_t n,
+                                  int64_t * __restrict__ block_sums) {
+  __shared__ int64_t warp_tot[32];
+  int64_t i = int64_t(blockIdx.x) * kScanBlock + threadIdx.x;
+  int64_t v = (i < n) ? int64_t(in[i]) : 0;
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int64_t t = warp_tot[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int64_t y = __shfl_up_sync(0xffffffffu, t, o);
+      if (lane >= o) t += y;
+    }
+    warp_tot[lane] = t;
+  }
+  __syncthreads();
+  int64_t excl = x - v + (wid > 0 ? warp_tot[wid - 1] : 0);
+  if (i < n) out[i] = excl;
+  if (threadIdx.x == kScanBlock - 1) block_sums[blockIdx.x] = excl + v;
+}
+
+__global__ void scan_add_kernel(int64_t * __restrict__ out, int64_t n,
+                                const int64_t * __restrict__ block_off) {
+  int64_t i = int64_t(blockIdx.x) * kScanBlock + threadIdx.x;
+  if (i < n) out[i] += block_off[blockIdx.x];
+}
+
+__global__ void scan_total_kernel(const int64_t * __restrict__ block_off, int nb,
+                                  int64_t * __restrict__ total) {
+  *total = block_off[nb];
+}
+
+template <typename Tin>
+void scan_impl(const Tin * in, int64_t * out, int64_t n, DevBuf & tmp, size_t tmp_off,
+               cudaStream_t st) {
+  int nb = div_up(n, kScanBlock);
+  if (nb == 0) {
+    cuda_check(cudaMemsetAsync(out, 0, sizeof(int64_t), st), "memset");
+    return;
+  }
+  int64_t * sums = reinterpret_cast<int64_t *>(static_cast<char *>(tmp.p) + tmp_off);
+  int64_t * sums_scan = sums + (nb + 1);
+  size_t used = tmp_off + sizeof(int64_t) * 2 * (nb + 1);
+  scan_block_kernel<Tin><<<nb, kScanBlock, 0, st>>>(in, out, n, sums);
+  RGPU_LAUNCHED();
+  if (nb == 1) {
+    // total = block sum
+    cuda_check(cudaMemcpyAsync(out + n, sums, sizeof(int64_t), cudaMemcpyDeviceToDevice, st), "copy");
+    return;
+  }
+  scan_impl<int64_t>(sums, sums_scan, nb, tmp, used, st);
+  scan_add_kernel<<<nb, kScanBlock, 0, st>>>(out, n, sums_scan);
+  RGPU_LAUNCHED();
+  scan_total_kernel<<<1, 1, 0, st>>>(sums_scan, nb, out + n);
+  RGPU_LAUNCHED();
+}
+
+size_t scan_tmp_bytes(int64_t n) {
+  size_t total = 0;
+  while (true) {
+    int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    total += sizeof(int64_t) * 2 * (nb + 1);
+    if (nb <= 1) break;
+    n = nb;
+  }
+  return total + 64;
+}
+
+// ---- stable counting sort of centres by species
+constexpr int kSortBlock = 1024;
+
+__global__ void species_count_kernel(int64_t n, const int32_t * __restrict__ types,
+                                     const int32_t * __restrict__ center_atom,
+                                     const int8_t * __restrict__ lut, int S,
+                                     int64_t * __restrict__ block_counts /*[S][nb]*/, int nb) {
+  __shared__ int cnt[32];
+  if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  int64_t i = int64_t(blockIdx.x) * kSortBlock + threadIdx.x;
+  if (i < n) atomicAdd(&cnt[lut[types[center_atom[i]]]], 1);
+  __syncthreads();
+  if (threadIdx.x < S) block_counts[int64_t(threadIdx.x) * nb + blockIdx.x] = cnt[threadIdx.x];
+}
+
+__global__ void species_rank_kernel(int64_t n, const int32_t * __restrict__ types,
+                                    const int32_t * __restrict__ center_atom,
+                                    const int8_t * __restrict__ lut, int S,
+                                    const int64_t * __restrict__ block_off /*[S][nb] scanned*/, int nb,
+                                    int32_t * __restrict__ row_of_center,
+                                    int32_t * __restrict__ center_of_row) {
+  __shared__ int wcnt[32][32];  // [warp][key]
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int k = lane; k < 32; k += 32) wcnt[wid][k] = 0;
+  __syncthreads();
+  int64_t i = int64_t(blockIdx.x) * kSortBlock + threadIdx.x;
+  int key = (i < n) ? lut[types[center_atom[i]]] : 31;
+  unsigned same = __match_any_sync(0xffffffffu, key);
+  int rank_w = __popc(same & lanemask_lt());
+  if ((same & lanemask_lt()) == 0) wcnt[wid][key] = __popc(same);
+  __syncthreads();
+  if (i < n) {
+    int before = 0;
+    for (int w = 0; w < wid; ++w) before += wcnt[w][key];
+    int64_t r = block_off[int64_t(key) * nb + blockIdx.x] + before + rank_w;
+    row_of_center[i] = int32_t(r);
+    center_of_row[r] = int32_t(i);
+  }
+}
+
+__global__ void species_total_kernel(const int64_t * __restrict__ counts, int S, int nb,
+                                     int64_t * __restrict__ out) {
+  int s = threadIdx.x;
+  if (s >= S) return;
+  int64_t t = 0;
+  for (int b = 0; b < nb; ++b) t += counts[int64_t(s) * nb + b];
+  out[s] = t;
+}
+
+__global__ void round_tf32_kernel(float * x, int64_t n) {
+  int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = to_tf32(x[i]);
+}
+__global__ void fill_f64_kernel(double * p, int64_t n, double v) {
+  int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+__global__ void fill_f32_kernel(float * p, int64_t n, float v) {
+  int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+}  // namespace
+
+void scan_exclusive_i64(const int64_t * in, int64_t * out, int64_t n, DevBuf & tmp, cudaStream_t st) {
+  tmp.ensure(scan_tmp_bytes(n));
+  scan_impl<int64_t>(in, out, n, tmp, 0, st);
+}
+void scan_exclusive_i32to64(const int32_t * in, int64_t * out, int64_t n, DevBuf & tmp,
+                            cudaStream_t st) {
+  tmp.ensure(scan_tmp_bytes(n));
+  scan_impl<int32_t>(in, out, n, tmp, 0, st);
+}
+
+void launch_species_sort(int64_t n, const int32_t * types, const int32_t * center_atom,
+                         const int8_t * lut, int S, int64_t * species_count, int32_t * row_of_center,
+                         int32_t * center_of_row, DevBuf & tmp, cudaStream_t st) {
+  int nb = div_up(n, kSortBlock);
+  if (nb == 0) {
+    cuda_check(cudaMemsetAsync(species_count, 0, sizeof(int64_t) * S, st), "memset");
+    return;
+  }
+  size_t cbytes = sizeof(int64_t) * (size_t(S) * nb + 1);
+  size_t stmp = scan_tmp_bytes(int64_t(S) * nb);
+  tmp.ensure(2 * cbytes + stmp + 256);
+  int64_t * counts = tmp.as<int64_t>();
+  int64_t * offs = counts + (size_t(S) * nb + 1);
+  species_count_kernel<<<nb, kSortBlock, 0, st>>>(n, types, center_atom, lut, S, counts, nb);
+  RGPU_LAUNCHED();
+  species_total_kernel<<<1, 32, 0, st>>>(counts, S, nb, species_count);
+  RGPU_LAUNCHED();
+  // scan of counts in key-major order gives each (key, block) its first row
+  scan_impl<int64_t>(counts, offs, int64_t(S) * nb, tmp, 2 * cbytes, st);
+  species_rank_kernel<<<nb, kSortBlock, 0, st>>>(n, types, center_atom, lut, S, offs, nb,
+                                                 row_of_center, center_of_row);
+  RGPU_LAUNCHED();
+}
+
+void launch_round_tf32(float * x, int64_t n, cudaStream_t st) {
+  if (n <= 0) return;
+  round_tf32_kernel<<<div_up(n, 256), 256, 0, st>>>(x, n);
+  RGPU_LAUNCHED();
+}
+void launch_fill_f64(double * p, int64_t n, double v, cudaStream_t st) {
+  if (n <= 0) return;
+  fill_f64_kernel<<<div_up(n, 256), 256, 0, st>>>(p, n, v);
+  RGPU_LAUNCHED();
+}
+void launch_fill_f32(float * p, int64_t n, float v, cudaStream_t st) {
+  if (n <= 0) return;
+  fill_f32_kernel<<<div_up(n, 256), 256, 0, st>>>(p, n, v);
+  RGPU_LAUNCHED();
+}
+
+}  // namespace rgpu

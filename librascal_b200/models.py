@@ -1,0 +1,292 @@
+"""Sparse GAP prediction on the B200 path.
+
+Mirrors bindings/rascal/models/{sparse_points.py, kernels.py, krr.py} for
+prediction: SparsePoints (the reference's SparsePointsBlockSparse,
+src/rascal/models/sparse_points.hh:50-448), Kernel (GAP, Sparse),
+KRR.predict / predict_forces (models/krr.py:92-166) and
+compute_sparse_kernel_gradients (bind_py_models.cc:148-200). Energies and
+forces of a whole AtomsList come from one rgpu_gap_predict call:
+
+  precision="fp64"  the reference's own algorithm on the GPU (materialised
+                    dX/dr contracted with the scaled sparse points), FP64;
+  precision="fp32"  the adjoint path: FP32 expansion, TF32 tensor-core GEMMs
+                    with FP32 accumulation, dE/dC contracted with dC/dr
+                    recomputed per pair; FP64 energy reduction.
+
+PyTorch is used only by GAPEnergy (a torch.autograd.Function around the
+adjoint path) and is imported lazily.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _native as N
+from .neighbourlist import AtomsList, StructureSet, frames_to_batch
+
+_PREC = {"fp64": N.PRECISION_FP64, "fp32": N.PRECISION_FP32}
+
+
+class SparsePoints:
+    """Selected environments (sparse points) with their dense features.
+
+    Rows are stored per key, as the reference stores `values[sp][key]`; the
+    dense matrix over a species layout is assembled on demand.
+    """
+
+    def __init__(self, representation):
+        self._representation = representation
+        self.species = []       # central species of each point
+        self.values = []        # dict key -> vector, per point
+
+    def size(self):
+        return len(self.species)
+
+    def __len__(self):
+        return self.size()
+
+    def extend(self, managers, selected_ids):
+        """Add the centres `selected_ids[i_structure]` of `managers`
+        (models/sparse_points.py extend, sparse_points.hh:360-417)."""
+        calc = self._representation
+        keys = managers.get_keys(calc)
+        X = managers.get_features(calc, keys=keys)
+        info = managers.get_representation_info()
+        inner = calc.inner_size()
+        row0 = 0
+        off = managers.batch["atom_offsets"]
+        mask = managers.batch.get("center_atoms_mask")
+        for i_struct, ids in enumerate(selected_ids):
+            if mask is not None:
+                n_c = int(np.sum(mask[off[i_struct]:off[i_struct + 1]]))
+            else:
+                n_c = int(off[i_struct + 1] - off[i_struct])
+            for i in ids:
+                if i >= n_c:
+                    raise RuntimeError("selected id %d out of range" % i)
+                r = row0 + int(i)
+                v = {}
+                for k, key in enumerate(keys):
+                    blk = X[r, k * inner:(k + 1) * inner]
+                    if np.any(blk != 0):
+                        v[(int(key[0]), int(key[1]))] = blk.copy()
+                self.values.append(v)
+                self.species.append(int(info[r, 2]))
+            row0 += n_c
+
+    def add_dense(self, species, T, keys):
+        """Add points from a dense matrix with the given key layout."""
+        inner = self._representation.inner_size()
+        for s, row in zip(species, np.asarray(T)):
+            v = {}
+            for k, key in enumerate(keys):
+                blk = row[k * inner:(k + 1) * inner]
+                if np.any(blk != 0):
+                    v[(int(key[0]), int(key[1]))] = np.array(blk, dtype=float)
+            self.values.append(v)
+            self.species.append(int(s))
+
+    def get_species(self):
+        sp = set(self.species)
+        for v in self.values:
+            for k in v:
+                sp.update(k)
+        return sorted(sp)
+
+    def dense(self, species):
+        """T [n_points x D] in the power-spectrum layout of `species`."""
+        species = sorted(species)
+        keys = self._representation.get_keys(species)
+        inner = self._representation.inner_size()
+        T = np.zeros((self.size(), len(keys) * inner))
+        kid = {(int(a), int(b)): i for i, (a, b) in enumerate(keys)}
+        for r, v in enumerate(self.values):
+            for key, blk in v.items():
+                T[r, kid[key] * inner:(kid[key] + 1) * inner] = blk
+        return T
+
+    def get_features(self):
+        return self.dense(self.get_species())
+
+
+class Kernel:
+    """GAP kernel description (models/kernels.py:16-164), Sparse only."""
+
+    def __init__(self, representation, name="GAP", kernel_type="Sparse", target_type="Structure", zeta=2,
+                 **kwargs):
+        if name != "GAP" or kernel_type != "Sparse":
+            raise NotImplementedError("only the sparse GAP kernel is on the B200 path")
+        self._representation = representation
+        self.name = name
+        self.kernel_type = kernel_type
+        self.target_type = target_type
+        self.zeta = int(zeta)
+
+    def __call__(self, X, Y=None, grad=(False, False)):
+        """K_NM between the structures of an AtomsList and sparse points
+        (models/sparse_kernels.hh:104-191), FP64 on the host from the GPU
+        features."""
+        if grad != (False, False):
+            raise NotImplementedError("kernel gradients: use KRR.predict_forces")
+        if not isinstance(Y, SparsePoints):
+            raise NotImplementedError("the sparse kernel needs SparsePoints as its second argument")
+        calc = self._representation
+        species = sorted(set(X.get_species()) | set(Y.get_species()))
+        keys = calc.get_keys(species)
+        feats = X.get_features(calc, keys=keys)
+        T = Y.dense(species)
+        info = X.get_representation_info()
+        k = (feats @ T.T)
+        same = info[:, 2][:, None] == np.asarray(Y.species)[None, :]
+        k = np.where(same, k ** self.zeta, 0.)
+        if self.target_type == "Atom":
+            return k
+        K = np.zeros((len(X), Y.size()))
+        np.add.at(K, info[:, 0], k)
+        return K
+
+
+class GAPModel:
+    """Device copy of a sparse GAP model (one rgpu_gap_model handle)."""
+
+    def __init__(self, representation, sparse_points, weights, zeta, self_contributions=None):
+        self.representation = representation
+        self.species = sparse_points.get_species()
+        T = N.f64(sparse_points.dense(self.species))
+        w = N.f64(np.asarray(weights).reshape(-1))
+        if len(w) != sparse_points.size():
+            raise ValueError("weights size mismatch {}!={}".format(len(w), sparse_points.size()))
+        sp = N.i32(self.species)
+        sps = N.i32(sparse_points.species)
+        sc = N.f64([(self_contributions or {}).get(s, 0.) for s in self.species])
+        h = ctypes.c_void_p()
+        N.check(N.lib().rgpu_gap_model_create(representation.handle, len(sp), N.ptr(sp, N.c_int_p), len(sps),
+                                              N.ptr(sps, N.c_int_p), N.ptr(T, N.c_dbl_p), N.ptr(w, N.c_dbl_p),
+                                              int(zeta), N.ptr(sc, N.c_dbl_p), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def predict(self, structures, precision="fp32", energies=True, forces=True):
+        """(energies per structure, forces N x 3) for a StructureSet."""
+        E = np.zeros(structures.n_structures) if energies else None
+        F = np.zeros((structures.n_atoms, 3)) if forces else None
+        N.check(N.lib().rgpu_gap_predict(self._h, structures.handle, _PREC[precision], N.ptr(E, N.c_dbl_p),
+                                         N.ptr(F, N.c_dbl_p)))
+        return E, F
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and N._lib is not None:
+            N._lib.rgpu_gap_model_destroy(h)
+            self._h = None
+
+
+class KRR:
+    """Sparse GAP model: predictions of energies and forces
+    (bindings/rascal/models/krr.py:12-166)."""
+
+    def __init__(self, weights, kernel, X_train, self_contributions, description="KRR potential model",
+                 units=None, precision="fp64"):
+        self.weights = np.asarray(weights, dtype=float)
+        self.kernel = kernel
+        self.X_train = X_train
+        self.self_contributions = self_contributions
+        self.target_type = kernel.target_type
+        self.description = description
+        self.units = dict(units or {})
+        self.units.setdefault("energy", "eV")
+        self.units.setdefault("length", "AA")
+        self.precision = precision
+        self._model = None
+
+    def _gap(self):
+        if self._model is None:
+            self._model = GAPModel(self.kernel._representation, self.X_train, self.weights.reshape(-1),
+                                   self.kernel.zeta, self.self_contributions)
+        return self._model
+
+    def _structures(self, managers):
+        if isinstance(managers, AtomsList):
+            return managers.structures
+        if isinstance(managers, StructureSet):
+            return managers
+        return StructureSet(frames_to_batch(managers))
+
+    def predict(self, managers, KNM=None):
+        if KNM is not None:
+            Y0 = self._baseline(managers)
+            return Y0 + np.dot(KNM, self.weights).reshape(-1)
+        if self.target_type != "Structure":
+            raise NotImplementedError("per-atom targets are not on the B200 path")
+        E, _ = self._gap().predict(self._structures(managers), self.precision, forces=False)
+        return E
+
+    def predict_forces(self, managers, KNM=None):
+        if self.kernel.kernel_type != "Sparse":
+            raise NotImplementedError("force prediction only implemented for kernels with kernel_type=='Sparse'")
+        if KNM is not None:
+            return -np.dot(KNM, self.weights).reshape((-1, 3))
+        _, F = self._gap().predict(self._structures(managers), self.precision, energies=False)
+        return F
+
+    def predict_energy_forces(self, managers):
+        return self._gap().predict(self._structures(managers), self.precision)
+
+    def _baseline(self, managers):
+        st = self._structures(managers)
+        b = st.batch
+        Y0 = np.zeros(st.n_structures)
+        for i in range(st.n_structures):
+            for z in b["numbers"][b["atom_offsets"][i]:b["atom_offsets"][i + 1]]:
+                Y0[i] += self.self_contributions.get(int(z), 0.)
+        return Y0
+
+
+def compute_sparse_kernel_gradients(representation, kernel, managers, sparse_points, weights,
+                                    precision="fp64"):
+    """Gradients of the GAP energy w.r.t. positions, N_atoms x 3
+    (models/sparse_kernel_predict.hh:206-266)."""
+    model = GAPModel(representation, sparse_points, np.asarray(weights).reshape(-1), kernel.zeta)
+    st = managers.structures if isinstance(managers, AtomsList) else managers
+    _, F = model.predict(st, precision, energies=False)
+    return -F
+
+
+def gap_energy(positions, model, structures):
+    """Energies of `structures` at `positions` (torch tensor, N x 3) through
+    the adjoint path; differentiable w.r.t. positions."""
+    return _gap_function().apply(positions, model, structures)
+
+
+_GAPFn = None
+
+
+def _gap_function():
+    global _GAPFn
+    if _GAPFn is None:
+        import torch
+
+        class GAPEnergy(torch.autograd.Function):
+            """E(r) forward; dE/dr from the adjoint kernels (no stored dX/dr)."""
+
+            @staticmethod
+            def forward(ctx, positions, model, structures):
+                pos = positions.detach().to("cpu", torch.float64).numpy()
+                structures.update_positions(pos)
+                E, F = model.predict(structures, "fp32")
+                b = structures.batch
+                sidx = np.repeat(np.arange(structures.n_structures), np.diff(b["atom_offsets"]))
+                ctx.save_for_backward(torch.from_numpy(F).to(positions.device),
+                                      torch.from_numpy(sidx).to(positions.device))
+                return torch.from_numpy(E).to(positions.device, positions.dtype)
+
+            @staticmethod
+            def backward(ctx, gE):
+                F, sidx = ctx.saved_tensors
+                g = -(F * gE.to(F.dtype)[sidx][:, None])
+                return g, None, None
+
+        _GAPFn = GAPEnergy
+    return _GAPFn

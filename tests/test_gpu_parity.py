@@ -1,0 +1,289 @@
+"""GPU parity against the CPU oracle, through the C ABI.
+
+Bars (BASELINE / north_star):
+  * neighbour list: identical pairs, order, shifts, distances and directions
+    (bit-exact; the oracle fixes the FP association, no FMA);
+  * plain FP64 features and gradients: <= 1e-10 in the reference's
+    relative_error convention (math/utils.hh:152-225);
+  * plain FP64 GAP energies/forces: <= 1e-10 relative;
+  * fast FP32/TF32 adjoint forces: max|F - F_ref| / max|F_ref| <= 1e-4.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import librascal_b200 as rb
+from helpers import GOLDEN, batch_from_frames, load_structures, relative_error, wrap
+from librascal_b200 import synthetic
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def soap(rc=3.5, sw=0.5, n=4, l=3, sigma=0.4, spline=True, grads=False, normalize=True):
+    opt = dict(Spline=dict(accuracy=1e-8)) if spline else {}
+    return rb.SphericalInvariants(interaction_cutoff=rc, cutoff_smooth_width=sw, max_radial=n,
+                                  max_angular=l, gaussian_sigma_type="Constant",
+                                  gaussian_sigma_constant=sigma, optimization=opt,
+                                  compute_gradients=grads, normalize=normalize)
+
+
+def oracle_calc(rc=3.5, sw=0.5, n=4, l=3, sigma=0.4, spline=True, normalize=True):
+    return O.Calculator(rc, sw, n, l, sigma, spline=spline, normalize=normalize,
+                        accuracy=1e-8 if spline else 1e-8)
+
+
+def subset(batch, idx):
+    off = batch["atom_offsets"]
+    parts = dict(positions=[], numbers=[], cells=[], pbc=[])
+    new_off = [0]
+    for i in idx:
+        a0, a1 = off[i], off[i + 1]
+        parts["positions"].append(batch["positions"][a0:a1])
+        parts["numbers"].append(batch["numbers"][a0:a1])
+        parts["cells"].append(batch["cells"][i])
+        parts["pbc"].append(batch["pbc"][i])
+        new_off.append(new_off[-1] + a1 - a0)
+    return dict(atom_offsets=np.asarray(new_off, np.int64), positions=np.concatenate(parts["positions"]),
+                numbers=np.concatenate(parts["numbers"]), cells=np.asarray(parts["cells"]),
+                pbc=np.asarray(parts["pbc"]))
+
+
+def nl_cases():
+    structs = load_structures()
+    cases = []
+    for name, rcs in [("CaCrP2O7_mvc-11955_symmetrized.json", [2.0, 3.0, 5.5]),
+                      ("small_molecule.json", [2.0, 3.5]),
+                      ("simple_cubic_8.json", [1.0, 2.5]),
+                      ("linked_cell_break_0.json", [3.0]),
+                      ("diamond_cubic_distorted.json", [5.0]),
+                      ("SiC_moissanite.json", [4.0]),
+                      ("methane.json", [3.0])]:
+        if name in structs:
+            for rc in rcs:
+                cases.append((name, batch_from_frames(structs[name]), rc))
+    cases.append(("periodic_boxes", synthetic.periodic_boxes(n_struct=4), 4.0))
+    cases.append(("triclinic_cells", subset(synthetic.triclinic_cells(n_struct=8), range(8)), 5.0))
+    cases.append(("molecule_clusters", synthetic.molecule_clusters(n_struct=64), 5.0))
+    return cases
+
+
+@pytest.mark.parametrize("case", nl_cases(), ids=lambda c: "%s-rc%s" % (c[0], c[2]))
+def test_neighbour_list_bit_exact(case):
+    name, batch, rc = case
+    st = rb.StructureSet(batch)
+    st.build_neighbour_list(rc)
+    g = st.neighbour_list()
+    species = np.unique(batch["numbers"])
+    r = O.Run(oracle_calc(rc=rc), batch, species)
+    ca, cs, po = r.centers()
+    p = r.pairs()
+    assert np.array_equal(g["center_atom"], ca)
+    assert np.array_equal(g["pair_offsets"], po)
+    assert np.array_equal(g["j"], p["j"])
+    assert np.array_equal(g["shift"], p["shift"])
+    assert np.array_equal(g["distance"], p["distance"])  # bitwise
+    assert np.array_equal(g["direction"], p["direction"])
+
+
+def test_neighbour_list_center_mask():
+    structs = load_structures()
+    frames = [dict(f) for f in structs["CaCrP2O7_mvc-11955_symmetrized.json"]]
+    n = len(frames[0]["numbers"])
+    frames[0]["center_atoms_mask"] = [i % 3 != 1 for i in range(n)]
+    batch = batch_from_frames(frames)
+    st = rb.StructureSet(batch)
+    st.build_neighbour_list(3.0)
+    g = st.neighbour_list()
+    r = O.Run(oracle_calc(rc=3.0), batch, np.unique(batch["numbers"]))
+    ca, cs, po = r.centers()
+    p = r.pairs()
+    assert np.array_equal(g["center_atom"], ca)
+    assert np.array_equal(g["j"], p["j"]) and np.array_equal(g["distance"], p["distance"])
+
+
+def test_rc_epsilon_edge_case():
+    # Twelve atoms, six at distance rc and six at rc - 2 eps from the
+    # centre; pairs exactly at rc are kept (d^2 <= rc^2).
+    rc, eps = 3.0, 1e-6
+    pos = [[0, 0, 0]]
+    for k, d in enumerate([rc] * 3 + [rc - 2 * eps] * 3):
+        v = np.zeros(3)
+        v[k % 3] = d if k < 3 else -d
+        pos.append(v)
+    pos = np.asarray(pos, float) + 10.0
+    batch = batch_from_frames([dict(positions=pos, numbers=[1] * len(pos), cell=np.eye(3) * 20.,
+                                    pbc=[False] * 3)])
+    st = rb.StructureSet(batch)
+    st.build_neighbour_list(rc)
+    g = st.neighbour_list()
+    r = O.Run(oracle_calc(rc=rc), batch, [1])
+    assert np.array_equal(g["j"], r.pairs()["j"])
+    assert g["pair_offsets"][1] - g["pair_offsets"][0] == 1 + 6
+
+
+def test_invalid_structures_raise():
+    good = dict(positions=[[1., 1., 1.], [2., 1., 1.]], numbers=[1, 1], cell=np.eye(3) * 5., pbc=[True] * 3)
+    bad = dict(good, positions=[[1., 1., 1.], [6., 1., 1.]])
+    with pytest.raises(RuntimeError, match="inside the unit cell"):
+        st = rb.StructureSet(batch_from_frames([good, bad]))
+        st.build_neighbour_list(3.0)
+    zero = dict(good, cell=np.zeros((3, 3)))
+    with pytest.raises(RuntimeError, match="filled with zeros"):
+        st = rb.StructureSet(batch_from_frames([zero]))
+        st.build_neighbour_list(3.0)
+    badz = dict(good, numbers=[1, 200])
+    with pytest.raises(RuntimeError, match="range"):
+        rb.StructureSet(batch_from_frames([badz]))
+
+
+def features_vs_oracle(batch, calc_kwargs, species=None):
+    calc = soap(**calc_kwargs)
+    al = calc.transform(rb.AtomsList(rb.StructureSet(batch)))
+    species = np.unique(batch["numbers"]) if species is None else species
+    keys = calc.get_keys(species)
+    X = al.get_features(calc, keys=keys)
+    oc = oracle_calc(**{k: v for k, v in calc_kwargs.items() if k != "grads"})
+    r = O.Run(oc, batch, species)
+    return X, r.power_spectrum(), al, calc, r
+
+
+@pytest.mark.parametrize("which", ["periodic_boxes", "molecule_clusters", "CaCrP2O7"])
+def test_powerspectrum_fp64_parity(which):
+    if which == "periodic_boxes":
+        batch, kw = synthetic.periodic_boxes(n_struct=4), dict(rc=4.0, n=6, l=4, sigma=0.3)
+    elif which == "molecule_clusters":
+        batch, kw = synthetic.molecule_clusters(n_struct=40), dict(rc=5.0, n=8, l=6, sigma=0.4)
+    else:
+        batch = batch_from_frames(load_structures()["CaCrP2O7_mvc-11955_symmetrized.json"])
+        kw = dict(rc=5.0, n=6, l=5, sigma=0.3)
+    X, Xo, *_ = features_vs_oracle(batch, kw)
+    assert X.shape == Xo.shape
+    assert relative_error(Xo, X).max() <= 1e-10
+
+
+def test_expansion_golden_on_gpu():
+    z = np.load(os.path.join(GOLDEN, "expansion_reference.npz"))
+    meta = json.loads(str(z["meta"]))
+    structs = load_structures()
+    for i, m in enumerate(meta):
+        batch = batch_from_frames(structs[m["structure"]])
+        opt = dict(Spline=dict(accuracy=m["accuracy"])) if m["spline"] else {}
+        calc = rb.SphericalExpansion(interaction_cutoff=m["cutoff"], cutoff_smooth_width=m["smooth_width"],
+                                     max_radial=m["max_radial"], max_angular=m["max_angular"],
+                                     gaussian_sigma_type="Constant", gaussian_sigma_constant=m["sigma"],
+                                     optimization=opt)
+        al = calc.transform(rb.AtomsList(rb.StructureSet(batch)))
+        C = al.get_features(calc, keys=calc.get_keys(np.unique(batch["numbers"])))
+        ref = z["features_%d" % i]
+        assert relative_error(ref, C, 1e-14).max() < 3e-6  # tests/test_calculator.cc:460-496
+
+
+def test_kernel_golden_on_gpu():
+    z = np.load(os.path.join(GOLDEN, "kernel_reference.npz"))
+    meta = json.loads(str(z["meta"]))
+    batch = batch_from_frames(load_structures()[str(z["structures"])])
+    S = len(batch["atom_offsets"]) - 1
+    for i, m in enumerate(meta):
+        calc = soap(rc=m["cutoff"], sw=m["smooth_width"], n=m["max_radial"], l=m["max_angular"],
+                    sigma=m["sigma"], spline=m["spline"], normalize=m["normalize"])
+        al = calc.transform(rb.AtomsList(rb.StructureSet(batch)))
+        X = al.get_features(calc, keys=calc.get_keys(np.unique(batch["numbers"])))
+        info = al.get_representation_info()
+        kk = (X @ X.T) ** m["zeta"]
+        if m["target_type"] == "Structure":
+            K = np.array([[kk[np.ix_(info[:, 0] == a, info[:, 0] == c)].mean() for c in range(S)]
+                          for a in range(S)])
+        else:
+            K = kk
+        assert relative_error(z["kernel_%d" % i], K).max() < 1e-10  # tests/test_kernels.cc:68-136
+
+
+def test_powerspectrum_gradient_fp64_parity():
+    batch = synthetic.molecule_clusters(n_struct=6, seed=3)
+    kw = dict(rc=5.0, n=4, l=3, sigma=0.4)
+    calc = soap(grads=True, **kw)
+    al = calc.transform(rb.AtomsList(rb.StructureSet(batch)))
+    species = np.unique(batch["numbers"])
+    keys = calc.get_keys(species)
+    dX = al.get_features_gradient(calc, keys=keys)
+    r = O.Run(oracle_calc(**kw), batch, species, gradients=True)
+    ref = r.power_spectrum_gradient().reshape(dX.shape)
+    scale = np.abs(ref).max()
+    assert np.abs(dX - ref).max() <= 1e-10 * scale
+    info = al.get_gradients_info()
+    assert info.shape == (r.n_pairs, 5)
+
+
+def gap_setup(batch, kw, n_sparse=6, seed=0, zeta=2):
+    species = np.unique(batch["numbers"])
+    oc = oracle_calc(**kw)
+    r = O.Run(oc, batch, species, gradients=True)
+    X = r.power_spectrum()
+    ca, _, _ = r.centers()
+    sp_row = batch["numbers"][ca]
+    idx = synthetic.select_sparse_points(X, sp_row, n_sparse, seed=seed)
+    rng = np.random.default_rng(seed)
+    alpha = rng.normal(size=len(idx))
+    return r, X[idx], sp_row[idx], alpha, species
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_gap_energy_forces_parity(precision):
+    batch = synthetic.molecule_clusters(n_struct=12, seed=5)
+    kw = dict(rc=5.0, n=8, l=6, sigma=0.4)
+    r, T, sps, alpha, species = gap_setup(batch, kw, n_sparse=8)
+    E_ref, F_ref = r.gap(sps, T, alpha, 2)
+    calc = soap(**kw)
+    sp = rb.SparsePoints(calc)
+    sp.add_dense(sps, T, calc.get_keys(species))
+    model = rb.GAPModel(calc, sp, alpha, 2)
+    st = rb.StructureSet(batch)
+    E, F = model.predict(st, precision)
+    if precision == "fp64":
+        assert np.abs(E - E_ref).max() <= 1e-10 * np.abs(E_ref).max()
+        assert np.abs(F - F_ref).max() <= 1e-10 * np.abs(F_ref).max()
+    else:
+        assert np.abs(E - E_ref).max() <= 1e-5 * np.abs(E_ref).max()
+        assert np.abs(F - F_ref).max() <= 1e-4 * np.abs(F_ref).max()
+
+
+def test_gap_forces_periodic_and_fd():
+    batch = synthetic.periodic_boxes(n_struct=2, seed=2)
+    kw = dict(rc=4.0, n=6, l=4, sigma=0.3)
+    r, T, sps, alpha, species = gap_setup(batch, kw, n_sparse=5)
+    E_ref, F_ref = r.gap(sps, T, alpha, 2)
+    calc = soap(**kw)
+    sp = rb.SparsePoints(calc)
+    sp.add_dense(sps, T, calc.get_keys(species))
+    model = rb.GAPModel(calc, sp, alpha, 2)
+    st = rb.StructureSet(batch)
+    for prec, tol in [("fp64", 1e-10), ("fp32", 1e-4)]:
+        E, F = model.predict(st, prec)
+        assert np.abs(F - F_ref).max() <= tol * np.abs(F_ref).max(), prec
+    # central finite differences of the GPU FP64 energy (h = 1e-4 A)
+    h = 1e-4
+    rng = np.random.default_rng(0)
+    for a in rng.choice(batch["atom_offsets"][-1], 4, replace=False):
+        for c in range(3):
+            ep = []
+            for sgn in (1, -1):
+                b2 = dict(batch)
+                b2["positions"] = batch["positions"].copy()
+                b2["positions"][a, c] += sgn * h
+                b2 = wrap(b2)
+                st2 = rb.StructureSet(b2)
+                ep.append(model.predict(st2, "fp64", forces=False)[0].sum())
+            fd = -(ep[0] - ep[1]) / (2 * h)
+            assert abs(fd - F_ref[a, c]) <= 1e-6 * max(1.0, np.abs(F_ref).max())
+
+
+def test_empty_and_isolated_atoms():
+    frames = [dict(positions=[[5., 5., 5.]], numbers=[1], cell=np.eye(3) * 10., pbc=[False] * 3),
+              dict(positions=[[1., 1., 1.], [9., 9., 9.]], numbers=[8, 1], cell=np.eye(3) * 10.,
+                   pbc=[False] * 3)]
+    batch = batch_from_frames(frames)
+    X, Xo, *_ = features_vs_oracle(batch, dict(rc=3.0, n=4, l=3, sigma=0.4))
+    assert relative_error(Xo, X).max() <= 1e-10
