@@ -363,10 +363,11 @@ def main():
                         stage_ms=dict(zip(["total", "neighbour_list", "expansion", "power_spectrum",
                                            "gemm_fwd", "gemm_bwd", "ps_backward", "pair_adjoint"],
                                           [round(float(x), 4) for x in stages]))),
-            roofline=dict(bound="tensor", kernel="TF32 tensor-core GEMMs (forward + backward)",
+            roofline=dict(bound="tensor", kernel="tcgen05 BF16x3 GEMMs (forward + backward)",
                           achieved=achieved, peak=bf16_peak, unit="TFLOP/s",
                           frac=(achieved / bf16_peak) if achieved else None, traffic=None,
-                          peak_kind="%s dense bf16 (TF32 issues at half that rate)" % peak_kind,
+                          peak_kind="%s dense bf16; achieved counts algorithmic 2MNK flops, the "
+                                    "3-term split issues 3x that on the tensor pipe" % peak_kind,
                           flops_per_step=gemm_flops),
             cpu_baseline=cpu, e2e=e2e, gpu_launches=launches, clocks=clk.summary())
         print(json.dumps(line), flush=True)

@@ -225,6 +225,20 @@ int64_t rgpu_kernel_launches(int reset);
 rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out,
                              int32_t n_stages);
 
+/* ---------------------------------------------------------------------- */
+/* Unit-test hook for the tensor-core GEMM (no reference counterpart; the
+ * reference computes these contractions as per-centre GEMVs,
+ * models/sparse_kernels.hh:104-131 and sparse_kernel_predict.hh:130-172).
+ * DEVICE pointers, row-major FP32: A [M x K], B [N x K]. mode 0: C = A B^T
+ * [M x N]; mode 1: the GAP forward epilogue with alpha [N] and zeta,
+ * C = alpha zeta (A B^T)^(zeta-1) [M x N] (read back from its BF16 split) and
+ * e [M] = sum_n alpha_n (A B^T)^zeta. `stream` is a cudaStream_t or NULL. */
+rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K,
+                                   const float * A_dev, const float * B_dev,
+                                   const float * alpha_dev, int32_t zeta,
+                                   float * C_dev, float * e_dev,
+                                   void * stream);
+
 #ifdef __cplusplus
 }
 #endif

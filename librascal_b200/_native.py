@@ -62,6 +62,9 @@ SIGNATURES = {
     "rgpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "rgpu_kernel_launches": (ctypes.c_int64, [ctypes.c_int]),
     "rgpu_stage_times": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p, ctypes.c_int32]),
+    "rgpu_debug_gemm_bf16x3": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 _lib = None

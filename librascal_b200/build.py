@@ -23,15 +23,18 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # compiled without FMA contraction so their FP64 results are reproducible
 # bit for bit against the CPU restatement.
 SOURCES = [
-    ("nl.cu", ["--fmad=false"]),
-    ("util.cu", []),
-    ("expansion.cu", []),
-    ("powerspectrum.cu", []),
-    ("gemm.cu", []),
-    ("adjoint.cu", []),
-    ("api.cu", []),
-    ("radial_gto.cpp", ["-Xcompiler", "-ffp-contract=off"]),
-    ("json_lite.cpp", []),
+    ("nl.cu", ["--fmad=false"], "nl"),
+    ("util.cu", [], "util"),
+    ("expansion.cu", ["--fmad=false", "-DRGPU_PART_FP64"], "expansion_f64"),
+    ("expansion.cu", ["-DRGPU_PART_FP32"], "expansion_f32"),
+    ("powerspectrum.cu", ["--fmad=false", "-DRGPU_PART_FP64"], "powerspectrum_f64"),
+    ("powerspectrum.cu", ["-DRGPU_PART_FP32"], "powerspectrum_f32"),
+    ("gemm.cu", [], "gemm"),
+    ("gemm_tc.cu", [], "gemm_tc"),
+    ("adjoint.cu", [], "adjoint"),
+    ("api.cu", [], "api"),
+    ("radial_gto.cpp", ["-Xcompiler", "-ffp-contract=off"], "radial_gto"),
+    ("json_lite.cpp", [], "json_lite"),
 ]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "--extended-lambda", "-I" + SRC, "-I" + os.path.join(os.path.dirname(HERE), "include")]
@@ -48,9 +51,9 @@ def build(verbose=False, jobs=None):
     os.makedirs(OBJ, exist_ok=True)
     newest_header = max(os.path.getmtime(h) for h in _headers())
     procs, objs = [], []
-    for src, flags in SOURCES:
+    for src, flags, name in SOURCES:
         s = os.path.join(SRC, src)
-        o = os.path.join(OBJ, src + ".o")
+        o = os.path.join(OBJ, name + ".o")
         objs.append(o)
         if os.path.exists(o) and os.path.getmtime(o) >= max(os.path.getmtime(s), newest_header):
             continue

@@ -180,7 +180,8 @@ struct rgpu_structures {
   bool feat_gradients{false};
   bool feat_valid{false};
   // GAP work
-  DevBuf E_d, F_d, K64, t64, erow64, W32, dX32, dC32, epart;
+  DevBuf E_d, F_d, K64, t64, erow64, Wh, Wl, dX32, dC32, epart, Xh, Xl;
+  bool feat_x32{false};  // FP32 features also kept unsplit (for export)
   DevBuf dCp, dCs, dXp;
   // status and timing
   DevStatus * status_d{nullptr};
@@ -203,7 +204,7 @@ struct rgpu_gap_model {
   std::vector<int> layout_species;
   int layout_D{0};
   std::vector<GapSpecies> segs;  // per batch species
-  DevBuf T64, alpha64, T32, Tt32, alpha32;
+  DevBuf T64, alpha64, Th, Tl, Tth, Ttl, alpha32;
   std::vector<int64_t> tt_off;  // per batch species offset into Tt32
 };
 
@@ -333,10 +334,11 @@ void sort_rows(rgpu_structures * s) {
 }
 
 void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, bool grads,
-                      const std::vector<int> & extra_species) {
+                      const std::vector<int> & extra_species, bool need_x32 = true) {
   build_nl(s, c->hy.cutoff);
   set_layout(s, c->hy, extra_species);
-  if (s->feat_valid && s->feat_calc == c && s->feat_precision == precision) {
+  if (s->feat_valid && s->feat_calc == c && s->feat_precision == precision &&
+      (precision == RGPU_PRECISION_FP64 || s->feat_x32 || !need_x32)) {
     s->feat_gradients = s->feat_gradients || grads;
     return;
   }
@@ -365,10 +367,14 @@ void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, b
     launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), s->st);
     mark(s, 3);
     if (c->hy.kind == "sphericalinvariants") {
-      s->X32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
+      if (need_x32) s->X32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
+      s->Xh.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dpad + 64);
+      s->Xl.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dpad + 64);
       s->norm32.ensure(sizeof(float) * (nc + 1));
-      launch_ps_fwd_fp32(pa, s->C32.as<float>(), s->X32.as<float>(), s->norm32.as<float>(), s->st);
+      launch_ps_fwd_fp32(pa, s->C32.as<float>(), need_x32 ? s->X32.as<float>() : nullptr,
+                         s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(), s->norm32.as<float>(), s->st);
     }
+    s->feat_x32 = need_x32;
   }
   s->feat_valid = true;
   s->feat_calc = c;
@@ -465,21 +471,46 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
       ++pos;
     }
   }
-  std::vector<float> T32(T.size()), al32(al.size());
-  for (size_t i = 0; i < T.size(); ++i) T32[i] = float(T[i]);
+  // BF16 hi/lo splits of T (rows = sparse points) and of T^T per species
+  // (rows = feature index, padded to Mpad columns) for the tensor-core GEMMs
+  auto f2bf = [](float f) -> uint16_t {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return 0x7fc0;
+    return uint16_t((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
+  };
+  auto bf2f = [](uint16_t h) -> float {
+    uint32_t u = uint32_t(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+  };
+  std::vector<uint16_t> Th(T.size()), Tl(T.size());
+  for (size_t i = 0; i < T.size(); ++i) {
+    const float v = float(T[i]);
+    Th[i] = f2bf(v);
+    Tl[i] = f2bf(v - bf2f(Th[i]));
+  }
+  std::vector<float> al32(al.size());
   for (size_t i = 0; i < al.size(); ++i) al32[i] = float(al[i]);
-  std::vector<float> Tt(size_t(std::max<int64_t>(tt_total, 1)), 0.f);
+  std::vector<uint16_t> Tth(size_t(std::max<int64_t>(tt_total, 1)), 0), Ttl(Tth.size(), 0);
   for (int sI = 0; sI < fd.S; ++sI) {
     const GapSpecies & g = m->segs[sI];
-    float * dst = &Tt[m->tt_off[sI]];
     for (int mm = 0; mm < g.M; ++mm)
-      for (int d = 0; d < fd.D; ++d) dst[size_t(d) * g.Mpad + mm] = T32[size_t(g.m0 + mm) * fd.Dpad + d];
+      for (int d = 0; d < fd.D; ++d) {
+        const size_t src = size_t(g.m0 + mm) * fd.Dpad + d;
+        const size_t dst = size_t(m->tt_off[sI]) + size_t(d) * g.Mpad + mm;
+        Tth[dst] = Th[src];
+        Ttl[dst] = Tl[src];
+      }
   }
   upload(s, m->T64, T.data(), sizeof(double) * T.size());
   upload(s, m->alpha64, al.data(), sizeof(double) * al.size());
-  upload(s, m->T32, T32.data(), sizeof(float) * T32.size());
+  upload(s, m->Th, Th.data(), sizeof(uint16_t) * Th.size());
+  upload(s, m->Tl, Tl.data(), sizeof(uint16_t) * Tl.size());
   upload(s, m->alpha32, al32.data(), sizeof(float) * al32.size());
-  upload(s, m->Tt32, Tt.data(), sizeof(float) * Tt.size());
+  upload(s, m->Tth, Tth.data(), sizeof(uint16_t) * Tth.size());
+  upload(s, m->Ttl, Ttl.data(), sizeof(uint16_t) * Ttl.size());
   RGPU_CUDA(cudaStreamSynchronize(s->st));
   m->layout_species = s->species;
   m->layout_D = fd.D;
@@ -569,15 +600,20 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
   const int64_t nc = s->nl.n_centers;
   cudaStream_t st = s->st;
   mark(s, 4);
-  // per-species W and energy partial buffers
+  // per-species W (BF16 hi/lo) and energy partial buffers
   int64_t wtot = 0, eparts = 0;
   for (int sI = 0; sI < fd.S; ++sI) {
     wtot += s->species_count[sI] * m->segs[sI].Mpad;
-    eparts = std::max<int64_t>(eparts, s->species_count[sI] * ((m->segs[sI].M + 127) / 128));
+    eparts = std::max<int64_t>(eparts, s->species_count[sI] * ((m->segs[sI].M + kTcTileN - 1) / kTcTileN));
   }
-  s->W32.ensure(sizeof(float) * size_t(std::max<int64_t>(wtot, 1)) + 64);
+  s->Wh.ensure(sizeof(uint16_t) * size_t(std::max<int64_t>(wtot, 1)) + 64);
+  s->Wl.ensure(sizeof(uint16_t) * size_t(std::max<int64_t>(wtot, 1)) + 64);
   s->epart.ensure(sizeof(float) * size_t(std::max<int64_t>(eparts, 1)) + 64);
   s->dX32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
+  const __nv_bfloat16 * Xh = s->Xh.as<__nv_bfloat16>();
+  const __nv_bfloat16 * Xl = s->Xl.as<__nv_bfloat16>();
+  __nv_bfloat16 * Wh = s->Wh.as<__nv_bfloat16>();
+  __nv_bfloat16 * Wl = s->Wl.as<__nv_bfloat16>();
   int64_t row0 = 0, woff = 0;
   std::vector<int64_t> wofs(fd.S);
   for (int sI = 0; sI < fd.S; ++sI) {
@@ -585,22 +621,25 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
     const GapSpecies & g = m->segs[sI];
     wofs[sI] = woff;
     if (rows > 0 && g.M > 0) {
-      Tf32GemmArgs a{};
+      Bf16x3Gemm a{};
       a.M = rows;
       a.N = g.M;
       a.K = fd.Dpad;
-      a.A = s->X32.as<float>() + size_t(row0) * fd.Dpad;
+      a.A_hi = Xh + size_t(row0) * fd.Dpad;
+      a.A_lo = Xl + size_t(row0) * fd.Dpad;
       a.lda = fd.Dpad;
-      a.B = m->T32.as<float>() + size_t(g.m0) * fd.Dpad;
+      a.B_hi = m->Th.as<__nv_bfloat16>() + size_t(g.m0) * fd.Dpad;
+      a.B_lo = m->Tl.as<__nv_bfloat16>() + size_t(g.m0) * fd.Dpad;
       a.ldb = fd.Dpad;
-      a.C = s->W32.as<float>() + woff;
-      a.ldc = g.Mpad;
       a.epilogue = 1;
+      a.W_hi = Wh + woff;
+      a.W_lo = Wl + woff;
+      a.ldw = g.Mpad;
       a.alpha = m->alpha32.as<float>() + g.m0;
       a.zeta = m->zeta;
       a.e_part = s->epart.as<float>();
-      gemm_tf32(a, st);
-      const int nparts = (g.M + 127) / 128;
+      gemm_bf16x3(a, st);
+      const int nparts = (g.M + kTcTileN - 1) / kTcTileN;
       launch_energy_reduce(rows, nparts, s->epart.as<float>(), rows, nullptr, row0,
                            s->center_of_row.as<int32_t>(), s->nl.center_struct, E_d, st);
     }
@@ -614,18 +653,20 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
     const int64_t rows = s->species_count[sI];
     const GapSpecies & g = m->segs[sI];
     if (rows > 0 && g.M > 0) {
-      Tf32GemmArgs a{};
+      Bf16x3Gemm a{};
       a.M = rows;
       a.N = fd.Dpad;
       a.K = g.Mpad;
-      a.A = s->W32.as<float>() + wofs[sI];
+      a.A_hi = Wh + wofs[sI];
+      a.A_lo = Wl + wofs[sI];
       a.lda = g.Mpad;
-      a.B = m->Tt32.as<float>() + m->tt_off[sI];
+      a.B_hi = m->Tth.as<__nv_bfloat16>() + m->tt_off[sI];
+      a.B_lo = m->Ttl.as<__nv_bfloat16>() + m->tt_off[sI];
       a.ldb = g.Mpad;
+      a.epilogue = 0;
       a.C = s->dX32.as<float>() + size_t(row0) * fd.Dpad;
       a.ldc = fd.Dpad;
-      a.epilogue = 0;
-      gemm_tf32(a, st);
+      gemm_bf16x3(a, st);
     } else if (rows > 0) {
       launch_fill_f32(s->dX32.as<float>() + size_t(row0) * fd.Dpad, rows * fd.Dpad, 0.f, st);
     }
@@ -638,8 +679,8 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
   pa.normalize = c->hy.normalize;
   pa.row_of_center = s->row_of_center.as<int32_t>();
   s->dC32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.nK + 64);
-  launch_ps_bwd_fp32(pa, s->C32.as<float>(), s->X32.as<float>(), s->norm32.as<float>(),
-                     s->dX32.as<float>(), s->dC32.as<float>(), st);
+  launch_ps_bwd_fp32(pa, s->C32.as<float>(), Xh, Xl, s->norm32.as<float>(), s->dX32.as<float>(),
+                     s->dC32.as<float>(), st);
   mark(s, 7);
   ExpansionArgs ea = exp_args(c, s);
   launch_pair_adjoint_fp32(ea, s->dC32.as<float>(), F_d, st);
@@ -1040,7 +1081,7 @@ rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precis
     // neighbour list, layout, features
     build_nl(s, m->calc->hy.cutoff);
     mark(s, 1);
-    compute_features(m->calc, s, precision, want_forces, m->species);
+    compute_features(m->calc, s, precision, want_forces, m->species, /*need_x32=*/false);
     model_layout(m, s);
     const int64_t na = s->n_atoms;
     s->E_d.ensure(sizeof(double) * (s->n_struct + 1));
@@ -1059,6 +1100,12 @@ rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precis
       RGPU_CUDA(cudaMemcpyAsync(forces, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s->st));
     }
     RGPU_CUDA(cudaStreamSynchronize(s->st));
+    if (precision == RGPU_PRECISION_FP32) {
+      const int where = gemm_tc_timeout(true);
+      if (where)
+        throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM: a bounded pipeline wait gave up (stage " +
+                                          std::to_string(where) + ")");
+    }
     if (energies) {
       // baseline (models/krr.py:68-90) on the host, FP64
       std::map<int, double> sc;
@@ -1074,6 +1121,73 @@ rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precis
     }
     if (forces && precision == RGPU_PRECISION_FP64)
       for (int64_t i = 0; i < 3 * na; ++i) forces[i] = -forces[i];
+  });
+}
+
+namespace {
+__global__ void bf16_pair_to_f32_kernel(const __nv_bfloat16 * hi, const __nv_bfloat16 * lo, int64_t rows,
+                                        int64_t cols, int64_t ld, float * out) {
+  int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= rows * cols) return;
+  int64_t r = i / cols, c = i - r * cols;
+  out[i] = __bfloat162float(hi[r * ld + c]) + __bfloat162float(lo[r * ld + c]);
+}
+__global__ void sum_parts_kernel(const float * parts, int n_parts, int64_t M, float * e) {
+  int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (r >= M) return;
+  float s = 0.f;
+  for (int t = 0; t < n_parts; ++t) s += parts[int64_t(t) * M + r];
+  e[r] = s;
+}
+}  // namespace
+
+rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K, const float * A, const float * B,
+                                   const float * alpha, int32_t zeta, float * C, float * e, void * stream) {
+  return guard([&] {
+    if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) throw Error(RGPU_ERR_INVALID_ARGUMENT, "bad GEMM arguments");
+    if (mode == 0 && N % 4 != 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "N must be a multiple of 4");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    static DevBuf ah, al, bh, bl, wh, wl, parts;
+    const int64_t Kp = (K + 63) / 64 * 64, Np = (N + 31) / 32 * 32;
+    ah.ensure(2 * size_t(M) * Kp);
+    al.ensure(2 * size_t(M) * Kp);
+    bh.ensure(2 * size_t(N) * Kp);
+    bl.ensure(2 * size_t(N) * Kp);
+    split_bf16(A, M, K, K, ah.as<__nv_bfloat16>(), al.as<__nv_bfloat16>(), Kp, st);
+    split_bf16(B, N, K, K, bh.as<__nv_bfloat16>(), bl.as<__nv_bfloat16>(), Kp, st);
+    Bf16x3Gemm g{};
+    g.M = M;
+    g.N = N;
+    g.K = Kp;
+    g.A_hi = ah.as<__nv_bfloat16>();
+    g.A_lo = al.as<__nv_bfloat16>();
+    g.lda = Kp;
+    g.B_hi = bh.as<__nv_bfloat16>();
+    g.B_lo = bl.as<__nv_bfloat16>();
+    g.ldb = Kp;
+    g.epilogue = mode;
+    if (mode == 0) {
+      g.C = C;
+      g.ldc = N;
+      gemm_bf16x3(g, st);
+    } else {
+      const int n_parts = int((N + kTcTileN - 1) / kTcTileN);
+      wh.ensure(2 * size_t(M) * Np);
+      wl.ensure(2 * size_t(M) * Np);
+      parts.ensure(sizeof(float) * size_t(n_parts) * M);
+      g.W_hi = wh.as<__nv_bfloat16>();
+      g.W_lo = wl.as<__nv_bfloat16>();
+      g.ldw = Np;
+      g.alpha = alpha;
+      g.zeta = zeta;
+      g.e_part = parts.as<float>();
+      gemm_bf16x3(g, st);
+      bf16_pair_to_f32_kernel<<<div_up(M * N, 256), 256, 0, st>>>(g.W_hi, g.W_lo, M, N, Np, C);
+      if (e) sum_parts_kernel<<<div_up(M, 256), 256, 0, st>>>(parts.as<float>(), n_parts, M, e);
+    }
+    RGPU_CUDA(cudaStreamSynchronize(st));
+    const int where = gemm_tc_timeout(true);
+    if (where) throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM wait gave up at stage " + std::to_string(where));
   });
 }
 

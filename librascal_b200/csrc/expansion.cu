@@ -100,6 +100,10 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
     const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
     const int ti = a.species_lut[a.types[a.center_atom[ci]]];
     uint32_t mask_all = 1u << ti;
+    // centre contribution first, as the reference accumulates
+    // (calculator_spherical_expansion.hh:2244-2247)
+    for (int nn = lane; nn < n; nn += 32) Ci[size_t(ti) * nK + nn * K] = T(a.center_contrib[nn]);
+    __syncwarp();
     for (int64_t p0 = p_lo; p0 < p_hi; p0 += 32) {
       const int np = int(min(int64_t(32), p_hi - p0));
       int my_sp = 31;
@@ -140,19 +144,17 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
           const int l = lofk[lm];
           const T * ri = RI + (nn * L1 + l) * 32;
           const T * yy = Y + lm * 32;
-          T acc = T(0);
+          T acc = Cs[e];  // pairs added in neighbour-list order
           for (int q = 0; q < cnt; ++q) {
             const int pl = order_s[wid][start + q];
             acc += (ri[pl] * yy[pl]) * FC[pl];
           }
-          Cs[e] += acc;
+          Cs[e] = acc;
         }
         start += cnt;
       }
       __syncwarp();
     }
-    // centre contribution, orthonormalised (calculator_spherical_expansion.hh:2244-2247)
-    for (int nn = lane; nn < n; nn += 32) Ci[size_t(ti) * nK + nn * K] += T(a.center_contrib[nn]);
     if (lane == 0) present[ci] = mask_all;
     __syncwarp();
   }
@@ -269,15 +271,22 @@ void launch_exp(const ExpansionArgs & a, T * C, uint32_t * present, cudaStream_t
 
 }  // namespace
 
+// The library compiles this file twice: RGPU_PART_FP64 (with --fmad=false, so
+// the FP64 arithmetic rounds like the CPU restatement) and RGPU_PART_FP32.
+#ifndef RGPU_PART_FP32
 void launch_expansion_fp64(const ExpansionArgs & a, double * C, uint32_t * present,
                            cudaStream_t st) {
   launch_exp<double>(a, C, present, st);
 }
+#endif
+#ifndef RGPU_PART_FP64
 void launch_expansion_fp32(const ExpansionArgs & a, float * C, uint32_t * present,
                            cudaStream_t st) {
   launch_exp<float>(a, C, present, st);
 }
+#endif
 
+#ifndef RGPU_PART_FP32
 void launch_expansion_grad_fp64(const ExpansionArgs & a, int64_t c0, int64_t c1, int64_t p_base,
                                 double * dCp, cudaStream_t st) {
   if (c1 <= c0) return;
@@ -320,5 +329,6 @@ void launch_expansion_selfgrad_fp64(const ExpansionArgs & a, int64_t c0, int64_t
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
+#endif
 
 }  // namespace rgpu

@@ -1,0 +1,408 @@
+// tcgen05 (5th-generation tensor core) GEMM for the GAP contractions.
+//
+//   C[M x N] = A[M x K] B[N x K]^T, A and B K-major (row-major, K fastest),
+//   computed as a 3-term BF16 split product with FP32 accumulation in TMEM:
+//     A B^T ~= A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T,
+//   A_hi = bf16(A), A_lo = bf16(A - A_hi) (same for B), which keeps ~16
+//   mantissa bits per product: enough for the 1e-4 force bar that a single
+//   TF32 or BF16 pass misses.
+//
+// One CTA computes one 128 x BN output tile:
+//   warp 0   TMA producer: per K block, 4 tiles (A_hi, A_lo, B_hi, B_lo)
+//            into a STAGES-deep ring of 128B-swizzled shared buffers;
+//   warp 1   MMA issuer: 3 tcgen05.mma (kind::f16, BF16 in, FP32 out) per
+//            16-wide K step into a 128 x BN FP32 accumulator in TMEM;
+//   warps 2-5 epilogue: tcgen05.ld of their 32-lane TMEM quadrant, then
+//            either a plain FP32 store or the fused GAP forward epilogue
+//            (k^zeta, per-row energy partial, W = alpha zeta k^(zeta-1)
+//            written as a BF16 hi/lo pair for the backward GEMM).
+// Every mbarrier wait is bounded; a wait that gives up records an error in
+// a device status word and the kernel winds down (TMEM is always freed).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace rgpu {
+namespace {
+
+constexpr int kBM = 128;
+constexpr int kBK = 64;  // bf16 elements per K block = 128 bytes (one swizzle row)
+constexpr int kThreads = 192;
+// Polls of one mbarrier before giving up (each try_wait may also suspend
+// briefly in hardware): far beyond any legitimate pipeline wait, and short
+// enough that a stuck wait ends the kernel in seconds. A wait that gives up
+// sets the shared status flag, which every other wait checks.
+constexpr long long kSpinLimit = 1ll << 22;
+
+struct TcStatus {
+  int timeout;
+  int where;
+};
+
+// ---------------------------------------------------------------- PTX wrappers
+__device__ __forceinline__ uint32_t smem_u32(const void * p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t * bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t * bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t * bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: false when the limit was hit (the status word records it).
+__device__ __forceinline__ bool mbar_wait(uint64_t * bar, uint32_t parity, TcStatus * st, int where) {
+  for (long long i = 0; i < kSpinLimit; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 63) == 63 && *reinterpret_cast<volatile int *>(&st->timeout)) return false;
+  }
+  if (atomicCAS(&st->timeout, 0, 1) == 0) st->where = where;
+  return false;
+}
+__device__ __forceinline__ void tma_load_2d(void * dst, const CUtensorMap * map, uint64_t * bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+__device__ __forceinline__ void prefetch_map(const CUtensorMap * map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (start, LBO, SBO in 16-byte units; version 1; layout 2).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= uint64_t((addr >> 4) & 0x3FFF);
+  d |= uint64_t(1) << 16;            // leading byte offset (unused for swizzled K-major)
+  d |= uint64_t(1024 >> 4) << 32;    // stride byte offset: next 8-row group
+  d |= uint64_t(1) << 46;            // descriptor version
+  d |= uint64_t(2) << 61;            // 128-byte swizzle
+  return d;
+}
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}"
+      ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t * bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float * v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
+// bits 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t make_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+struct TcArgs {
+  int64_t M, N, K;
+  int epilogue;        // 0 store FP32 C; 1 GAP forward
+  float * C;           // FP32 output (epilogue 0), row stride ldc
+  int64_t ldc;
+  __nv_bfloat16 * W_hi;  // epilogue 1 outputs, row stride ldw (zero beyond N)
+  __nv_bfloat16 * W_lo;
+  int64_t ldw;
+  const float * alpha;  // [N]
+  int zeta;
+  float * e_part;       // [gridDim.x][M]
+  TcStatus * status;
+};
+
+template <int BN, int STAGES>
+struct Smem {
+  static constexpr int A_BYTES = kBM * kBK * 2;  // 16 KB
+  static constexpr int B_BYTES = BN * kBK * 2;
+  static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int TOTAL = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+};
+
+__device__ __forceinline__ float powz(float v, int z) {
+  float r = 1.f;
+  for (int i = 0; i < z; ++i) r *= v;
+  return r;
+}
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(kThreads, 1)
+gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant__ CUtensorMap mA_lo,
+               const __grid_constant__ CUtensorMap mB_hi, const __grid_constant__ CUtensorMap mB_lo, TcArgs g) {
+  using SM = Smem<BN, STAGES>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // 1024-byte alignment for the 128B-swizzle atoms
+  unsigned char * base = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t * full = reinterpret_cast<uint64_t *>(base + STAGES * SM::STAGE_BYTES);
+  uint64_t * empty = full + STAGES;
+  uint64_t * accum = empty + STAGES;
+  uint32_t * tmem_slot = reinterpret_cast<uint32_t *>(accum + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t n0 = int64_t(blockIdx.x) * BN, m0 = int64_t(blockIdx.y) * kBM;
+  const int nk = int((g.K + kBK - 1) / kBK);
+
+  if (warp == 0 && lane == 0) {
+    prefetch_map(&mA_hi);
+    prefetch_map(&mA_lo);
+    prefetch_map(&mB_hi);
+    prefetch_map(&mB_lo);
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) {  // TMEM accumulator: BN FP32 columns x 128 lanes
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(uint32_t(BN)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int kb = 0; kb < nk; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t ph = uint32_t(kb / STAGES) & 1u;
+        if (!mbar_wait(&empty[s], ph ^ 1u, g.status, 1)) break;
+        unsigned char * st = base + s * SM::STAGE_BYTES;
+        mbar_expect_tx(&full[s], SM::STAGE_BYTES);
+        const int kx = kb * kBK;
+        tma_load_2d(st, &mA_hi, &full[s], kx, int(m0));
+        tma_load_2d(st + SM::A_BYTES, &mA_lo, &full[s], kx, int(m0));
+        tma_load_2d(st + 2 * SM::A_BYTES, &mB_hi, &full[s], kx, int(n0));
+        tma_load_2d(st + 2 * SM::A_BYTES + SM::B_BYTES, &mB_lo, &full[s], kx, int(n0));
+        ++issued;
+      }
+      // drain: the last copies must have landed before the CTA releases its
+      // shared memory (they normally have; this matters after a timeout)
+      for (int kb = issued > STAGES ? issued - STAGES : 0; kb < issued; ++kb)
+        mbar_wait(&full[kb % STAGES], uint32_t(kb / STAGES) & 1u, g.status, 4);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = make_idesc(kBM, BN);
+      bool ok = true;
+      for (int kb = 0; kb < nk && ok; ++kb) {
+        const int s = kb % STAGES;
+        const uint32_t ph = uint32_t(kb / STAGES) & 1u;
+        if (!mbar_wait(&full[s], ph, g.status, 2)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        unsigned char * st = base + s * SM::STAGE_BYTES;
+        const uint32_t a_hi = smem_u32(st), a_lo = smem_u32(st + SM::A_BYTES);
+        const uint32_t b_hi = smem_u32(st + 2 * SM::A_BYTES), b_lo = smem_u32(st + 2 * SM::A_BYTES + SM::B_BYTES);
+#pragma unroll
+        for (int k = 0; k < kBK / 16; ++k) {
+          const uint32_t off = uint32_t(k) * 32u;  // 16 bf16 = 32 bytes along the swizzled row
+          const uint32_t acc0 = (kb > 0 || k > 0) ? 1u : 0u;
+          mma_bf16(tmem, smem_desc(a_lo + off), smem_desc(b_hi + off), idesc, acc0);
+          mma_bf16(tmem, smem_desc(a_hi + off), smem_desc(b_lo + off), idesc, 1u);
+          mma_bf16(tmem, smem_desc(a_hi + off), smem_desc(b_hi + off), idesc, 1u);
+        }
+        mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
+      }
+      mma_commit(accum);  // accumulator complete (also fires if no MMA was issued)
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lane quadrant = warp % 4
+    const int q = warp & 3;
+    const int64_t row = m0 + q * 32 + lane;
+    const bool ok = __all_sync(0xffffffffu, mbar_wait(accum, 0u, g.status, 3));
+    tc_fence_after();
+    float e_acc = 0.f;
+    if (ok) {
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(c0), v);
+        const int64_t col = n0 + c0;
+        if (row >= g.M) continue;
+        if (g.epilogue == 0) {
+          float * out = g.C + row * g.ldc + col;
+          if (col + 16 <= g.N) {
+#pragma unroll
+            for (int i = 0; i < 16; i += 4)
+              *reinterpret_cast<float4 *>(out + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+          } else {
+            for (int i = 0; i < 16; ++i)
+              if (col + i < g.N) out[i] = v[i];
+          }
+        } else {
+          if (col >= g.ldw) continue;
+          __align__(16) __nv_bfloat16 hi[16], lo[16];
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const float al = (col + i < g.N) ? __ldg(g.alpha + col + i) : 0.f;
+            e_acc += al * powz(v[i], g.zeta);
+            const float w = al * (float(g.zeta) * powz(v[i], g.zeta - 1));
+            hi[i] = __float2bfloat16_rn(w);
+            lo[i] = __float2bfloat16_rn(w - __bfloat162float(hi[i]));
+          }
+          uint4 * dh = reinterpret_cast<uint4 *>(g.W_hi + row * g.ldw + col);
+          uint4 * dl = reinterpret_cast<uint4 *>(g.W_lo + row * g.ldw + col);
+          dh[0] = reinterpret_cast<uint4 *>(hi)[0];
+          dh[1] = reinterpret_cast<uint4 *>(hi)[1];
+          dl[0] = reinterpret_cast<uint4 *>(lo)[0];
+          dl[1] = reinterpret_cast<uint4 *>(lo)[1];
+        }
+      }
+    }
+    if (g.epilogue == 1 && row < g.M) g.e_part[int64_t(blockIdx.x) * g.M + row] = e_acc;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(BN)));
+  }
+}
+
+// ------------------------------------------------------------------ host side
+using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeFn encode_fn() {
+  static EncodeFn fn = nullptr;
+  if (!fn) {
+    void * p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cuda_check(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q),
+               "cudaGetDriverEntryPoint(cuTensorMapEncodeTiled)");
+    if (!p || q != cudaDriverEntryPointSuccess) throw Error(RGPU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<EncodeFn>(p);
+  }
+  return fn;
+}
+
+// 2D bf16 tensor map over a row-major [rows x cols] matrix with row stride
+// ld elements; box = box_rows x 64 columns, 128-byte swizzle, zero fill
+// outside the matrix.
+CUtensorMap make_map(const __nv_bfloat16 * ptr, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
+  if ((reinterpret_cast<uintptr_t>(ptr) & 15) != 0 || (ld * 2) % 16 != 0)
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, "tensor map: base or stride not 16-byte aligned");
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(ld * 2)};
+  cuuint32_t box[2] = {cuuint32_t(kBK), cuuint32_t(box_rows)};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(ptr), dims, strides,
+                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(RGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+  return m;
+}
+
+__global__ void split_bf16_kernel(const float * __restrict__ x, int64_t rows, int64_t cols, int64_t ldx,
+                                  __nv_bfloat16 * __restrict__ hi, __nv_bfloat16 * __restrict__ lo, int64_t ldo) {
+  int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= rows * ldo) return;
+  int64_t r = i / ldo, c = i - r * ldo;
+  float v = (c < cols) ? x[r * ldx + c] : 0.f;
+  __nv_bfloat16 h = __float2bfloat16_rn(v);
+  hi[i] = h;
+  lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+}  // namespace
+
+void split_bf16(const float * x, int64_t rows, int64_t cols, int64_t ldx, __nv_bfloat16 * hi, __nv_bfloat16 * lo,
+                int64_t ldo, cudaStream_t st) {
+  if (rows * ldo <= 0) return;
+  split_bf16_kernel<<<div_up(rows * ldo, 256), 256, 0, st>>>(x, rows, cols, ldx, hi, lo, ldo);
+  RGPU_LAUNCHED();
+}
+
+// Status word of the tcgen05 GEMM (device global, one per process).
+static TcStatus * tc_status() {
+  static TcStatus * p = nullptr;
+  if (!p) {
+    cuda_check(cudaMalloc(&p, sizeof(TcStatus)), "cudaMalloc(tc status)");
+    cuda_check(cudaMemset(p, 0, sizeof(TcStatus)), "cudaMemset(tc status)");
+  }
+  return p;
+}
+
+void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0) return;
+  constexpr int BN = kTcTileN, STAGES = 2;
+  const size_t smem = Smem<BN, STAGES>::TOTAL;
+  CUtensorMap a_hi = make_map(g.A_hi, g.M, g.K, g.lda, kBM);
+  CUtensorMap a_lo = make_map(g.A_lo, g.M, g.K, g.lda, kBM);
+  CUtensorMap b_hi = make_map(g.B_hi, g.N, g.K, g.ldb, BN);
+  CUtensorMap b_lo = make_map(g.B_lo, g.N, g.K, g.ldb, BN);
+  TcArgs t;
+  t.M = g.M;
+  t.N = g.N;
+  t.K = g.K;
+  t.epilogue = g.epilogue;
+  t.C = g.C;
+  t.ldc = g.ldc;
+  t.W_hi = g.W_hi;
+  t.W_lo = g.W_lo;
+  t.ldw = g.ldw;
+  t.alpha = g.alpha;
+  t.zeta = g.zeta;
+  t.e_part = g.e_part;
+  t.status = tc_status();
+  cuda_check(cudaFuncSetAttribute(gemm_tc_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem)),
+             "cudaFuncSetAttribute(gemm_tc)");
+  dim3 grid(div_up(g.N, BN), div_up(g.M, kBM));
+  gemm_tc_kernel<BN, STAGES><<<grid, kThreads, smem, st>>>(a_hi, a_lo, b_hi, b_lo, t);
+  RGPU_LAUNCHED();
+  cuda_check(cudaGetLastError(), "gemm_tc launch");
+}
+
+int gemm_tc_timeout(bool reset) {
+  TcStatus h{};
+  cuda_check(cudaMemcpy(&h, tc_status(), sizeof(h), cudaMemcpyDeviceToHost), "tc status");
+  if (reset && h.timeout) cuda_check(cudaMemset(tc_status(), 0, sizeof(TcStatus)), "tc status reset");
+  return h.timeout ? h.where : 0;
+}
+
+}  // namespace rgpu

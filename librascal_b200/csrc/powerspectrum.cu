@@ -62,8 +62,8 @@ __device__ __forceinline__ void decode(int d, int n, int L1, int blk, int & k, i
 
 template <typename T>
 __global__ void __launch_bounds__(kThreads)
-ps_fwd_kernel(PsArgs a, const T * __restrict__ C, T * __restrict__ X, T * __restrict__ norm_out,
-              bool inv) {
+ps_fwd_kernel(PsArgs a, const T * __restrict__ C, T * __restrict__ X, __nv_bfloat16 * __restrict__ Xh,
+              __nv_bfloat16 * __restrict__ Xl, T * __restrict__ norm_out, bool inv) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FeatureDims fd = a.fd;
   T * Cs = reinterpret_cast<T *>(smem_raw);
@@ -92,12 +92,17 @@ ps_fwd_kernel(PsArgs a, const T * __restrict__ C, T * __restrict__ X, T * __rest
   }
   ss = block_sum(ss, red);
   const T nrm = sqrt(ss);
-  T * Xr = X + size_t(a.row_of_center[ci]) * fd.Dpad;
+  const size_t roff = size_t(a.row_of_center[ci]) * fd.Dpad;
   const bool do_norm = a.normalize && fabs(double(nrm)) > 0.;
   for (int d = threadIdx.x; d < fd.Dpad; d += blockDim.x) {
     T v = d < fd.D ? Ps[d] : T(0);
     if (do_norm) v /= nrm;
-    Xr[d] = v;
+    if (X) X[roff + d] = v;
+    if (Xh) {  // BF16 hi/lo pair for the tensor-core GEMMs
+      const __nv_bfloat16 h = __float2bfloat16_rn(float(v));
+      Xh[roff + d] = h;
+      Xl[roff + d] = __float2bfloat16_rn(float(v) - __bfloat162float(h));
+    }
   }
   if (threadIdx.x == 0) {
     T nn = a.normalize ? nrm : T(1);
@@ -204,9 +209,9 @@ __global__ void pair_center_kernel(int64_t c0, int64_t c1, const int64_t * __res
 
 // Fast path adjoint: dE/dc from dE/dx (both FP32).
 __global__ void __launch_bounds__(kThreads)
-ps_bwd_kernel(PsArgs a, const float * __restrict__ C, const float * __restrict__ X,
-              const float * __restrict__ norm, const float * __restrict__ dX,
-              float * __restrict__ dC) {
+ps_bwd_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
+              const __nv_bfloat16 * __restrict__ Xl, const float * __restrict__ norm,
+              const float * __restrict__ dX, float * __restrict__ dC) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const FeatureDims fd = a.fd;
   float * Cs = reinterpret_cast<float *>(smem_raw);
@@ -217,13 +222,18 @@ ps_bwd_kernel(PsArgs a, const float * __restrict__ C, const float * __restrict__
   const int64_t ci = blockIdx.x;
   const int64_t row = a.row_of_center[ci];
   for (int i = threadIdx.x; i < fd.S * fd.nK; i += blockDim.x) Cs[i] = C[size_t(ci) * fd.S * fd.nK + i];
-  const float * xr = X + size_t(row) * fd.Dpad;
+  const __nv_bfloat16 * xh = Xh + size_t(row) * fd.Dpad;
+  const __nv_bfloat16 * xl = Xl + size_t(row) * fd.Dpad;
   const float * gr = dX + size_t(row) * fd.Dpad;
   float dot = 0.f;
-  for (int d = threadIdx.x; d < fd.D; d += blockDim.x) dot += xr[d] * gr[d];
+  for (int d = threadIdx.x; d < fd.D; d += blockDim.x) {
+    const float x = __bfloat162float(xh[d]) + __bfloat162float(xl[d]);
+    Gs[d] = x;
+    dot += x * gr[d];
+  }
   dot = a.normalize ? block_sum(dot, red) : 0.f;
   const float invn = 1.f / norm[ci];
-  for (int d = threadIdx.x; d < fd.D; d += blockDim.x) Gs[d] = (gr[d] - xr[d] * dot) * invn;
+  for (int d = threadIdx.x; d < fd.D; d += blockDim.x) Gs[d] = (gr[d] - Gs[d] * dot) * invn;
   __syncthreads();
   const int L1 = fd.L + 1, n = fd.n, blk = n * n * L1;
   for (int e = threadIdx.x; e < fd.S * fd.nK; e += blockDim.x) {
@@ -257,27 +267,33 @@ ps_bwd_kernel(PsArgs a, const float * __restrict__ C, const float * __restrict__
 
 }  // namespace
 
+// Compiled twice: RGPU_PART_FP64 (--fmad=false) and RGPU_PART_FP32.
+#ifndef RGPU_PART_FP32
 void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double * inv_norm,
                         cudaStream_t st) {
   if (a.n_centers == 0) return;
   size_t smem = sizeof(double) * (size_t(a.fd.S) * a.fd.nK + a.fd.D);
   RGPU_CUDA(cudaFuncSetAttribute(ps_fwd_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)));
-  ps_fwd_kernel<double><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, inv_norm, true);
+  ps_fwd_kernel<double><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, nullptr, nullptr, inv_norm, true);
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
-void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, float * norm,
-                        cudaStream_t st) {
+#endif
+#ifndef RGPU_PART_FP64
+void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
+                        __nv_bfloat16 * Xl, float * norm, cudaStream_t st) {
   if (a.n_centers == 0) return;
   size_t smem = sizeof(float) * (size_t(a.fd.S) * a.fd.nK + a.fd.D);
   RGPU_CUDA(cudaFuncSetAttribute(ps_fwd_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)));
-  ps_fwd_kernel<float><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, norm, false);
+  ps_fwd_kernel<float><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, Xh, Xl, norm, false);
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
+#endif
 
+#ifndef RGPU_PART_FP32
 void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, int64_t c1,
                          int64_t p_base, const double * C, const double * X,
                          const double * inv_norm, const double * dCp, const double * dCs,
@@ -301,15 +317,19 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
+#endif
 
-void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const float * X, const float * norm,
-                        const float * dX, float * dC, cudaStream_t st) {
+#ifndef RGPU_PART_FP64
+void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh,
+                        const __nv_bfloat16 * Xl, const float * norm, const float * dX, float * dC,
+                        cudaStream_t st) {
   if (a.n_centers == 0) return;
   size_t smem = sizeof(float) * (size_t(a.fd.S) * a.fd.nK + a.fd.D);
   RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  ps_bwd_kernel<<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, norm, dX, dC);
+  ps_bwd_kernel<<<int(a.n_centers), kThreads, smem, st>>>(a, C, Xh, Xl, norm, dX, dC);
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
+#endif
 
 }  // namespace rgpu

@@ -2,6 +2,7 @@
 // kernel files. Not part of the C ABI.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -188,8 +189,9 @@ struct PsArgs {
 // X rows (normalised) and inverse norms.
 void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double * inv_norm,
                         cudaStream_t st);
-void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, float * norm,
-                        cudaStream_t st);
+// FP32 forward: X (FP32, may be null) and/or its BF16 hi/lo split (may be null).
+void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
+                        __nv_bfloat16 * Xl, float * norm, cudaStream_t st);
 // Plain-path gradients of the normalised power spectrum for pairs of centres
 // [c0,c1): dX[p - p_base][3][D].
 void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, int64_t c1,
@@ -197,8 +199,10 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
                          const double * inv_norm, const double * dCp, const double * dCs,
                          double * dX, cudaStream_t st);
 // Adjoint: dE/dC[i][S][n][K] from dE/dX rows (species-sorted) for all centres.
-void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const float * X,
-                        const float * norm, const float * dX, float * dC, cudaStream_t st);
+// x is read back as hi + lo of its BF16 split.
+void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh,
+                        const __nv_bfloat16 * Xl, const float * norm, const float * dX, float * dC,
+                        cudaStream_t st);
 
 // ------------------------------------------------------------------ GAP
 struct GapSpecies {
@@ -230,6 +234,37 @@ struct Tf32GemmArgs {
   float * e_part;        // [n_tiles_N][M] row partial energies
 };
 void gemm_tf32(const Tf32GemmArgs & g, cudaStream_t st);
+
+// tcgen05 GEMM, C = A B^T as a 3-term BF16 split (A_hi B_hi + A_hi B_lo +
+// A_lo B_hi), FP32 accumulation in TMEM. A [M x K] and B [N x K] are
+// row-major hi/lo BF16 pairs (row strides lda, ldb; 16-byte aligned).
+// epilogue 0: C [M x ldc] FP32; epilogue 1: GAP forward (W_hi/W_lo
+// [M x ldw] BF16, zero for columns >= N; e_part [ceil(N/256)][M]).
+struct Bf16x3Gemm {
+  int64_t M, N, K;
+  const __nv_bfloat16 * A_hi;
+  const __nv_bfloat16 * A_lo;
+  int64_t lda;
+  const __nv_bfloat16 * B_hi;
+  const __nv_bfloat16 * B_lo;
+  int64_t ldb;
+  int epilogue;
+  float * C;
+  int64_t ldc;
+  __nv_bfloat16 * W_hi;
+  __nv_bfloat16 * W_lo;
+  int64_t ldw;
+  const float * alpha;
+  int zeta;
+  float * e_part;
+};
+constexpr int kTcTileN = 256;
+void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st);
+// 0 when no bounded wait of the tcgen05 GEMM gave up, else where it did.
+int gemm_tc_timeout(bool reset);
+// hi/lo BF16 split of a row-major FP32 matrix (columns >= cols become 0).
+void split_bf16(const float * x, int64_t rows, int64_t cols, int64_t ldx, __nv_bfloat16 * hi,
+                __nv_bfloat16 * lo, int64_t ldo, cudaStream_t st);
 // energies[structure of centre(center_of_row[row0 + r])] += e(r), where e(r)
 // is e_row_fp64[r] or the sum of the n_parts FP32 partials e_part[t*ld + r].
 void launch_energy_reduce(int64_t rows, int n_parts, const float * e_part, int64_t ld,
