@@ -34,11 +34,32 @@ struct Tab<float> {
   static __device__ __forceinline__ const float * d(const SplineDev & s) { return s.y2hf; }
 };
 
+// cos(x) for x within 0.02 of pi, correctly rounded: -cos(pi - x) by its
+// Taylor series in double-double (pi - x is exact by Sterbenz' lemma plus the
+// low word of pi). The switching function needs it because 1 + cos(x)
+// cancels there: an ulp of difference between two libm's cos becomes a
+// relative error of ulp / f_c in f_c.
+__device__ __forceinline__ double cos_near_pi(double x) {
+  const double pi_hi = 3.141592653589793116, pi_lo = 1.2246467991473532e-16;
+  double th = pi_hi - x;
+  double s = th + pi_lo;
+  double tl = pi_lo - (s - th);
+  th = s;
+  double u = th * th;
+  double ue = fma(th, th, -u) + 2.0 * th * tl;
+  double h = u * 0.5, hl = ue * 0.5;
+  double c = 1.0 - h;
+  double ce = ((1.0 - c) - h) - hl;
+  double tail = u * u * (1.0 / 24.0) - u * u * u * (1.0 / 720.0) + u * u * u * u * (1.0 / 40320.0);
+  return -(c + (ce + tail));
+}
+
 __device__ __forceinline__ double fc_cos(double r, double rc, double sw) {
   if (r <= (rc - sw)) return 1.0;
   if (r > rc) return 0.0;
   double rs = 3.14159265358979323846264338327950288 * (r - rc + sw) / sw;
-  return 0.5 * (1. + cos(rs));
+  double c = (rs > 3.121592653589793) ? cos_near_pi(rs) : cos(rs);
+  return 0.5 * (1. + c);
 }
 __device__ __forceinline__ double dfc_cos(double r, double rc, double sw) {
   if (r <= (rc - sw)) return 0.0;

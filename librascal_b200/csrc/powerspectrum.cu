@@ -70,38 +70,65 @@ ps_fwd_kernel(PsArgs a, const T * __restrict__ C, T * __restrict__ X, __nv_bfloa
   T * Ps = Cs + fd.S * fd.nK;
   __shared__ KeyTables kt;
   __shared__ T red[32];
+  __shared__ T lfs[kMaxL + 1];
   build_keys(kt, fd.S);
   const int64_t ci = blockIdx.x;
   const T * Ci = C + size_t(ci) * fd.S * fd.nK;
   for (int e = threadIdx.x; e < fd.S * fd.nK; e += blockDim.x) Cs[e] = Ci[e];
+  const int n = fd.n, S = fd.S, L1 = fd.L + 1, nn2 = n * n, blk = nn2 * L1;
+  // 1/sqrt(2l+1) (calculator_spherical_invariants.hh:62-69)
+  if (threadIdx.x < L1) lfs[threadIdx.x] = T(1.0 / sqrt(double(2 * threadIdx.x + 1)));
   __syncthreads();
-  const int L1 = fd.L + 1, blk = fd.n * fd.n * L1;
+  // task t = (l, n1, n2) with l slowest, so a warp shares l (uniform trip
+  // counts; the c^a and c^b reads are a few broadcast addresses per warp)
   T ss = T(0);
-  for (int d = threadIdx.x; d < fd.D; d += blockDim.x) {
-    int k, n1, n2, l;
-    decode(d, fd.n, L1, blk, k, n1, n2, l);
-    const int sa = kt.ka[k], sb = kt.kb[k];
-    const T * c1 = Cs + sa * fd.nK + n1 * fd.K + l * l;
-    const T * c2 = Cs + sb * fd.nK + n2 * fd.K + l * l;
-    T s = T(0);
-    for (int m = 0; m < 2 * l + 1; ++m) s += c1[m] * c2[m];
-    T v = s * T(1.0 / sqrt(double(2 * l + 1)));
-    if (sa < sb) v *= T(kSqrt2);
-    Ps[d] = v;
-    ss += v * v;
+  for (int t = threadIdx.x; t < blk; t += blockDim.x) {
+    const int l = t / nn2;
+    const int r = t - l * nn2;
+    const int n1 = r / n, n2 = r - n1 * n;
+    const int off = l * l, cnt = 2 * l + 1;
+    const T lf = lfs[l];
+    const int out = r * L1 + l;
+    for (int sa = 0; sa < S; ++sa) {
+      const T * c1 = Cs + sa * fd.nK + n1 * fd.K + off;
+      for (int sb = sa; sb < S; ++sb) {
+        const T * c2 = Cs + sb * fd.nK + n2 * fd.K + off;
+        T s = T(0);
+        for (int m = 0; m < cnt; ++m) s += c1[m] * c2[m];
+        T v = s * lf;
+        if (sa < sb) v *= T(kSqrt2);
+        Ps[kt.kid[sa][sb] * blk + out] = v;
+        ss += v * v;
+      }
+    }
   }
   ss = block_sum(ss, red);
   const T nrm = sqrt(ss);
   const size_t roff = size_t(a.row_of_center[ci]) * fd.Dpad;
   const bool do_norm = a.normalize && fabs(double(nrm)) > 0.;
-  for (int d = threadIdx.x; d < fd.Dpad; d += blockDim.x) {
-    T v = d < fd.D ? Ps[d] : T(0);
-    if (do_norm) v /= nrm;
-    if (X) X[roff + d] = v;
+  const T rinv = do_norm ? T(1) / nrm : T(1);
+  // 8 consecutive outputs per thread: 16-byte BF16 stores
+  for (int d0 = threadIdx.x * 8; d0 < fd.Dpad; d0 += blockDim.x * 8) {
+    T v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int d = d0 + i;
+      v[i] = d < fd.D ? Ps[d] : T(0);
+      if (do_norm) v[i] = (sizeof(T) == 8) ? v[i] / nrm : v[i] * rinv;
+    }
+    if (X) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) X[roff + d0 + i] = v[i];
+    }
     if (Xh) {  // BF16 hi/lo pair for the tensor-core GEMMs
-      const __nv_bfloat16 h = __float2bfloat16_rn(float(v));
-      Xh[roff + d] = h;
-      Xl[roff + d] = __float2bfloat16_rn(float(v) - __bfloat162float(h));
+      __align__(16) __nv_bfloat16 h[8], lo[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        h[i] = __float2bfloat16_rn(float(v[i]));
+        lo[i] = __float2bfloat16_rn(float(v[i]) - __bfloat162float(h[i]));
+      }
+      *reinterpret_cast<uint4 *>(Xh + roff + d0) = *reinterpret_cast<uint4 *>(h);
+      *reinterpret_cast<uint4 *>(Xl + roff + d0) = *reinterpret_cast<uint4 *>(lo);
     }
   }
   if (threadIdx.x == 0) {
@@ -207,7 +234,8 @@ __global__ void pair_center_kernel(int64_t c0, int64_t c1, const int64_t * __res
     pc[p - p_first] = ci;
 }
 
-// Fast path adjoint: dE/dc from dE/dx (both FP32).
+// Fast path adjoint: dE/dc from dE/dx (both FP32); L = max_angular.
+template <int L>
 __global__ void __launch_bounds__(kThreads)
 ps_bwd_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
               const __nv_bfloat16 * __restrict__ Xl, const float * __restrict__ norm,
@@ -235,33 +263,42 @@ ps_bwd_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * __re
   const float invn = 1.f / norm[ci];
   for (int d = threadIdx.x; d < fd.D; d += blockDim.x) Gs[d] = (gr[d] - Gs[d] * dot) * invn;
   __syncthreads();
-  const int L1 = fd.L + 1, n = fd.n, blk = n * n * L1;
-  for (int e = threadIdx.x; e < fd.S * fd.nK; e += blockDim.x) {
-    const int sa = e / fd.nK;
-    const int r = e - sa * fd.nK;
-    const int n1 = r / fd.K, lm = r - n1 * fd.K;
-    int l = 0;
-    while ((l + 1) * (l + 1) <= lm) ++l;
-    const float lf = rsqrtf(float(2 * l + 1));
-    float acc = 0.f;
-    for (int sb = 0; sb < fd.S; ++sb) {
-      const int k = kt.kid[sa][sb];
-      const float * gk = Gs + size_t(k) * blk;
-      const float * cb = Cs + sb * fd.nK + lm;
-      float part = 0.f;
-      if (sa < sb) {
-        for (int n2 = 0; n2 < n; ++n2) part += gk[(n1 * n + n2) * L1 + l] * cb[n2 * fd.K];
-        part *= float(kSqrt2);
-      } else if (sa > sb) {
-        for (int n2 = 0; n2 < n; ++n2) part += gk[(n2 * n + n1) * L1 + l] * cb[n2 * fd.K];
-        part *= float(kSqrt2);
-      } else {
-        for (int n2 = 0; n2 < n; ++n2)
-          part += (gk[(n1 * n + n2) * L1 + l] + gk[(n2 * n + n1) * L1 + l]) * cb[n2 * fd.K];
+  const int L1 = fd.L + 1, n = fd.n, S = fd.S, blk = n * n * L1, Sn = S * n;
+  // dE/dc_{a n1, lm} = lf_l sum_{b, n2} H_{(a n1),(b n2)}^l c_{b n2, lm} with
+  // H = sqrt2 G_(a,b) for a < b, its transpose for a > b, G + G^T on the
+  // diagonal keys. Task t = (l, a, n1) with l slowest: a warp shares l, so
+  // the c_{b n2, lm} reads are broadcasts; each thread keeps its 2l+1
+  // outputs in registers.
+  constexpr int MM = 2 * L + 1;
+  for (int t = threadIdx.x; t < Sn * L1; t += blockDim.x) {
+    const int l = t / Sn;
+    const int r = t - l * Sn;
+    const int sa = r / n, n1 = r - sa * n;
+    const int off = l * l, cnt = 2 * l + 1;
+    float acc[MM];
+#pragma unroll
+    for (int m = 0; m < MM; ++m) acc[m] = 0.f;
+    for (int sb = 0; sb < S; ++sb) {
+      const float * gk = Gs + size_t(kt.kid[sa][sb]) * blk + l;
+      const float w = (sa == sb) ? 1.f : float(kSqrt2);
+      for (int n2 = 0; n2 < n; ++n2) {
+        float h;
+        if (sa < sb)
+          h = gk[(n1 * n + n2) * L1];
+        else if (sa > sb)
+          h = gk[(n2 * n + n1) * L1];
+        else
+          h = gk[(n1 * n + n2) * L1] + gk[(n2 * n + n1) * L1];
+        h *= w;
+        const float * cb = Cs + sb * fd.nK + n2 * fd.K + off;
+#pragma unroll
+        for (int m = 0; m < MM; ++m)
+          if (m < cnt) acc[m] += h * cb[m];
       }
-      acc += part;
     }
-    dC[size_t(ci) * fd.S * fd.nK + e] = acc * lf;
+    const float lf = rsqrtf(float(2 * l + 1));
+    float * out = dC + size_t(ci) * fd.S * fd.nK + sa * fd.nK + n1 * fd.K + off;
+    for (int m = 0; m < cnt; ++m) out[m] = acc[m] * lf;
   }
 }
 
@@ -325,8 +362,30 @@ void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 *
                         cudaStream_t st) {
   if (a.n_centers == 0) return;
   size_t smem = sizeof(float) * (size_t(a.fd.S) * a.fd.nK + a.fd.D);
-  RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  ps_bwd_kernel<<<int(a.n_centers), kThreads, smem, st>>>(a, C, Xh, Xl, norm, dX, dC);
+#define RGPU_BWD_CASE(LL)                                                                     \
+  case LL:                                                                                    \
+    RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                   int(smem)));                                               \
+    ps_bwd_kernel<LL><<<int(a.n_centers), kThreads, smem, st>>>(a, C, Xh, Xl, norm, dX, dC);   \
+    break;
+  switch (a.fd.L) {
+    RGPU_BWD_CASE(0)
+    RGPU_BWD_CASE(1)
+    RGPU_BWD_CASE(2)
+    RGPU_BWD_CASE(3)
+    RGPU_BWD_CASE(4)
+    RGPU_BWD_CASE(5)
+    RGPU_BWD_CASE(6)
+    RGPU_BWD_CASE(7)
+    RGPU_BWD_CASE(8)
+    RGPU_BWD_CASE(9)
+    RGPU_BWD_CASE(10)
+    RGPU_BWD_CASE(11)
+    RGPU_BWD_CASE(12)
+    default:
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
+  }
+#undef RGPU_BWD_CASE
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }

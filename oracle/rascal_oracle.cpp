@@ -792,12 +792,33 @@ struct SphericalHarmonics {
   }
 };
 
+// cos(x) for x within 0.02 of pi, correctly rounded: -cos(pi - x) from its
+// Taylor series in double-double. In f_c = (1 + cos x)/2 the sum cancels
+// near the cutoff, so the last bit of cos decides the relative accuracy of
+// f_c there; a libm's cos may be off by an ulp in near-tie cases, and the
+// GPU and this oracle both use this correctly rounded value instead.
+static double cos_near_pi(double x) {
+  const double pi_hi = 3.141592653589793116, pi_lo = 1.2246467991473532e-16;
+  double th = pi_hi - x;
+  double s = th + pi_lo;
+  double tl = pi_lo - (s - th);
+  th = s;
+  double u = th * th;
+  double ue = std::fma(th, th, -u) + 2.0 * th * tl;
+  double h = u * 0.5, hl = ue * 0.5;
+  double c = 1.0 - h;
+  double ce = ((1.0 - c) - h) - hl;
+  double tail = u * u * (1.0 / 24.0) - u * u * u * (1.0 / 720.0) + u * u * u * u * (1.0 / 40320.0);
+  return -(c + (ce + tail));
+}
+
 // representations/cutoff_functions.hh:69-107
 static double fc_cos(double r, double rc, double sw) {
   if (r <= (rc - sw)) return 1.0;
   if (r > rc) return 0.0;
   double rs{PI * (r - rc + sw) / sw};
-  return (0.5 * (1. + std::cos(rs)));
+  double c = (rs > 3.121592653589793) ? cos_near_pi(rs) : std::cos(rs);
+  return (0.5 * (1. + c));
 }
 static double dfc_cos(double r, double rc, double sw) {
   if (r <= (rc - sw)) return 0.0;
