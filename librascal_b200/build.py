@@ -28,7 +28,7 @@ SOURCES = [
     ("expansion.cu", ["--fmad=false", "-DRGPU_PART_FP64"], "expansion_f64"),
     ("expansion.cu", ["-DRGPU_PART_FP32"], "expansion_f32"),
     ("powerspectrum.cu", ["--fmad=false", "-DRGPU_PART_FP64"], "powerspectrum_f64"),
-    ("powerspectrum.cu", ["-DRGPU_PART_FP32"], "powerspectrum_f32"),
+    ("ps_fast.cu", [], "ps_fast"),
     ("gemm.cu", [], "gemm"),
     ("gemm_tc.cu", [], "gemm_tc"),
     ("adjoint.cu", [], "adjoint"),

@@ -20,7 +20,7 @@
 namespace rgpu {
 namespace {
 
-constexpr int kWarps = 4;
+constexpr int kThreads = 128;
 
 __device__ __forceinline__ float fc_cos_f(double r, double rc, double sw) {
   if (r <= (rc - sw)) return 1.f;
@@ -35,101 +35,95 @@ __device__ __forceinline__ float dfc_cos_f(double r, double rc, double sw) {
   return float(-0.5 * 3.14159265358979323846264338327950288 / sw * sin(rs));
 }
 
+constexpr int kMaxN = 16;  // largest max_radial of the register-staged path
+
+// One thread per pair (pairs of many centres share a warp, so no lane idles
+// when centres have few neighbours). Per l, the n radial values RI and
+// p1 = dRI f_c + RI df_c are staged in registers; the spherical-harmonics
+// recurrence then streams (Y, grad Y) for that l.
 template <int L>
-__global__ void __launch_bounds__(kWarps * 32)
-pair_adjoint_kernel(ExpansionArgs a, const float * __restrict__ dC, double * __restrict__ F) {
+__global__ void __launch_bounds__(kThreads)
+pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, int64_t n_pairs,
+                    const float * __restrict__ dC, double * __restrict__ F) {
   constexpr int K = (L + 1) * (L + 1);
   constexpr int L1 = L + 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int W = a.fd.W, n = a.fd.n, S = a.fd.S, nK = a.fd.nK;
-  float * Es = reinterpret_cast<float *>(smem_raw) + size_t(wid) * (S * nK + 2 * W * 32);
-  float * RI = Es + S * nK;
-  float * P1 = RI + W * 32;
-  for (int64_t ci = int64_t(blockIdx.x) * kWarps + wid; ci < a.n_centers;
-       ci += int64_t(gridDim.x) * kWarps) {
-    const float * Ei = dC + size_t(ci) * S * nK;
-    for (int e = lane; e < S * nK; e += 32) Es[e] = Ei[e];
-    __syncwarp();
-    const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
+  for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n_pairs;
+       p += int64_t(gridDim.x) * blockDim.x) {
+    const int32_t ci = pair_center[p];
+    if (p == a.pair_off[ci]) continue;  // self pair: carried by the other pairs' F_i terms
     const int32_t self_atom = a.center_atom[ci];
-    float fi[3] = {0.f, 0.f, 0.f};
-    for (int64_t p = p_lo + lane; p < p_hi; p += 32) {
-      const double r = a.pair_dist[p];
-      const int32_t j = a.pair_j[p];
-      const int s = a.species_lut[a.types[j]];
-      const float fc = fc_cos_f(r, a.rc, a.sw), dfc = dfc_cos_f(r, a.rc, a.sw);
-      // RI and dRI of this pair (dRI is turned into p1 = dRI fc + RI dfc)
-      {
-        SplinePos q = spline_pos(a.sp, r);
-        const float aa = float(q.a), bb = float(q.b);
-        const float ca = aa * aa - 1.f, cb = bb * bb - 1.f;
-        const float ea = 3.f * aa * aa - 1.f, eb = 3.f * bb * bb - 1.f;
-        const float ih = float(a.sp.inv_h);
-        const float * y0 = a.sp.yf + size_t(q.k) * W;
-        const float * d0 = a.sp.y2hf + size_t(q.k) * W;
-        for (int c = 0; c < W; ++c) {
-          const float yy0 = __ldg(y0 + c), yy1 = __ldg(y0 + W + c);
-          const float dd0 = __ldg(d0 + c), dd1 = __ldg(d0 + W + c);
-          const float ri = aa * (yy0 + ca * dd0) + bb * (yy1 + cb * dd1);
-          const float dri = (yy1 - yy0 - ea * dd0 + eb * dd1) * ih;
-          RI[c * 32 + lane] = ri;
-          P1[c * 32 + lane] = dri * fc + ri * dfc;
-        }
-      }
-      const float * E = Es + s * nK;
-      float sY = 0.f, sd[3] = {0.f, 0.f, 0.f};
-      const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
-                  dz = float(a.pair_dir[3 * p + 2]);
-      spherical_harmonics<L, true, float>(dx, dy, dz, [&](int lm, float y, float gx, float gy,
-                                                          float gz) {
-        int l = 0;
+    const double r = a.pair_dist[p];
+    const int32_t j = a.pair_j[p];
+    const int s = a.species_lut[a.types[j]];
+    const float fc = fc_cos_f(r, a.rc, a.sw), dfc = dfc_cos_f(r, a.rc, a.sw);
+    const SplinePos q = spline_pos(a.sp, r);
+    const float aa = float(q.a), bb = float(q.b);
+    const float ca = aa * aa - 1.f, cb = bb * bb - 1.f;
+    const float ea = 3.f * aa * aa - 1.f, eb = 3.f * bb * bb - 1.f;
+    const float ih = float(a.sp.inv_h);
+    const float * y0 = a.sp.yf + size_t(q.k) * W;
+    const float * d0 = a.sp.y2hf + size_t(q.k) * W;
+    const float * E = dC + (size_t(ci) * S + s) * nK;
+    float rl[kMaxN], pl[kMaxN];
+    float sY = 0.f, sd0 = 0.f, sd1 = 0.f, sd2 = 0.f;
+    const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
+                dz = float(a.pair_dir[3 * p + 2]);
+    spherical_harmonics<L, true, float>(
+        dx, dy, dz,
+        [&](int lm, float y, float gx, float gy, float gz) {
+          float A = 0.f, B = 0.f;
 #pragma unroll
-        for (int ll = 1; ll <= L; ++ll) l += (lm >= ll * ll);
-        float A = 0.f, B = 0.f;
-        for (int nn = 0; nn < n; ++nn) {
-          const float ev = E[nn * K + lm];
-          A += ev * P1[(nn * L1 + l) * 32 + lane];
-          B += ev * RI[(nn * L1 + l) * 32 + lane];
-        }
-        sY += A * y;
-        sd[0] += B * gx;
-        sd[1] += B * gy;
-        sd[2] += B * gz;
-      });
-      const float fr = fc / float(r);
-      const float g[3] = {dx * sY + fr * sd[0], dy * sY + fr * sd[1], dz * sY + fr * sd[2]};
+          for (int nn = 0; nn < kMaxN; ++nn) {
+            if (nn < n) {
+              const float ev = __ldg(E + nn * K + lm);
+              A += ev * pl[nn];
+              B += ev * rl[nn];
+            }
+          }
+          sY += A * y;
+          sd0 += B * gx;
+          sd1 += B * gy;
+          sd2 += B * gz;
+        },
+        [&](int l) {
 #pragma unroll
-      for (int c = 0; c < 3; ++c) atomicAdd(&F[3 * size_t(j) + c], -double(g[c]));
-      if (j != self_atom) {
-        fi[0] += g[0];
-        fi[1] += g[1];
-        fi[2] += g[2];
-      }
+          for (int nn = 0; nn < kMaxN; ++nn) {
+            if (nn < n) {
+              const int c = nn * L1 + l;
+              const float yy0 = __ldg(y0 + c), yy1 = __ldg(y0 + W + c);
+              const float dd0 = __ldg(d0 + c), dd1 = __ldg(d0 + W + c);
+              const float ri = aa * (yy0 + ca * dd0) + bb * (yy1 + cb * dd1);
+              const float dri = (yy1 - yy0 - ea * dd0 + eb * dd1) * ih;
+              rl[nn] = ri;
+              pl[nn] = dri * fc + ri * dfc;
+            }
+          }
+        });
+    const float fr = fc / float(r);
+    const float g0 = dx * sY + fr * sd0, g1 = dy * sY + fr * sd1, g2 = dz * sY + fr * sd2;
+    atomicAdd(&F[3 * size_t(j) + 0], -double(g0));
+    atomicAdd(&F[3 * size_t(j) + 1], -double(g1));
+    atomicAdd(&F[3 * size_t(j) + 2], -double(g2));
+    if (j != self_atom) {
+      atomicAdd(&F[3 * size_t(self_atom) + 0], double(g0));
+      atomicAdd(&F[3 * size_t(self_atom) + 1], double(g1));
+      atomicAdd(&F[3 * size_t(self_atom) + 2], double(g2));
     }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) fi[c] = warp_sum(fi[c]);
-    if (lane == 0) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) atomicAdd(&F[3 * size_t(self_atom) + c], double(fi[c]));
-    }
-    __syncwarp();
   }
 }
 
 }  // namespace
 
-void launch_pair_adjoint_fp32(const ExpansionArgs & a, const float * dC, double * forces,
-                              cudaStream_t st) {
-  if (a.n_centers == 0) return;
+void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_center, int64_t n_pairs,
+                              const float * dC, double * forces, cudaStream_t st) {
+  if (a.n_centers == 0 || n_pairs == 0) return;
   sph_constants_tu();
-  const size_t smem = size_t(kWarps) * (size_t(a.fd.S) * a.fd.nK + 2 * a.fd.W * 32) * sizeof(float);
-  int grid = int(std::min<int64_t>((a.n_centers + kWarps - 1) / kWarps, 148 * 16));
-#define RGPU_ADJ_CASE(LL)                                                                   \
-  case LL:                                                                                  \
-    RGPU_CUDA(cudaFuncSetAttribute(pair_adjoint_kernel<LL>,                                 \
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    pair_adjoint_kernel<LL><<<grid, kWarps * 32, smem, st>>>(a, dC, forces);                \
+  if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
+  const int grid = int(std::min<int64_t>((n_pairs + kThreads - 1) / kThreads, int64_t(148) * 64));
+#define RGPU_ADJ_CASE(LL)                                                                            \
+  case LL:                                                                                           \
+    pair_adjoint_kernel<LL><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces);         \
     break;
   switch (a.fd.L) {
     RGPU_ADJ_CASE(0)

@@ -683,7 +683,7 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
                      s->dC32.as<float>(), st);
   mark(s, 7);
   ExpansionArgs ea = exp_args(c, s);
-  launch_pair_adjoint_fp32(ea, s->dC32.as<float>(), F_d, st);
+  launch_pair_adjoint_fp32(ea, s->nl.pair_center, s->nl.n_pairs, s->dC32.as<float>(), F_d, st);
 }
 
 }  // namespace

@@ -92,8 +92,14 @@ struct SphC<float> {
 // Legendre functions by the l-recurrence, cos/sin(m phi) by the Chebyshev
 // recurrence, storage order (l, m = -l..l), pole branch at sin(theta) <= 0.1.
 // The callback receives (lm, Y, dY/dx, dY/dy, dY/dz) for every lm in order.
-template <int L, bool DER, typename T, typename Emit>
-__device__ __forceinline__ void spherical_harmonics(T x, T y, T z, Emit && emit) {
+struct NoBeginL {
+  __device__ __forceinline__ void operator()(int) const {}
+};
+
+// `begin_l(l)` runs before the first emit of every l (compile-time l after
+// unrolling), so a caller can stage per-l data in registers.
+template <int L, bool DER, typename T, typename Emit, typename BeginL = NoBeginL>
+__device__ __forceinline__ void spherical_harmonics(T x, T y, T z, Emit && emit, BeginL && begin_l = BeginL()) {
   constexpr int S = kMaxL + 2;
   const T nrm2 = x * x + y * y + z * z;
   if (fabs(double(nrm2) - 1.0) > (sizeof(T) == 8 ? 100.0 * 2.220446049250313e-16 : 1e-5)) {
@@ -154,6 +160,7 @@ __device__ __forceinline__ void spherical_harmonics(T x, T y, T z, Emit && emit)
 #pragma unroll
     for (int m = l + 1; m < L + 2; ++m) p0[m] = T(0);
     const int base = l * l + l;
+    begin_l(l);
     // Y values
     T Yv[2 * L + 1];
 #pragma unroll

@@ -20,6 +20,7 @@ namespace rgpu {
 namespace {
 
 constexpr int kWarps = 4;
+constexpr int kPad = 33;  // shared row stride of the per-pair tiles
 
 template <typename T>
 struct Tab;
@@ -101,9 +102,12 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int W = a.fd.W, nK = a.fd.nK, S = a.fd.S, n = a.fd.n;
-  T * RI = reinterpret_cast<T *>(smem_raw) + size_t(wid) * (W + K + 1) * 32;
-  T * Y = RI + W * 32;
-  T * FC = Y + K * 32;
+  // per-pair values in columns of a row-major [item][kPad] tile: the
+  // accumulation reads one pair column across many rows, so the row stride
+  // is 33 words to keep those reads on distinct banks
+  T * RI = reinterpret_cast<T *>(smem_raw) + size_t(wid) * (W + K + 1) * kPad;
+  T * Y = RI + W * kPad;
+  T * FC = Y + K * kPad;
   __shared__ int8_t sp_s[kWarps][32];
   __shared__ uint8_t order_s[kWarps][32];
   __shared__ uint8_t lofk[K];
@@ -133,11 +137,11 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
         const double r = a.pair_dist[p];
         my_sp = a.species_lut[a.types[a.pair_j[p]]];
         FC[lane] = T(fc_cos(r, a.rc, a.sw));
-        spline_eval<T, false>(a.sp, r, RI + lane, nullptr, 32);
+        spline_eval<T, false>(a.sp, r, RI + lane, nullptr, kPad);
         const T dx = T(a.pair_dir[3 * p]), dy = T(a.pair_dir[3 * p + 1]),
                 dz = T(a.pair_dir[3 * p + 2]);
         spherical_harmonics<L, false, T>(dx, dy, dz, [&](int lm, T y, T, T, T) {
-          Y[lm * 32 + lane] = y;
+          Y[lm * kPad + lane] = y;
         });
       }
       // stable order of the chunk's pairs by species
@@ -163,8 +167,8 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
         for (int e = lane; e < nK; e += 32) {
           const int nn = e / K, lm = e - nn * K;
           const int l = lofk[lm];
-          const T * ri = RI + (nn * L1 + l) * 32;
-          const T * yy = Y + lm * 32;
+          const T * ri = RI + (nn * L1 + l) * kPad;
+          const T * yy = Y + lm * kPad;
           T acc = Cs[e];  // pairs added in neighbour-list order
           for (int q = 0; q < cnt; ++q) {
             const int pl = order_s[wid][start + q];
@@ -250,7 +254,7 @@ __global__ void expansion_selfgrad_kernel(ExpansionArgs a, int64_t c0, int64_t p
 
 template <typename T>
 size_t exp_smem(const FeatureDims & fd) {
-  return size_t(kWarps) * (fd.W + fd.K + 1) * 32 * sizeof(T);
+  return size_t(kWarps) * (fd.W + fd.K + 1) * kPad * sizeof(T);
 }
 
 template <typename T>

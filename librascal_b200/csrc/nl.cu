@@ -294,7 +294,8 @@ __global__ void nl_gather_kernel(int64_t n_centers, GatherCtx c, int64_t * __res
                                  const int32_t * __restrict__ site_shift,
                                  int32_t * __restrict__ center_atom,
                                  int32_t * __restrict__ pair_j, int32_t * __restrict__ pair_shift,
-                                 double * __restrict__ pair_dist, double * __restrict__ pair_dir) {
+                                 double * __restrict__ pair_dist, double * __restrict__ pair_dir,
+                                 int32_t * __restrict__ pair_center) {
   const int lane = threadIdx.x & 31;
   int64_t ci = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   if (ci >= n_centers) return;
@@ -364,6 +365,8 @@ __global__ void nl_gather_kernel(int64_t n_centers, GatherCtx c, int64_t * __res
     }
   }
   if (MODE == 0 && lane == 0) count[ci] = out + 1;
+  if (MODE == 1)
+    for (int64_t p = base - 1 + lane; p < base + out; p += 32) pair_center[p] = int32_t(ci);
   (void)site_type;
 }
 
@@ -515,7 +518,7 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   if (n_centers > 0) {
     nl_gather_kernel<0><<<grid, kThreads, 0, st>>>(n_centers, c, w.counts64.as<int64_t>(), nullptr,
                                                    nullptr, nullptr, nullptr, nullptr, nullptr,
-                                                   nullptr, nullptr, nullptr);
+                                                   nullptr, nullptr, nullptr, nullptr);
     RGPU_LAUNCHED();
   }
   scan_exclusive_i64(w.counts64.as<int64_t>(), w.pair_off.as<int64_t>(), n_centers, w.scan_tmp, st);
@@ -527,12 +530,13 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   w.pair_shift.ensure(sizeof(int32_t) * 3 * (n_pairs + 1));
   w.pair_dist.ensure(sizeof(double) * (n_pairs + 1));
   w.pair_dir.ensure(sizeof(double) * 3 * (n_pairs + 1));
+  w.pair_center.ensure(sizeof(int32_t) * (n_pairs + 1));
   if (n_centers > 0) {
     nl_gather_kernel<1><<<grid, kThreads, 0, st>>>(
         n_centers, c, nullptr, w.pair_off.as<int64_t>(), w.site_type.as<int32_t>(),
         w.site_real.as<int32_t>(), w.site_shift.as<int32_t>(), w.center_atom.as<int32_t>(),
         w.pair_j.as<int32_t>(), w.pair_shift.as<int32_t>(), w.pair_dist.as<double>(),
-        w.pair_dir.as<double>());
+        w.pair_dir.as<double>(), w.pair_center.as<int32_t>());
     RGPU_LAUNCHED();
   }
   out.n_centers = n_centers;
@@ -541,6 +545,7 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   out.center_struct = w.center_struct.as<int32_t>();
   out.pair_off = w.pair_off.as<int64_t>();
   out.pair_j = w.pair_j.as<int32_t>();
+  out.pair_center = w.pair_center.as<int32_t>();
   out.pair_shift = w.pair_shift.as<int32_t>();
   out.pair_dist = w.pair_dist.as<double>();
   out.pair_dir = w.pair_dir.as<double>();

@@ -234,77 +234,9 @@ __global__ void pair_center_kernel(int64_t c0, int64_t c1, const int64_t * __res
     pc[p - p_first] = ci;
 }
 
-// Fast path adjoint: dE/dc from dE/dx (both FP32); L = max_angular.
-template <int L>
-__global__ void __launch_bounds__(kThreads)
-ps_bwd_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
-              const __nv_bfloat16 * __restrict__ Xl, const float * __restrict__ norm,
-              const float * __restrict__ dX, float * __restrict__ dC) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const FeatureDims fd = a.fd;
-  float * Cs = reinterpret_cast<float *>(smem_raw);
-  float * Gs = Cs + fd.S * fd.nK;
-  __shared__ KeyTables kt;
-  __shared__ float red[32];
-  build_keys(kt, fd.S);
-  const int64_t ci = blockIdx.x;
-  const int64_t row = a.row_of_center[ci];
-  for (int i = threadIdx.x; i < fd.S * fd.nK; i += blockDim.x) Cs[i] = C[size_t(ci) * fd.S * fd.nK + i];
-  const __nv_bfloat16 * xh = Xh + size_t(row) * fd.Dpad;
-  const __nv_bfloat16 * xl = Xl + size_t(row) * fd.Dpad;
-  const float * gr = dX + size_t(row) * fd.Dpad;
-  float dot = 0.f;
-  for (int d = threadIdx.x; d < fd.D; d += blockDim.x) {
-    const float x = __bfloat162float(xh[d]) + __bfloat162float(xl[d]);
-    Gs[d] = x;
-    dot += x * gr[d];
-  }
-  dot = a.normalize ? block_sum(dot, red) : 0.f;
-  const float invn = 1.f / norm[ci];
-  for (int d = threadIdx.x; d < fd.D; d += blockDim.x) Gs[d] = (gr[d] - Gs[d] * dot) * invn;
-  __syncthreads();
-  const int L1 = fd.L + 1, n = fd.n, S = fd.S, blk = n * n * L1, Sn = S * n;
-  // dE/dc_{a n1, lm} = lf_l sum_{b, n2} H_{(a n1),(b n2)}^l c_{b n2, lm} with
-  // H = sqrt2 G_(a,b) for a < b, its transpose for a > b, G + G^T on the
-  // diagonal keys. Task t = (l, a, n1) with l slowest: a warp shares l, so
-  // the c_{b n2, lm} reads are broadcasts; each thread keeps its 2l+1
-  // outputs in registers.
-  constexpr int MM = 2 * L + 1;
-  for (int t = threadIdx.x; t < Sn * L1; t += blockDim.x) {
-    const int l = t / Sn;
-    const int r = t - l * Sn;
-    const int sa = r / n, n1 = r - sa * n;
-    const int off = l * l, cnt = 2 * l + 1;
-    float acc[MM];
-#pragma unroll
-    for (int m = 0; m < MM; ++m) acc[m] = 0.f;
-    for (int sb = 0; sb < S; ++sb) {
-      const float * gk = Gs + size_t(kt.kid[sa][sb]) * blk + l;
-      const float w = (sa == sb) ? 1.f : float(kSqrt2);
-      for (int n2 = 0; n2 < n; ++n2) {
-        float h;
-        if (sa < sb)
-          h = gk[(n1 * n + n2) * L1];
-        else if (sa > sb)
-          h = gk[(n2 * n + n1) * L1];
-        else
-          h = gk[(n1 * n + n2) * L1] + gk[(n2 * n + n1) * L1];
-        h *= w;
-        const float * cb = Cs + sb * fd.nK + n2 * fd.K + off;
-#pragma unroll
-        for (int m = 0; m < MM; ++m)
-          if (m < cnt) acc[m] += h * cb[m];
-      }
-    }
-    const float lf = rsqrtf(float(2 * l + 1));
-    float * out = dC + size_t(ci) * fd.S * fd.nK + sa * fd.nK + n1 * fd.K + off;
-    for (int m = 0; m < cnt; ++m) out[m] = acc[m] * lf;
-  }
-}
-
 }  // namespace
 
-// Compiled twice: RGPU_PART_FP64 (--fmad=false) and RGPU_PART_FP32.
+// FP64 kernels; compiled with --fmad=false (the FP32 path is in ps_fast.cu).
 #ifndef RGPU_PART_FP32
 void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double * inv_norm,
                         cudaStream_t st) {
@@ -313,18 +245,6 @@ void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double *
   RGPU_CUDA(cudaFuncSetAttribute(ps_fwd_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem)));
   ps_fwd_kernel<double><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, nullptr, nullptr, inv_norm, true);
-  RGPU_LAUNCHED();
-  RGPU_CUDA(cudaGetLastError());
-}
-#endif
-#ifndef RGPU_PART_FP64
-void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
-                        __nv_bfloat16 * Xl, float * norm, cudaStream_t st) {
-  if (a.n_centers == 0) return;
-  size_t smem = sizeof(float) * (size_t(a.fd.S) * a.fd.nK + a.fd.D);
-  RGPU_CUDA(cudaFuncSetAttribute(ps_fwd_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(smem)));
-  ps_fwd_kernel<float><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, Xh, Xl, norm, false);
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
@@ -356,39 +276,5 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
 }
 #endif
 
-#ifndef RGPU_PART_FP64
-void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh,
-                        const __nv_bfloat16 * Xl, const float * norm, const float * dX, float * dC,
-                        cudaStream_t st) {
-  if (a.n_centers == 0) return;
-  size_t smem = sizeof(float) * (size_t(a.fd.S) * a.fd.nK + a.fd.D);
-#define RGPU_BWD_CASE(LL)                                                                     \
-  case LL:                                                                                    \
-    RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                   int(smem)));                                               \
-    ps_bwd_kernel<LL><<<int(a.n_centers), kThreads, smem, st>>>(a, C, Xh, Xl, norm, dX, dC);   \
-    break;
-  switch (a.fd.L) {
-    RGPU_BWD_CASE(0)
-    RGPU_BWD_CASE(1)
-    RGPU_BWD_CASE(2)
-    RGPU_BWD_CASE(3)
-    RGPU_BWD_CASE(4)
-    RGPU_BWD_CASE(5)
-    RGPU_BWD_CASE(6)
-    RGPU_BWD_CASE(7)
-    RGPU_BWD_CASE(8)
-    RGPU_BWD_CASE(9)
-    RGPU_BWD_CASE(10)
-    RGPU_BWD_CASE(11)
-    RGPU_BWD_CASE(12)
-    default:
-      throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
-  }
-#undef RGPU_BWD_CASE
-  RGPU_LAUNCHED();
-  RGPU_CUDA(cudaGetLastError());
-}
-#endif
 
 }  // namespace rgpu

@@ -127,6 +127,7 @@ struct NlOutputs {
   int32_t * center_struct{nullptr}; // [n_centers]
   int64_t * pair_off{nullptr};      // [n_centers+1]
   int32_t * pair_j{nullptr};        // [n_pairs] global original index of the real atom
+  int32_t * pair_center{nullptr};   // [n_pairs] centre row of each pair
   int32_t * pair_shift{nullptr};    // [n_pairs*3]
   double * pair_dist{nullptr};      // [n_pairs]
   double * pair_dir{nullptr};       // [n_pairs*3]
@@ -135,7 +136,7 @@ struct NlWork {
   DevBuf geom, counts64, scan_tmp, ghost_off, site_x, site_type, site_real, site_shift,
       site_box, box_base, box_count, box_ptr, box_fill, sorted, sorted_x, sorted_info,
       pair_count;
-  DevBuf center_atom, center_struct, pair_off, pair_j, pair_shift, pair_dist, pair_dir;
+  DevBuf center_atom, center_struct, pair_off, pair_j, pair_shift, pair_dist, pair_dir, pair_center;
 };
 // Builds the full list with self pairs and the strict cutoff. Synchronises
 // the stream a few times to size buffers. Throws Error on invalid input.
@@ -277,7 +278,8 @@ void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, 
                                 const int32_t * row_of_center, const double * dX,
                                 const double * t, int64_t ldt, double * grad, cudaStream_t st);
 // Adjoint pair kernel: forces from dE/dC (FP32) and recomputed dC/dr.
-void launch_pair_adjoint_fp32(const ExpansionArgs & a, const float * dC, double * forces,
+void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_center, int64_t n_pairs,
+                              const float * dC, double * forces,
                               cudaStream_t st);
 
 // ------------------------------------------------------------------ helpers
