@@ -64,16 +64,30 @@ __device__ __forceinline__ float block_sum_f(float v, float * red) {
   return red[0];
 }
 
+// Source index (l^2 + m) of every padded column, -1 for padding.
+template <int L>
+struct PadMap {
+  int8_t src[row_stride(L)];
+  constexpr PadMap() : src() {
+    int c = 0;
+    for (int l = 0; l <= L; ++l)
+      for (int m = 0; m < pad4(2 * l + 1); ++m) src[c++] = int8_t(m < 2 * l + 1 ? l * l + m : -1);
+    for (; c < row_stride(L); ++c) src[c] = -1;
+  }
+};
+
 // Load c^i (S x n x K, K = (L+1)^2) into the padded layout.
 template <int L>
 __device__ __forceinline__ void load_padded(const float * __restrict__ Ci, float * Cp, int S, int n) {
   constexpr int K = (L + 1) * (L + 1), RS = row_stride(L);
+  constexpr PadMap<L> pm;
+  __shared__ int8_t src[RS];
+  if (threadIdx.x < RS) src[threadIdx.x] = pm.src[threadIdx.x];
+  __syncthreads();
   for (int e = threadIdx.x; e < S * n * RS; e += blockDim.x) {
     const int row = e / RS, c = e - row * RS;
-    int l = 0;
-    while (l < L && offp(l + 1) <= c) ++l;
-    const int m = c - offp(l);
-    Cp[e] = (m < 2 * l + 1 && c < offp(L + 1)) ? Ci[row * K + l * l + m] : 0.f;
+    const int s = src[c];
+    Cp[e] = (s >= 0) ? Ci[row * K + s] : 0.f;
   }
 }
 
