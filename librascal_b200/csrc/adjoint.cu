@@ -39,76 +39,122 @@ constexpr int kMaxN = 16;  // largest max_radial of the register-staged path
 
 // One thread per pair (pairs of many centres share a warp, so no lane idles
 // when centres have few neighbours). Per l, the n radial values RI and
-// p1 = dRI f_c + RI df_c are staged in registers; the spherical-harmonics
-// recurrence then streams (Y, grad Y) for that l.
-template <int L>
-__global__ void __launch_bounds__(kThreads)
+// p1 = dRI f_c + RI df_c are staged in registers (NV >= n of them); the
+// spherical-harmonics recurrence then streams (Y, grad Y) for that l.
+// dE/dc of the pair's centre is read as dC[i][lm][s*n + n'], n contiguous
+// values per lm (float4 loads when n == NV).
+template <int L, int NV>
+__global__ void __launch_bounds__(kThreads, 4)  // 128 registers, no spills at L = 6
 pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, int64_t n_pairs,
                     const float * __restrict__ dC, double * __restrict__ F) {
   constexpr int K = (L + 1) * (L + 1);
   constexpr int L1 = L + 1;
-  const int W = a.fd.W, n = a.fd.n, S = a.fd.S, nK = a.fd.nK;
-  for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n_pairs;
-       p += int64_t(gridDim.x) * blockDim.x) {
-    const int32_t ci = pair_center[p];
-    if (p == a.pair_off[ci]) continue;  // self pair: carried by the other pairs' F_i terms
-    const int32_t self_atom = a.center_atom[ci];
-    const double r = a.pair_dist[p];
-    const int32_t j = a.pair_j[p];
-    const int s = a.species_lut[a.types[j]];
-    const float fc = fc_cos_f(r, a.rc, a.sw), dfc = dfc_cos_f(r, a.rc, a.sw);
-    const SplinePos q = spline_pos(a.sp, r);
-    const float aa = float(q.a), bb = float(q.b);
-    const float ca = aa * aa - 1.f, cb = bb * bb - 1.f;
-    const float ea = 3.f * aa * aa - 1.f, eb = 3.f * bb * bb - 1.f;
-    const float ih = float(a.sp.inv_h);
-    const float * y0 = a.sp.yf + size_t(q.k) * W;
-    const float * d0 = a.sp.y2hf + size_t(q.k) * W;
-    const float * E = dC + (size_t(ci) * S + s) * nK;
-    float rl[kMaxN], pl[kMaxN];
-    float sY = 0.f, sd0 = 0.f, sd1 = 0.f, sd2 = 0.f;
-    const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
-                dz = float(a.pair_dir[3 * p + 2]);
-    spherical_harmonics<L, true, float>(
-        dx, dy, dz,
-        [&](int lm, float y, float gx, float gy, float gz) {
-          float A = 0.f, B = 0.f;
+  const int W = a.fd.W, n = a.fd.n, Sn = a.fd.S * a.fd.n;
+  const bool vec = (n == NV);
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  // the loop bound is warp-uniform: the F_i sums below shuffle across lanes
+  for (int64_t base = int64_t(blockIdx.x) * blockDim.x + threadIdx.x - lane; base < n_pairs; base += stride) {
+    const int64_t p = base + lane;
+    const int32_t ci = p < n_pairs ? pair_center[p] : -1;
+    float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+    int32_t j = -1, self_atom = -1;
+    // the self pair carries no force of its own: the other pairs' F_i terms do
+    if (ci >= 0 && p != a.pair_off[ci]) {
+      self_atom = a.center_atom[ci];
+      const double r = a.pair_dist[p];
+      j = a.pair_j[p];
+      const int s = a.species_lut[a.types[j]];
+      const float fc = fc_cos_f(r, a.rc, a.sw), dfc = dfc_cos_f(r, a.rc, a.sw);
+      const SplinePos q = spline_pos(a.sp, r);
+      const float aa = float(q.a), bb = float(q.b);
+      const float ca = aa * aa - 1.f, cb = bb * bb - 1.f;
+      const float ea = 3.f * aa * aa - 1.f, eb = 3.f * bb * bb - 1.f;
+      const float ih = float(a.sp.inv_h);
+      const float * y0 = a.sp.yf + size_t(q.k) * W;
+      const float * d0 = a.sp.y2hf + size_t(q.k) * W;
+      const float * E = dC + size_t(ci) * Sn * K + s * n;
+      float rl[NV], pl[NV];
+      float sY = 0.f, sd0 = 0.f, sd1 = 0.f, sd2 = 0.f;
+      const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
+                  dz = float(a.pair_dir[3 * p + 2]);
+      spherical_harmonics<L, true, float>(
+          dx, dy, dz,
+          [&](int lm, float y, float gx, float gy, float gz) {
+            float A = 0.f, B = 0.f;
+            const float * El = E + lm * Sn;
+            if (vec) {
+              const float4 * E4 = reinterpret_cast<const float4 *>(El);
 #pragma unroll
-          for (int nn = 0; nn < kMaxN; ++nn) {
-            if (nn < n) {
-              const float ev = __ldg(E + nn * K + lm);
-              A += ev * pl[nn];
-              B += ev * rl[nn];
-            }
-          }
-          sY += A * y;
-          sd0 += B * gx;
-          sd1 += B * gy;
-          sd2 += B * gz;
-        },
-        [&](int l) {
+              for (int qq = 0; qq < NV / 4; ++qq) {
+                const float4 ev = __ldg(E4 + qq);
+                A += ev.x * pl[4 * qq] + ev.y * pl[4 * qq + 1] + ev.z * pl[4 * qq + 2] + ev.w * pl[4 * qq + 3];
+                B += ev.x * rl[4 * qq] + ev.y * rl[4 * qq + 1] + ev.z * rl[4 * qq + 2] + ev.w * rl[4 * qq + 3];
+              }
+            } else {
 #pragma unroll
-          for (int nn = 0; nn < kMaxN; ++nn) {
-            if (nn < n) {
-              const int c = nn * L1 + l;
-              const float yy0 = __ldg(y0 + c), yy1 = __ldg(y0 + W + c);
-              const float dd0 = __ldg(d0 + c), dd1 = __ldg(d0 + W + c);
-              const float ri = aa * (yy0 + ca * dd0) + bb * (yy1 + cb * dd1);
-              const float dri = (yy1 - yy0 - ea * dd0 + eb * dd1) * ih;
-              rl[nn] = ri;
-              pl[nn] = dri * fc + ri * dfc;
+              for (int nn = 0; nn < NV; ++nn) {
+                if (nn < n) {
+                  const float ev = __ldg(El + nn);
+                  A += ev * pl[nn];
+                  B += ev * rl[nn];
+                }
+              }
             }
-          }
-        });
-    const float fr = fc / float(r);
-    const float g0 = dx * sY + fr * sd0, g1 = dy * sY + fr * sd1, g2 = dz * sY + fr * sd2;
-    atomicAdd(&F[3 * size_t(j) + 0], -double(g0));
-    atomicAdd(&F[3 * size_t(j) + 1], -double(g1));
-    atomicAdd(&F[3 * size_t(j) + 2], -double(g2));
-    if (j != self_atom) {
-      atomicAdd(&F[3 * size_t(self_atom) + 0], double(g0));
-      atomicAdd(&F[3 * size_t(self_atom) + 1], double(g1));
-      atomicAdd(&F[3 * size_t(self_atom) + 2], double(g2));
+            sY += A * y;
+            sd0 += B * gx;
+            sd1 += B * gy;
+            sd2 += B * gz;
+          },
+          [&](int l) {
+#pragma unroll
+            for (int nn = 0; nn < NV; ++nn) {
+              if (nn < n) {
+                const int c = nn * L1 + l;
+                const float yy0 = __ldg(y0 + c), yy1 = __ldg(y0 + W + c);
+                const float dd0 = __ldg(d0 + c), dd1 = __ldg(d0 + W + c);
+                const float ri = aa * (yy0 + ca * dd0) + bb * (yy1 + cb * dd1);
+                const float dri = (yy1 - yy0 - ea * dd0 + eb * dd1) * ih;
+                rl[nn] = ri;
+                pl[nn] = dri * fc + ri * dfc;
+              } else {
+                rl[nn] = 0.f;
+                pl[nn] = 0.f;
+              }
+            }
+          });
+      const float fr = fc / float(r);
+      g0 = dx * sY + fr * sd0;
+      g1 = dy * sY + fr * sd1;
+      g2 = dz * sY + fr * sd2;
+      atomicAdd(&F[3 * size_t(j) + 0], -double(g0));
+      atomicAdd(&F[3 * size_t(j) + 1], -double(g1));
+      atomicAdd(&F[3 * size_t(j) + 2], -double(g2));
+    }
+    // F_i += g unless j is a periodic image of i: the centre's pairs are
+    // consecutive lanes, so a segmented warp scan leaves each run's sum in
+    // its last lane and one atomic per run and component remains.
+    float h0 = (j >= 0 && j != self_atom) ? g0 : 0.f;
+    float h1 = (j >= 0 && j != self_atom) ? g1 : 0.f;
+    float h2 = (j >= 0 && j != self_atom) ? g2 : 0.f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const float u0 = __shfl_up_sync(0xffffffffu, h0, off);
+      const float u1 = __shfl_up_sync(0xffffffffu, h1, off);
+      const float u2 = __shfl_up_sync(0xffffffffu, h2, off);
+      const int32_t cu = __shfl_up_sync(0xffffffffu, ci, off);
+      if (lane >= off && cu == ci) {
+        h0 += u0;
+        h1 += u1;
+        h2 += u2;
+      }
+    }
+    const int32_t cn = __shfl_down_sync(0xffffffffu, ci, 1);
+    if (ci >= 0 && (lane == 31 || cn != ci)) {
+      const int32_t ia = a.center_atom[ci];
+      atomicAdd(&F[3 * size_t(ia) + 0], double(h0));
+      atomicAdd(&F[3 * size_t(ia) + 1], double(h1));
+      atomicAdd(&F[3 * size_t(ia) + 2], double(h2));
     }
   }
 }
@@ -123,7 +169,10 @@ void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_cent
   const int grid = int(std::min<int64_t>((n_pairs + kThreads - 1) / kThreads, int64_t(148) * 64));
 #define RGPU_ADJ_CASE(LL)                                                                            \
   case LL:                                                                                           \
-    pair_adjoint_kernel<LL><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces);         \
+    if (a.fd.n <= 8)                                                                                 \
+      pair_adjoint_kernel<LL, 8><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces);    \
+    else                                                                                             \
+      pair_adjoint_kernel<LL, 16><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces);   \
     break;
   switch (a.fd.L) {
     RGPU_ADJ_CASE(0)

@@ -485,12 +485,17 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
     std::memcpy(&f, &u, 4);
     return f;
   };
-  std::vector<uint16_t> Th(T.size()), Tl(T.size());
-  for (size_t i = 0; i < T.size(); ++i) {
-    const float v = float(T[i]);
-    Th[i] = f2bf(v);
-    Tl[i] = f2bf(v - bf2f(Th[i]));
-  }
+  // the BF16 copies use the fast column order of the FP32 path (padding stays 0)
+  std::vector<int> fcol(fd.D);
+  for (int d = 0; d < fd.D; ++d) fcol[d] = fast_column(fd, d);
+  std::vector<uint16_t> Th(T.size(), 0), Tl(T.size(), 0);
+  for (int r = 0; r < m->M; ++r)
+    for (int d = 0; d < fd.D; ++d) {
+      const float v = float(T[size_t(r) * fd.Dpad + d]);
+      const size_t o = size_t(r) * fd.Dpad + fcol[d];
+      Th[o] = f2bf(v);
+      Tl[o] = f2bf(v - bf2f(Th[o]));
+    }
   std::vector<float> al32(al.size());
   for (size_t i = 0; i < al.size(); ++i) al32[i] = float(al[i]);
   std::vector<uint16_t> Tth(size_t(std::max<int64_t>(tt_total, 1)), 0), Ttl(Tth.size(), 0);
@@ -958,7 +963,15 @@ rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structure
       const void * src = ps ? s->X32.p : s->C32.p;
       RGPU_CUDA(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, s->st));
       RGPU_CUDA(cudaStreamSynchronize(s->st));
-      for (size_t i = 0; i < tmp.size(); ++i) dense[i] = tmp[i];
+      if (ps) {
+        // FP32 feature rows are in the fast column order: back to the reference's
+        std::vector<int> fcol(fd.D);
+        for (int d = 0; d < fd.D; ++d) fcol[d] = fast_column(fd, d);
+        for (int64_t r = 0; r < nc; ++r)
+          for (int d = 0; d < fd.D; ++d) dense[size_t(r) * row_len + d] = tmp[size_t(r) * row_len + fcol[d]];
+      } else {
+        for (size_t i = 0; i < tmp.size(); ++i) dense[i] = tmp[i];
+      }
     }
     auto blocks = key_blocks(calc, s, n_keys, keys);
     for (int64_t ci = 0; ci < nc; ++ci) {

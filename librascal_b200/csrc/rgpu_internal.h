@@ -181,6 +181,20 @@ void launch_expansion_selfgrad_fp64(const ExpansionArgs & a, int64_t c0, int64_t
                                     int64_t p_base, const double * dCp, double * dCs,
                                     cudaStream_t st);
 
+// Column order of the FP32 fast path's feature rows (x and its BF16 split,
+// dE/dx, and the model's BF16 copies of T): ((l*P + key)*n + n2)*n + n1, the
+// first radial index fastest. The reference's dense order, used by the FP64
+// path and by every export, is ((key*n + n1)*n + n2)*(L+1) + l
+// (property_block_sparse.hh:911-931). A dot product x . t is the same in
+// either order as long as both operands use it.
+inline int fast_column(const FeatureDims & fd, int d_ref) {
+  const int L1 = fd.L + 1, blk = fd.n * fd.n * L1;
+  const int key = d_ref / blk, r = d_ref - key * blk;
+  const int q = r / L1, l = r - q * L1;
+  const int n1 = q / fd.n, n2 = q - n1 * fd.n;
+  return ((l * fd.P + key) * fd.n + n2) * fd.n + n1;
+}
+
 struct PsArgs {
   FeatureDims fd;
   int64_t n_centers;
@@ -199,7 +213,9 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
                          int64_t p_base, const double * C, const double * X,
                          const double * inv_norm, const double * dCp, const double * dCs,
                          double * dX, cudaStream_t st);
-// Adjoint: dE/dC[i][S][n][K] from dE/dX rows (species-sorted) for all centres.
+// Adjoint: dE/dC from dE/dX rows (species-sorted) for all centres, written
+// as dC[i][lm][s*n + n'] (lm = l^2 + m; the (species, radial) index is the
+// fastest so that the centre's 32 consecutive rows store coalesced).
 // x is read back as hi + lo of its BF16 split.
 void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh,
                         const __nv_bfloat16 * Xl, const float * norm, const float * dX, float * dC,
@@ -277,7 +293,8 @@ void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, 
                                 const int64_t * pair_off, const int32_t * pair_j,
                                 const int32_t * row_of_center, const double * dX,
                                 const double * t, int64_t ldt, double * grad, cudaStream_t st);
-// Adjoint pair kernel: forces from dE/dC (FP32) and recomputed dC/dr.
+// Adjoint pair kernel: forces from dE/dC (FP32, the layout written by
+// launch_ps_bwd_fp32) and recomputed dC/dr.
 void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_center, int64_t n_pairs,
                               const float * dC, double * forces,
                               cudaStream_t st);

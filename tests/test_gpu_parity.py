@@ -164,6 +164,23 @@ def test_powerspectrum_fp64_parity(which):
     assert_features_close(Xo, X)
 
 
+@pytest.mark.parametrize("which", ["periodic_boxes", "molecule_clusters"])
+def test_powerspectrum_fp32_features(which):
+    """FP32 fast-path features, exported back into the reference's key and
+    column order, within FP32 rounding of the FP64 oracle."""
+    if which == "periodic_boxes":
+        batch, kw = synthetic.periodic_boxes(n_struct=3, seed=4), dict(rc=4.0, n=6, l=4, sigma=0.3)
+    else:
+        batch, kw = synthetic.molecule_clusters(n_struct=30, seed=3), dict(rc=5.0, n=8, l=6, sigma=0.4)
+    calc = soap(**kw)
+    al = calc.transform(rb.AtomsList(rb.StructureSet(batch)), precision="fp32")
+    species = np.unique(batch["numbers"])
+    X = al.get_features(calc, keys=calc.get_keys(species))
+    Xo = O.Run(oracle_calc(**kw), batch, species).power_spectrum()
+    assert X.shape == Xo.shape
+    assert np.abs(X - Xo).max() <= 1e-5 * np.abs(Xo).max()
+
+
 def assert_features_close(ref, test, rel=1e-10):
     """<= 1e-10 relative on every entry above 1e-6 of its row maximum; below
     that, entries are sums over m that cancel to ~1e-9 of the row scale, so an
