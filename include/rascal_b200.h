@@ -239,6 +239,27 @@ rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K,
                                    float * C_dev, float * e_dev,
                                    void * stream);
 
+/* ---------------------------------------------------------------------- */
+/* GAP energies without device allocation. No counterpart in the reference:
+ * it is the per-row energy of the mode-1 GEMM above,
+ * e_dev[r] = sum_n alpha_dev[n] (A_r . B_n)^zeta, for callers that must not
+ * allocate or free device memory during a call (cudaMalloc and cudaFree
+ * synchronise the whole device, stalling every other stream of a process
+ * that shares the GPU, such as an MD integrator's own kernels).
+ * DEVICE pointers, row-major FP32: A [M x K], B [N x K], alpha [N], e [M].
+ * All scratch lives in one static 16 MiB device array; sizes needing more
+ * (about 4 M Kp + 4 N Kp + 4 M Np + 4 M ceil(N/256) bytes, Kp = K rounded up
+ * to 64, Np = N rounded up to 32) return RGPU_ERR_CAPACITY.
+ * The first call on each device does the setup (symbol lookup, kernel
+ * attributes) and should precede any stream capture. The call is ordered on
+ * `stream` (a cudaStream_t or NULL) and returns after it completes; calls
+ * that overlap in time share the scratch and race, so callers serialise
+ * them. */
+rgpu_status rgpu_gap_energies_noalloc(int64_t M, int64_t N, int64_t K,
+                                      const float * A_dev, const float * B_dev,
+                                      const float * alpha_dev, int32_t zeta,
+                                      float * e_dev, void * stream);
+
 #ifdef __cplusplus
 }
 #endif

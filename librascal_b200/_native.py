@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "librascal_b200.so")
 RGPU_OK = 0
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
+ERR_CAPACITY = 3  # RGPU_ERR_CAPACITY
 
 _EXC_OVERFLOW = 3
 
@@ -65,6 +66,9 @@ SIGNATURES = {
     "rgpu_debug_gemm_bf16x3": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rgpu_gap_energies_noalloc": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+                                                 ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 _lib = None

@@ -31,6 +31,7 @@ SOURCES = [
     ("ps_fast.cu", [], "ps_fast"),
     ("gemm.cu", [], "gemm"),
     ("gemm_tc.cu", [], "gemm_tc"),
+    ("noalloc.cu", [], "noalloc"),
     ("adjoint.cu", [], "adjoint"),
     ("api.cu", [], "api"),
     ("radial_gto.cpp", ["-Xcompiler", "-ffp-contract=off"], "radial_gto"),

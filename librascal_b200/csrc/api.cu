@@ -1204,6 +1204,11 @@ rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K, co
   });
 }
 
+rgpu_status rgpu_gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const float * A, const float * B,
+                                      const float * alpha, int32_t zeta, float * e, void * stream) {
+  return guard([&] { gap_energies_noalloc(M, N, K, A, B, alpha, zeta, e, static_cast<cudaStream_t>(stream)); });
+}
+
 rgpu_status rgpu_synchronize(rgpu_structures * s) {
   return guard([&] { RGPU_CUDA(cudaStreamSynchronize(s->st)); });
 }

@@ -398,6 +398,37 @@ void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st) {
   cuda_check(cudaGetLastError(), "gemm_tc launch");
 }
 
+void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0) return;
+  constexpr int BN = kTcTileN, STAGES = 2;
+  const size_t smem = Smem<BN, STAGES>::TOTAL;
+  CUtensorMap a_hi = make_map(g.A_hi, g.M, g.K, g.lda, kBM);
+  CUtensorMap a_lo = make_map(g.A_lo, g.M, g.K, g.lda, kBM);
+  CUtensorMap b_hi = make_map(g.B_hi, g.N, g.K, g.ldb, BN);
+  CUtensorMap b_lo = make_map(g.B_lo, g.N, g.K, g.ldb, BN);
+  TcArgs t;
+  t.M = g.M;
+  t.N = g.N;
+  t.K = g.K;
+  t.epilogue = g.epilogue;
+  t.C = g.C;
+  t.ldc = g.ldc;
+  t.W_hi = g.W_hi;
+  t.W_lo = g.W_lo;
+  t.ldw = g.ldw;
+  t.alpha = g.alpha;
+  t.zeta = g.zeta;
+  t.e_part = g.e_part;
+  t.status = reinterpret_cast<TcStatus *>(status_dev);
+  cuda_check(cudaFuncSetAttribute(gemm_tc_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem)),
+             "cudaFuncSetAttribute(gemm_tc)");
+  dim3 grid(div_up(g.N, BN), div_up(g.M, kBM));
+  gemm_tc_kernel<BN, STAGES><<<grid, kThreads, smem, st>>>(a_hi, a_lo, b_hi, b_lo, t);
+  RGPU_LAUNCHED();
+  cuda_check(cudaGetLastError(), "gemm_tc launch");
+}
+
 int gemm_tc_timeout(bool reset) {
   TcStatus h{};
   cuda_check(cudaMemcpy(&h, tc_status(), sizeof(h), cudaMemcpyDeviceToHost), "tc status");

@@ -279,6 +279,13 @@ constexpr int kTcTileN = 256;
 void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st);
 // 0 when no bounded wait of the tcgen05 GEMM gave up, else where it did.
 int gemm_tc_timeout(bool reset);
+// gemm_bf16x3 reporting a bounded wait that gave up into the caller's device
+// word pair status_dev[0..1] (timeout flag, stage; zero on entry) instead of
+// the process-wide status word. Allocates nothing.
+void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st);
+// Allocation-free GAP energies e[r] = sum_n alpha_n (A_r . B_n)^zeta (noalloc.cu).
+void gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const float * A, const float * B,
+                          const float * alpha, int zeta, float * e, cudaStream_t st);
 // hi/lo BF16 split of a row-major FP32 matrix (columns >= cols become 0).
 void split_bf16(const float * x, int64_t rows, int64_t cols, int64_t ldx, __nv_bfloat16 * hi,
                 __nv_bfloat16 * lo, int64_t ldo, cudaStream_t st);
