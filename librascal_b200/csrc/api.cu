@@ -174,7 +174,7 @@ struct rgpu_structures {
   FeatureDims fd{};
   std::vector<int64_t> species_count;
   DevBuf row_of_center, center_of_row, species_count_d, sort_tmp, present;
-  DevBuf C64, X64, invn64, C32, X32, norm32;
+  DevBuf C64, X64, invn64, C32, X32, xscale32;  // xscale32[row] = 1/|p| (FP32 path)
   int feat_precision{-1};
   const rgpu_calculator * feat_calc{nullptr};
   bool feat_gradients{false};
@@ -370,9 +370,9 @@ void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, b
       if (need_x32) s->X32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
       s->Xh.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dpad + 64);
       s->Xl.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dpad + 64);
-      s->norm32.ensure(sizeof(float) * (nc + 1));
+      s->xscale32.ensure(sizeof(float) * (nc + 1));
       launch_ps_fwd_fp32(pa, s->C32.as<float>(), need_x32 ? s->X32.as<float>() : nullptr,
-                         s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(), s->norm32.as<float>(), s->st);
+                         s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(), s->xscale32.as<float>(), s->st);
     }
     s->feat_x32 = need_x32;
   }
@@ -599,6 +599,14 @@ void gap_plain(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * g
   mark(s, 7);
 }
 
+// Offset of species sI's energy partials ([ceil(M/256)][rows]) in epart: the
+// grouped forward GEMM writes every species' partials in one launch.
+int64_t eofs_of(const rgpu_structures * s, const rgpu_gap_model * m, int sI) {
+  int64_t o = 0;
+  for (int k = 0; k < sI; ++k) o += s->species_count[k] * ((m->segs[k].M + kTcTileN - 1) / kTcTileN);
+  return o;
+}
+
 void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_d, bool forces) {
   rgpu_calculator * c = m->calc;
   const FeatureDims & fd = s->fd;
@@ -609,7 +617,7 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
   int64_t wtot = 0, eparts = 0;
   for (int sI = 0; sI < fd.S; ++sI) {
     wtot += s->species_count[sI] * m->segs[sI].Mpad;
-    eparts = std::max<int64_t>(eparts, s->species_count[sI] * ((m->segs[sI].M + kTcTileN - 1) / kTcTileN));
+    eparts += s->species_count[sI] * ((m->segs[sI].M + kTcTileN - 1) / kTcTileN);
   }
   s->Wh.ensure(sizeof(uint16_t) * size_t(std::max<int64_t>(wtot, 1)) + 64);
   s->Wl.ensure(sizeof(uint16_t) * size_t(std::max<int64_t>(wtot, 1)) + 64);
@@ -621,6 +629,7 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
   __nv_bfloat16 * Wl = s->Wl.as<__nv_bfloat16>();
   int64_t row0 = 0, woff = 0;
   std::vector<int64_t> wofs(fd.S);
+  std::vector<Bf16x3Gemm> fwd;
   for (int sI = 0; sI < fd.S; ++sI) {
     const int64_t rows = s->species_count[sI];
     const GapSpecies & g = m->segs[sI];
@@ -642,18 +651,29 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
       a.ldw = g.Mpad;
       a.alpha = m->alpha32.as<float>() + g.m0;
       a.zeta = m->zeta;
-      a.e_part = s->epart.as<float>();
-      gemm_bf16x3(a, st);
-      const int nparts = (g.M + kTcTileN - 1) / kTcTileN;
-      launch_energy_reduce(rows, nparts, s->epart.as<float>(), rows, nullptr, row0,
-                           s->center_of_row.as<int32_t>(), s->nl.center_struct, E_d, st);
+      a.e_part = s->epart.as<float>() + eofs_of(s, m, sI);
+      a.row_scale = s->xscale32.as<float>() + row0;  // k = (p . t) / |p|
+      fwd.push_back(a);
     }
     row0 += rows;
     woff += rows * g.Mpad;
   }
+  gemm_bf16x3_grouped(fwd.data(), int(fwd.size()), st);
+  row0 = 0;
+  for (int sI = 0; sI < fd.S; ++sI) {
+    const int64_t rows = s->species_count[sI];
+    const GapSpecies & g = m->segs[sI];
+    if (rows > 0 && g.M > 0) {
+      const int nparts = (g.M + kTcTileN - 1) / kTcTileN;
+      launch_energy_reduce(rows, nparts, s->epart.as<float>() + eofs_of(s, m, sI), rows, nullptr, row0,
+                           s->center_of_row.as<int32_t>(), s->nl.center_struct, E_d, st);
+    }
+    row0 += rows;
+  }
   mark(s, 5);
   if (!forces) return;
   row0 = 0;
+  std::vector<Bf16x3Gemm> bwd;
   for (int sI = 0; sI < fd.S; ++sI) {
     const int64_t rows = s->species_count[sI];
     const GapSpecies & g = m->segs[sI];
@@ -671,12 +691,13 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
       a.epilogue = 0;
       a.C = s->dX32.as<float>() + size_t(row0) * fd.Dpad;
       a.ldc = fd.Dpad;
-      gemm_bf16x3(a, st);
+      bwd.push_back(a);
     } else if (rows > 0) {
       launch_fill_f32(s->dX32.as<float>() + size_t(row0) * fd.Dpad, rows * fd.Dpad, 0.f, st);
     }
     row0 += rows;
   }
+  gemm_bf16x3_grouped(bwd.data(), int(bwd.size()), st);
   mark(s, 6);
   PsArgs pa;
   pa.fd = fd;
@@ -684,7 +705,7 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
   pa.normalize = c->hy.normalize;
   pa.row_of_center = s->row_of_center.as<int32_t>();
   s->dC32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.nK + 64);
-  launch_ps_bwd_fp32(pa, s->C32.as<float>(), Xh, Xl, s->norm32.as<float>(), s->dX32.as<float>(),
+  launch_ps_bwd_fp32(pa, s->C32.as<float>(), Xh, Xl, s->xscale32.as<float>(), s->dX32.as<float>(),
                      s->dC32.as<float>(), st);
   mark(s, 7);
   ExpansionArgs ea = exp_args(c, s);
@@ -964,11 +985,15 @@ rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structure
       RGPU_CUDA(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, s->st));
       RGPU_CUDA(cudaStreamSynchronize(s->st));
       if (ps) {
-        // FP32 feature rows are in the fast column order: back to the reference's
+        // FP32 rows hold the unnormalised p in the fast column order: scale
+        // by 1/|p| and map back to the reference's column order
+        std::vector<float> scale(nc);
+        RGPU_CUDA(cudaMemcpy(scale.data(), s->xscale32.p, sizeof(float) * nc, cudaMemcpyDeviceToHost));
         std::vector<int> fcol(fd.D);
         for (int d = 0; d < fd.D; ++d) fcol[d] = fast_column(fd, d);
         for (int64_t r = 0; r < nc; ++r)
-          for (int d = 0; d < fd.D; ++d) dense[size_t(r) * row_len + d] = tmp[size_t(r) * row_len + fcol[d]];
+          for (int d = 0; d < fd.D; ++d)
+            dense[size_t(r) * row_len + d] = double(tmp[size_t(r) * row_len + fcol[d]] * scale[r]);
       } else {
         for (size_t i = 0; i < tmp.size(); ++i) dense[i] = tmp[i];
       }

@@ -22,6 +22,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 
@@ -66,6 +67,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t * bar, uint32_t parity) {
       : "r"(smem_u32(bar)), "r"(parity)
       : "memory");
   return ok != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t * bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 // Bounded wait: false when the limit was hit (the status word records it).
 __device__ __forceinline__ bool mbar_wait(uint64_t * bar, uint32_t parity, TcStatus * st, int where) {
@@ -143,6 +147,7 @@ struct TcArgs {
   const float * alpha;  // [N]
   int zeta;
   float * e_part;       // [gridDim.x][M]
+  const float * row_scale;  // epilogue 1: k = row_scale[row] * (A B^T) (null: 1)
   TcStatus * status;
 };
 
@@ -272,6 +277,11 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant_
           }
         } else {
           if (col >= g.ldw) continue;
+          if (g.row_scale) {
+            const float rs = __ldg(g.row_scale + row);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] *= rs;
+          }
           __align__(16) __nv_bfloat16 hi[16], lo[16];
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
@@ -297,6 +307,224 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant_
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(BN)));
+  }
+}
+
+
+// ------------------------------------------------------- grouped, persistent
+// All species' GEMMs of one direction in one launch: one CTA per SM walks a
+// tile list (group, m tile, n tile; n fastest, so CTAs running at the same
+// time share A rows in L2). The 128 x BN accumulator is double-buffered in
+// TMEM (2 x BN of the 512 columns): the MMA warp fills one buffer while the
+// epilogue warps drain the other, and the smem ring runs across tiles.
+constexpr int kMaxGroups = 16;
+
+struct TcGroup {
+  int64_t M, N, K;
+  float * C;
+  int64_t ldc;
+  __nv_bfloat16 * W_hi;
+  __nv_bfloat16 * W_lo;
+  int64_t ldw;
+  const float * alpha;
+  float * e_part;           // [n_tiles][M]
+  const float * row_scale;  // may be null
+  int64_t tile0;            // first tile of this group in the launch
+  int64_t n_tiles;          // tiles along N
+};
+
+struct TcGroupedArgs {
+  CUtensorMap a_hi[kMaxGroups], a_lo[kMaxGroups], b_hi[kMaxGroups], b_lo[kMaxGroups];
+  TcGroup grp[kMaxGroups];
+  int n_groups;
+  int epilogue;
+  int zeta;
+  int64_t n_tiles;
+  TcStatus * status;
+};
+
+__device__ __forceinline__ int find_group(const TcGroupedArgs & p, int64_t t) {
+  int g = 0;
+  while (g + 1 < p.n_groups && t >= p.grp[g + 1].tile0) ++g;
+  return g;
+}
+
+template <int BN, int STAGES>
+__global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __grid_constant__ TcGroupedArgs p) {
+  using SM = Smem<BN, STAGES>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char * base = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t * full = reinterpret_cast<uint64_t *>(base + STAGES * SM::STAGE_BYTES);
+  uint64_t * empty = full + STAGES;
+  uint64_t * tfull = empty + STAGES;  // [2] accumulator buffer written
+  uint64_t * tempty = tfull + 2;      // [2] accumulator buffer read out
+  uint64_t * done = tempty + 2;       // every MMA of this CTA finished
+  uint32_t * tmem_slot = reinterpret_cast<uint32_t *>(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  TcStatus * status = p.status;
+
+  if (warp == 0 && lane == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(done, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) {  // two accumulators: 2 BN FP32 columns x 128 lanes
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(uint32_t(2 * BN)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t it = 0;  // K blocks issued by this CTA
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
+        const int g = find_group(p, t);
+        const TcGroup & G = p.grp[g];
+        const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
+        const int m0 = int(mt * kBM), n0 = int(nt * BN);
+        const int nk = int((G.K + kBK - 1) / kBK);
+        for (int kb = 0; kb < nk; ++kb) {
+          const int s = int(it % STAGES);
+          const uint32_t ph = (it / STAGES) & 1u;
+          if (!mbar_wait(&empty[s], ph ^ 1u, status, 1)) {
+            ok = false;
+            break;
+          }
+          unsigned char * st = base + s * SM::STAGE_BYTES;
+          mbar_expect_tx(&full[s], SM::STAGE_BYTES);
+          const int kx = kb * kBK;
+          tma_load_2d(st, &p.a_hi[g], &full[s], kx, m0);
+          tma_load_2d(st + SM::A_BYTES, &p.a_lo[g], &full[s], kx, m0);
+          tma_load_2d(st + 2 * SM::A_BYTES, &p.b_hi[g], &full[s], kx, n0);
+          tma_load_2d(st + 2 * SM::A_BYTES + SM::B_BYTES, &p.b_lo[g], &full[s], kx, n0);
+          ++it;
+        }
+      }
+      // the last copies must have landed before the CTA releases its shared
+      // memory (they normally have; this matters after a timeout)
+      for (uint32_t k = it > uint32_t(STAGES) ? it - STAGES : 0u; k < it; ++k)
+        mbar_wait(&full[k % STAGES], (k / STAGES) & 1u, status, 4);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = make_idesc(kBM, BN);
+      uint32_t it = 0;
+      int i = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x, ++i) {
+        const int g = find_group(p, t);
+        const int nk = int((p.grp[g].K + kBK - 1) / kBK);
+        const int b = i & 1;
+        const uint32_t use = uint32_t(i >> 1);
+        if (!mbar_wait(&tempty[b], (use & 1u) ^ 1u, status, 5)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc = tmem + uint32_t(b * BN);
+        for (int kb = 0; kb < nk; ++kb) {
+          const int s = int(it % STAGES);
+          const uint32_t ph = (it / STAGES) & 1u;
+          if (!mbar_wait(&full[s], ph, status, 2)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          unsigned char * st = base + s * SM::STAGE_BYTES;
+          const uint32_t a_hi = smem_u32(st), a_lo = smem_u32(st + SM::A_BYTES);
+          const uint32_t b_hi = smem_u32(st + 2 * SM::A_BYTES), b_lo = smem_u32(st + 2 * SM::A_BYTES + SM::B_BYTES);
+#pragma unroll
+          for (int k = 0; k < kBK / 16; ++k) {
+            const uint32_t off = uint32_t(k) * 32u;
+            const uint32_t acc0 = (kb > 0 || k > 0) ? 1u : 0u;
+            mma_bf16(acc, smem_desc(a_lo + off), smem_desc(b_hi + off), idesc, acc0);
+            mma_bf16(acc, smem_desc(a_hi + off), smem_desc(b_lo + off), idesc, 1u);
+            mma_bf16(acc, smem_desc(a_hi + off), smem_desc(b_hi + off), idesc, 1u);
+          }
+          mma_commit(&empty[s]);
+          ++it;
+        }
+        mma_commit(&tfull[b]);  // also after a failed wait, so the epilogue moves on
+      }
+      mma_commit(done);  // completes when every MMA issued above has finished
+      mbar_wait(done, 0u, status, 6);
+    }
+  } else {
+    const int q = warp & 3;  // TMEM lane quadrant of this warp
+    int i = 0;
+    for (int64_t t = blockIdx.x; t < p.n_tiles; t += gridDim.x, ++i) {
+      const int g = find_group(p, t);
+      const TcGroup & G = p.grp[g];
+      const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
+      const int64_t m0 = mt * kBM, n0 = nt * BN;
+      const int b = i & 1;
+      const uint32_t use = uint32_t(i >> 1);
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&tfull[b], use & 1u, status, 3));
+      if (!ok) break;
+      tc_fence_after();
+      const int64_t row = m0 + q * 32 + lane;
+      const float rs = (p.epilogue == 1 && G.row_scale && row < G.M) ? __ldg(G.row_scale + row) : 1.f;
+      float e_acc = 0.f;
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(b * BN + c0), v);
+        const int64_t col = n0 + c0;
+        if (row >= G.M) continue;
+        if (p.epilogue == 0) {
+          if (col >= G.N) continue;
+          float * out = G.C + row * G.ldc + col;
+          if (col + 16 <= G.N) {
+#pragma unroll
+            for (int k = 0; k < 16; k += 4)
+              *reinterpret_cast<float4 *>(out + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+          } else {
+            for (int k = 0; k < 16; ++k)
+              if (col + k < G.N) out[k] = v[k];
+          }
+        } else {
+          if (col >= G.ldw) continue;
+          __align__(16) __nv_bfloat16 hi[16], lo[16];
+#pragma unroll
+          for (int k = 0; k < 16; ++k) {
+            const float x = v[k] * rs;
+            const float al = (col + k < G.N) ? __ldg(G.alpha + col + k) : 0.f;
+            e_acc += al * powz(x, p.zeta);
+            const float w = al * (float(p.zeta) * powz(x, p.zeta - 1));
+            hi[k] = __float2bfloat16_rn(w);
+            lo[k] = __float2bfloat16_rn(w - __bfloat162float(hi[k]));
+          }
+          uint4 * dh = reinterpret_cast<uint4 *>(G.W_hi + row * G.ldw + col);
+          uint4 * dl = reinterpret_cast<uint4 *>(G.W_lo + row * G.ldw + col);
+          dh[0] = reinterpret_cast<uint4 *>(hi)[0];
+          dh[1] = reinterpret_cast<uint4 *>(hi)[1];
+          dl[0] = reinterpret_cast<uint4 *>(lo)[0];
+          dl[1] = reinterpret_cast<uint4 *>(lo)[1];
+        }
+      }
+      if (p.epilogue == 1 && row < G.M) G.e_part[nt * G.M + row] = e_acc;
+      tc_fence_before();  // the TMEM reads above are complete before the buffer is released
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[b]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(2 * BN)));
   }
 }
 
@@ -388,6 +616,7 @@ void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st) {
   t.alpha = g.alpha;
   t.zeta = g.zeta;
   t.e_part = g.e_part;
+  t.row_scale = g.row_scale;
   t.status = tc_status();
   cuda_check(cudaFuncSetAttribute(gemm_tc_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)),
@@ -419,6 +648,7 @@ void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st)
   t.alpha = g.alpha;
   t.zeta = g.zeta;
   t.e_part = g.e_part;
+  t.row_scale = g.row_scale;
   t.status = reinterpret_cast<TcStatus *>(status_dev);
   cuda_check(cudaFuncSetAttribute(gemm_tc_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)),
@@ -427,6 +657,59 @@ void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st)
   gemm_tc_kernel<BN, STAGES><<<grid, kThreads, smem, st>>>(a_hi, a_lo, b_hi, b_lo, t);
   RGPU_LAUNCHED();
   cuda_check(cudaGetLastError(), "gemm_tc launch");
+}
+
+
+void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
+  constexpr int BN = kTcTileN, STAGES = 2;
+  TcGroupedArgs p;
+  std::memset(&p, 0, sizeof(p));
+  int ng = 0;
+  int64_t tiles = 0;
+  for (int i = 0; i < n; ++i) {
+    const Bf16x3Gemm & g = gs[i];
+    if (g.M <= 0 || g.N <= 0) continue;
+    if (ng == kMaxGroups) throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: more than 16 groups");
+    if (ng > 0 && (g.epilogue != p.epilogue || g.zeta != p.zeta))
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: groups must share the epilogue");
+    p.epilogue = g.epilogue;
+    p.zeta = g.zeta;
+    p.a_hi[ng] = make_map(g.A_hi, g.M, g.K, g.lda, kBM);
+    p.a_lo[ng] = make_map(g.A_lo, g.M, g.K, g.lda, kBM);
+    p.b_hi[ng] = make_map(g.B_hi, g.N, g.K, g.ldb, BN);
+    p.b_lo[ng] = make_map(g.B_lo, g.N, g.K, g.ldb, BN);
+    TcGroup & G = p.grp[ng];
+    G.M = g.M;
+    G.N = g.N;
+    G.K = g.K;
+    G.C = g.C;
+    G.ldc = g.ldc;
+    G.W_hi = g.W_hi;
+    G.W_lo = g.W_lo;
+    G.ldw = g.ldw;
+    G.alpha = g.alpha;
+    G.e_part = g.e_part;
+    G.row_scale = g.row_scale;
+    G.n_tiles = (g.N + BN - 1) / BN;
+    G.tile0 = tiles;
+    tiles += G.n_tiles * ((g.M + kBM - 1) / kBM);
+    ++ng;
+  }
+  if (ng == 0) return;
+  p.n_groups = ng;
+  p.n_tiles = tiles;
+  p.status = tc_status();
+  int dev = 0, sms = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  const size_t smem = Smem<BN, STAGES>::TOTAL;
+  cuda_check(cudaFuncSetAttribute(gemm_tc_grouped_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  int(smem)),
+             "cudaFuncSetAttribute(gemm_tc_grouped)");
+  const int grid = int(std::min<int64_t>(tiles, sms));
+  gemm_tc_grouped_kernel<BN, STAGES><<<grid, kThreads, smem, st>>>(p);
+  RGPU_LAUNCHED();
+  cuda_check(cudaGetLastError(), "gemm_tc_grouped launch");
 }
 
 int gemm_tc_timeout(bool reset) {

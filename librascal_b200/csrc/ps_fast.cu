@@ -1,5 +1,6 @@
-// Power spectrum, FP32 fast path: forward (x and its BF16 hi/lo split for
-// the tensor-core GEMMs) and the adjoint dE/dx -> dE/dc.
+// Power spectrum, FP32 fast path: forward (the unnormalised p as a BF16
+// hi/lo split for the tensor-core GEMMs, plus 1/|p| per row, which the GEMM
+// epilogue and the backward apply) and the adjoint dE/dx -> dE/dc.
 //
 // Same contractions as powerspectrum.cu (calculator_spherical_invariants.hh:
 // 747-794 forward, 588-652 and 796-921 for the gradient it replaces), laid
@@ -17,6 +18,7 @@ namespace rgpu {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kBwdThreads = 320;  // 16 column groups x 20 row pairs at L = 6, S n = 40
 constexpr int kMaxN = 16;  // largest max_radial of the FP32 backward
 constexpr float kSqrt2f = 1.41421356237309504880f;
 
@@ -26,6 +28,12 @@ __host__ __device__ constexpr int offp(int l) {
   int o = 0;
   for (int i = 0; i < l; ++i) o += pad4(2 * i + 1);
   return o;
+}
+// the same sum in closed form for a runtime l: blocks of l' = 2k and 2k+1
+// pad to 4(k+1) each
+__device__ __forceinline__ int offp_rt(int l) {
+  const int k = l >> 1;
+  return 4 * k * (k + 1) + ((l & 1) ? 4 * (k + 1) : 0);
 }
 // row stride of the padded layout: the block sum rounded so that stride/4
 // is odd (conflict-free 16-byte loads across 8 consecutive rows)
@@ -65,25 +73,19 @@ __device__ __forceinline__ float block_sum_f(float v, float * red) {
   return red[0];
 }
 
-// Source index (l^2 + m) of every padded column, -1 for padding.
-template <int L>
-struct PadMap {
-  int8_t src[row_stride(L)];
-  constexpr PadMap() : src() {
-    int c = 0;
-    for (int l = 0; l <= L; ++l)
-      for (int m = 0; m < pad4(2 * l + 1); ++m) src[c++] = int8_t(m < 2 * l + 1 ? l * l + m : -1);
-    for (; c < row_stride(L); ++c) src[c] = -1;
-  }
-};
-
 // Load c^i (S x n x K, K = (L+1)^2) into the padded layout.
 template <int L>
 __device__ __forceinline__ void load_padded(const float * __restrict__ Ci, float * Cp, int S, int n) {
   constexpr int K = (L + 1) * (L + 1), RS = row_stride(L);
-  constexpr PadMap<L> pm;
+  // source index l^2 + m of every padded column, -1 for padding
   __shared__ int8_t src[RS];
-  if (threadIdx.x < RS) src[threadIdx.x] = pm.src[threadIdx.x];
+  if (threadIdx.x < RS) {
+    const int c = threadIdx.x;
+    int l = 0;
+    while (l <= L && c >= offp_rt(l + 1)) ++l;
+    const int m = c - offp_rt(l);
+    src[c] = int8_t((l <= L && m < 2 * l + 1) ? l * l + m : -1);
+  }
   __syncthreads();
   for (int e = threadIdx.x; e < S * n * RS; e += blockDim.x) {
     const int row = e / RS, c = e - row * RS;
@@ -104,11 +106,14 @@ __device__ __forceinline__ float dot4(const float4 * a, const float * b) {
   return s;
 }
 
-// Output (key, n1, n2, l) goes to Ps[key * n^2 + out] with
-// out = l * P * n^2 + n2 * n + n1 (the fast column order).
+// Output (key, n1, n2, l) is column key * n^2 + out of the row, with
+// out = l * P * n^2 + n2 * n + n1 (the fast column order): the 32 lanes of a
+// warp (consecutive n1, n2) store 32 consecutive columns for every key.
+// Values are the unnormalised p; the row's 1/|p| is applied by the consumers.
 template <int L, int l>
-__device__ __forceinline__ float fwd_task(const float * Cp, float * Ps, const Keys & kt, int S, int n,
-                                          int n1, int n2, int kstride, int out) {
+__device__ __forceinline__ float fwd_task(const float * Cp, const Keys & kt, int S, int n, int n1, int n2,
+                                          int kstride, int out, float * __restrict__ X,
+                                          __nv_bfloat16 * __restrict__ Xh, __nv_bfloat16 * __restrict__ Xl) {
   constexpr int RS = row_stride(L), Q = pad4(2 * l + 1) / 4, O = offp(l);
   const float lf = rsqrtf(float(2 * l + 1));
   float ss = 0.f;
@@ -120,7 +125,11 @@ __device__ __forceinline__ float fwd_task(const float * Cp, float * Ps, const Ke
     for (int sb = sa; sb < S; ++sb) {
       float v = dot4<Q>(c1, Cp + (sb * n + n2) * RS + O) * lf;
       if (sa < sb) v *= kSqrt2f;
-      Ps[kt.kid[sa][sb] * kstride + out] = v;
+      const int pos = kt.kid[sa][sb] * kstride + out;
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      Xh[pos] = h;
+      Xl[pos] = __float2bfloat16_rn(v - __bfloat162float(h));
+      if (X) X[pos] = v;
       ss += v * v;
     }
   }
@@ -128,70 +137,58 @@ __device__ __forceinline__ float fwd_task(const float * Cp, float * Ps, const Ke
 }
 
 template <int L, int l>
-__device__ __forceinline__ float fwd_dispatch(int lrt, const float * Cp, float * Ps, const Keys & kt, int S,
-                                              int n, int n1, int n2, int kstride, int out) {
+__device__ __forceinline__ float fwd_dispatch(int lrt, const float * Cp, const Keys & kt, int S, int n, int n1,
+                                              int n2, int kstride, int out, float * X, __nv_bfloat16 * Xh,
+                                              __nv_bfloat16 * Xl) {
   if constexpr (l > L) {
     return 0.f;
   } else {
-    if (lrt == l) return fwd_task<L, l>(Cp, Ps, kt, S, n, n1, n2, kstride, out);
-    return fwd_dispatch<L, l + 1>(lrt, Cp, Ps, kt, S, n, n1, n2, kstride, out);
+    if (lrt == l) return fwd_task<L, l>(Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
+    return fwd_dispatch<L, l + 1>(lrt, Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
   }
 }
 
+// One CTA per centre: p of the centre's row as a BF16 hi/lo split (and in
+// FP32 when X is given), straight from the dot products to HBM, and the
+// row's scale 1/|p| (1 without normalisation).
 template <int L>
 __global__ void __launch_bounds__(kThreads)
 ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X,
                   __nv_bfloat16 * __restrict__ Xh, __nv_bfloat16 * __restrict__ Xl,
-                  float * __restrict__ norm_out) {
+                  float * __restrict__ row_scale) {
   constexpr int L1 = L + 1, RS = row_stride(L);
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
   const int n = fd.n, S = fd.S, nn2 = n * n, blk = nn2 * L1;
-  float * Cp = smf;                        // [S*n][RS]
-  float * Ps = Cp + size_t(S) * n * RS;    // [D], fast column order
+  float * Cp = smf;  // [S*n][RS]
   __shared__ Keys kt;
   __shared__ float red[32];
   make_keys(kt, S);
   const int64_t ci = blockIdx.x;
+  const int64_t row = a.row_of_center[ci];
   load_padded<L>(C + size_t(ci) * S * fd.nK, Cp, S, n);
   __syncthreads();
+  const size_t roff = size_t(row) * fd.Dpad;
+  float * Xr = X ? X + roff : nullptr;
+  __nv_bfloat16 * hr = Xh + roff;
+  __nv_bfloat16 * lr = Xl + roff;
   float ss = 0.f;
   for (int t = threadIdx.x; t < blk; t += blockDim.x) {
     const int l = t / nn2;
     const int r = t - l * nn2;
-    const int n2 = r / n, n1 = r - n2 * n;  // consecutive lanes: consecutive n1 and Ps words
-    ss += fwd_dispatch<L, 0>(l, Cp, Ps, kt, S, n, n1, n2, nn2, l * fd.P * nn2 + r);
+    const int n2 = r / n, n1 = r - n2 * n;  // consecutive lanes: consecutive n1 and columns
+    ss += fwd_dispatch<L, 0>(l, Cp, kt, S, n, n1, n2, nn2, l * fd.P * nn2 + r, Xr, hr, lr);
+  }
+  for (int d = fd.D + threadIdx.x; d < fd.Dpad; d += blockDim.x) {
+    hr[d] = __float2bfloat16_rn(0.f);
+    lr[d] = __float2bfloat16_rn(0.f);
+    if (Xr) Xr[d] = 0.f;
   }
   ss = block_sum_f(ss, red);
-  const float nrm = sqrtf(ss);
-  const bool do_norm = a.normalize && nrm > 0.f;
-  const float rinv = do_norm ? 1.f / nrm : 1.f;
-  const size_t roff = size_t(a.row_of_center[ci]) * fd.Dpad;
-  for (int d0 = threadIdx.x * 4; d0 < fd.Dpad; d0 += blockDim.x * 4) {
-    float v[4];
-    if (d0 + 4 <= fd.D) {
-      const float4 p = *reinterpret_cast<const float4 *>(Ps + d0);
-      v[0] = p.x;
-      v[1] = p.y;
-      v[2] = p.z;
-      v[3] = p.w;
-    } else {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) v[i] = (d0 + i < fd.D) ? Ps[d0 + i] : 0.f;
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) v[i] *= rinv;
-    if (X) *reinterpret_cast<float4 *>(X + roff + d0) = make_float4(v[0], v[1], v[2], v[3]);
-    __align__(8) __nv_bfloat16 h[4], lo[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      h[i] = __float2bfloat16_rn(v[i]);
-      lo[i] = __float2bfloat16_rn(v[i] - __bfloat162float(h[i]));
-    }
-    *reinterpret_cast<uint2 *>(Xh + roff + d0) = *reinterpret_cast<uint2 *>(h);
-    *reinterpret_cast<uint2 *>(Xl + roff + d0) = *reinterpret_cast<uint2 *>(lo);
+  if (threadIdx.x == 0) {
+    const float nrm = sqrtf(ss);
+    row_scale[row] = (a.normalize && nrm > 0.f) ? 1.f / nrm : 1.f;
   }
-  if (threadIdx.x == 0) norm_out[ci] = a.normalize ? nrm : 1.f;
 }
 
 // ---------------------------------------------------------------- backward
@@ -206,51 +203,10 @@ struct FastDiv {
 
 struct BwdShape {
   FastDiv n, P, npair, Snp;  // n, key count, n(n-1)/2, S n(n-1)/2
+  int SnP;                   // row stride of H_l: S n rounded up to even
   int LS;                    // floats per H_l block in shared memory
   bool vec;                  // n and S n multiples of 4: 16-byte stores of 4 n1
 };
-
-// dE/dc_{i l m} = lf_l sum_j H_l[i][j] c_{j l m} for one row i = (a, n1);
-// H_l is read from the transposed slot H_l[j][i], so the 32 lanes of a warp
-// (consecutive i) read 32 consecutive words while the c_j loads broadcast.
-template <int L, int l>
-__device__ __forceinline__ void bwd_task(const float * Cp, const float * Hs, int LS, int Sn, int i,
-                                         float * __restrict__ out) {
-  constexpr int RS = row_stride(L), Q = pad4(2 * l + 1) / 4, O = offp(l), M = 2 * l + 1;
-  float4 acc[Q];
-#pragma unroll
-  for (int q = 0; q < Q; ++q) acc[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-  const float * h = Hs + l * LS + i;
-  const float * cb = Cp + O;
-#pragma unroll 4
-  for (int j = 0; j < Sn; ++j) {
-    const float hv = h[j * Sn];
-    const float4 * c4 = reinterpret_cast<const float4 *>(cb + j * RS);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      const float4 c = c4[q];
-      acc[q].x += hv * c.x;
-      acc[q].y += hv * c.y;
-      acc[q].z += hv * c.z;
-      acc[q].w += hv * c.w;
-    }
-  }
-  const float lf = rsqrtf(float(M));
-  const float * av = reinterpret_cast<const float *>(acc);
-#pragma unroll
-  for (int m = 0; m < M; ++m) out[(l * l + m) * Sn + i] = av[m] * lf;
-}
-
-template <int L, int l>
-__device__ __forceinline__ void bwd_dispatch(int lrt, const float * Cp, const float * Hs, int LS, int Sn, int i,
-                                             float * out) {
-  if constexpr (l <= L) {
-    if (lrt == l)
-      bwd_task<L, l>(Cp, Hs, LS, Sn, i, out);
-    else
-      bwd_dispatch<L, l + 1>(lrt, Cp, Hs, LS, Sn, i, out);
-  }
-}
 
 // One CTA per centre. The projected gradient G = (g - x (x.g)) / |p| (x as
 // BF16 hi + lo, g = dE/dx, both in the fast column order) is formed in two
@@ -260,19 +216,33 @@ __device__ __forceinline__ void bwd_dispatch(int lrt, const float * Cp, const fl
 //   H_l[(a n1)][(a n2)] = G(n1 n2 l) + G(n2 n1 l)
 // then each thread computes one (l, row) of dE/dc = lf_l H_l c_l.
 template <int L>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kBwdThreads, 4)
 ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
-                  const __nv_bfloat16 * __restrict__ Xl, const float * __restrict__ norm,
+                  const __nv_bfloat16 * __restrict__ Xl, const float * __restrict__ row_scale,
                   const float * __restrict__ dX, float * __restrict__ dC) {
   constexpr int L1 = L + 1, RS = row_stride(L), K = L1 * L1;
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
-  const int n = fd.n, S = fd.S, Sn = S * n, LS = bs.LS, P = fd.P;
+  const int n = fd.n, S = fd.S, Sn = S * n, SnP = bs.SnP, LS = bs.LS, P = fd.P;
   float * Cp = smf;             // [Sn][RS]
-  float * Hs = Cp + Sn * RS;    // H_l[j][i] at l*LS + j*Sn + i
+  float * Hs = Cp + Sn * RS;    // H_l[j][i] at l*LS + j*SnP + i
   __shared__ Keys kt;
   __shared__ float red[32];
   __shared__ int8_t pair_n1[kMaxN * (kMaxN - 1) / 2], pair_n2[kMaxN * (kMaxN - 1) / 2];
+  // column groups of the contraction: every 4-wide chunk q of every padded
+  // l-block, l descending; group g covers padded columns grp_off[g] + 0..3
+  constexpr int kG = offp(L + 1) / 4;
+  __shared__ int8_t grp_l[kG];
+  __shared__ int16_t grp_off[kG];
+  if (threadIdx.x < kG) {
+    int g = threadIdx.x, l = L;
+    while (g >= pad4(2 * l + 1) / 4) {
+      g -= pad4(2 * l + 1) / 4;
+      --l;
+    }
+    grp_l[threadIdx.x] = int8_t(l);
+    grp_off[threadIdx.x] = int16_t(offp_rt(l) + 4 * g);
+  }
   make_keys(kt, S);
   if (threadIdx.x < n * n) {
     const int n1 = threadIdx.x / n, n2 = threadIdx.x - n1 * n;
@@ -289,6 +259,7 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
   const uint2 * xl = reinterpret_cast<const uint2 *>(Xl + size_t(row) * fd.Dpad);
   const float4 * g4 = reinterpret_cast<const float4 *>(dX + size_t(row) * fd.Dpad);
   const int nq = (fd.D + 3) >> 2;
+  const float rs = row_scale[row];  // x = rs * p; G = rs * (g - x (x.g))
   float dot = 0.f;
   if (a.normalize) {
     for (int c = threadIdx.x; c < nq; c += blockDim.x) {
@@ -301,9 +272,8 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
       dot += (__bfloat162float(hb[2]) + __bfloat162float(lb[2])) * gq.z;
       dot += (__bfloat162float(hb[3]) + __bfloat162float(lb[3])) * gq.w;
     }
-    dot = block_sum_f(dot, red);  // padding columns are zero in x and g
+    dot = block_sum_f(dot, red) * rs;  // padding columns are zero in p and g
   }
-  const float invn = 1.f / norm[ci];
   for (int c = threadIdx.x; c < nq; c += blockDim.x) {
     const uint2 hv = __ldcs(xh + c), lv = __ldcs(xl + c);
     const float4 gq = __ldcs(g4 + c);
@@ -312,7 +282,7 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
     const float gv[4] = {gq.x, gq.y, gq.z, gq.w};
     float G[4];
 #pragma unroll
-    for (int e = 0; e < 4; ++e) G[e] = (gv[e] - (__bfloat162float(hb[e]) + __bfloat162float(lb[e])) * dot) * invn;
+    for (int e = 0; e < 4; ++e) G[e] = (gv[e] - (__bfloat162float(hb[e]) + __bfloat162float(lb[e])) * rs * dot) * rs;
     // decode the first column of the chunk: ((l*P + key)*n + n2)*n + n1
     const uint32_t d0 = 4u * uint32_t(c);
     const uint32_t q1 = bs.n.div(d0);
@@ -332,14 +302,14 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
         float v[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) v[e] = kSqrt2f * G[e];
-        *reinterpret_cast<float4 *>(Hl + j * Sn + i) = make_float4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<float4 *>(Hl + j * SnP + i) = make_float4(v[0], v[1], v[2], v[3]);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) Hl[(i + e) * Sn + j] = v[e];
+        for (int e = 0; e < 4; ++e) Hl[(i + e) * SnP + j] = v[e];
       } else {
         float v[4];
 #pragma unroll
         for (int e = 0; e < 4; ++e) v[e] = (n1 + e == n2) ? 2.f * G[e] : G[e];
-        *reinterpret_cast<float4 *>(Hl + j * Sn + i) = make_float4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<float4 *>(Hl + j * SnP + i) = make_float4(v[0], v[1], v[2], v[3]);
       }
     } else {
 #pragma unroll
@@ -349,10 +319,10 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
           const int i = sa * n + n1, j = sb * n + n2;
           float * Hl = Hs + l * LS;
           if (sa != sb) {
-            Hl[j * Sn + i] = kSqrt2f * G[e];
-            Hl[i * Sn + j] = kSqrt2f * G[e];
+            Hl[j * SnP + i] = kSqrt2f * G[e];
+            Hl[i * SnP + j] = kSqrt2f * G[e];
           } else {
-            Hl[j * Sn + i] = (n1 == n2) ? 2.f * G[e] : G[e];
+            Hl[j * SnP + i] = (n1 == n2) ? 2.f * G[e] : G[e];
           }
         }
         if (++n1 == n) {
@@ -378,21 +348,55 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
     const int p = int(r - sa * bs.npair.d);
     const int i = int(sa) * n + pair_n1[p], j = int(sa) * n + pair_n2[p];
     float * Hl = Hs + l * LS;
-    const float s = Hl[j * Sn + i] + Hl[i * Sn + j];
-    Hl[j * Sn + i] = s;
-    Hl[i * Sn + j] = s;
+    const float s = Hl[j * SnP + i] + Hl[i * SnP + j];
+    Hl[j * SnP + i] = s;
+    Hl[i * SnP + j] = s;
   }
   __syncthreads();
+  // dE/dc_{i l m} = lf_l sum_j H_l[i][j] c_{j l m}: each task is one pair of
+  // rows (2ip, 2ip+1) and one 4-wide column group (l, q). H_l is read from
+  // the transposed slots H_l[j][2ip..2ip+1] (consecutive lanes: consecutive
+  // 8-byte words), c_j from the broadcast 16-byte chunk of the padded tile.
   float * out = dC + size_t(ci) * Sn * K;
-  for (int t = threadIdx.x; t < L1 * Sn; t += blockDim.x) {
-    const int lr = t / Sn;
-    bwd_dispatch<L, 0>(L - lr, Cp, Hs, LS, Sn, t - lr * Sn, out);
+  const int NP = (Sn + 1) >> 1;
+  for (int t = threadIdx.x; t < kG * NP; t += blockDim.x) {
+    const int g = t / NP;
+    const int ip = t - g * NP;
+    const int l = grp_l[g];
+    const float * h = Hs + l * LS + 2 * ip;
+    const float * cb = Cp + grp_off[g];
+    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
+#pragma unroll 4
+    for (int j = 0; j < Sn; ++j) {
+      const float2 hv = *reinterpret_cast<const float2 *>(h + j * SnP);
+      const float4 c = *reinterpret_cast<const float4 *>(cb + j * RS);
+      a0.x += hv.x * c.x;
+      a0.y += hv.x * c.y;
+      a0.z += hv.x * c.z;
+      a0.w += hv.x * c.w;
+      a1.x += hv.y * c.x;
+      a1.y += hv.y * c.y;
+      a1.z += hv.y * c.z;
+      a1.w += hv.y * c.w;
+    }
+    const int M = 2 * l + 1, m0 = grp_off[g] - offp_rt(l);
+    const float lf = rsqrtf(float(M));
+    const float v0[4] = {a0.x, a0.y, a0.z, a0.w}, v1[4] = {a1.x, a1.y, a1.z, a1.w};
+    const int i = 2 * ip;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (m0 + e < M) {
+        float * o = out + (l * l + m0 + e) * Sn + i;
+        o[0] = v0[e] * lf;
+        if (i + 1 < Sn) o[1] = v1[e] * lf;
+      }
+    }
   }
 }
 
 template <int L>
 size_t fwd_smem(const FeatureDims & fd) {
-  return sizeof(float) * (size_t(fd.S) * fd.n * row_stride(L) + fd.D + 4);
+  return sizeof(float) * size_t(fd.S) * fd.n * row_stride(L);
 }
 
 BwdShape bwd_shape(const FeatureDims & fd) {
@@ -403,9 +407,10 @@ BwdShape bwd_shape(const FeatureDims & fd) {
   b.npair = FastDiv(npair > 0 ? npair : 1u);
   b.Snp = FastDiv(npair > 0 ? uint32_t(fd.S) * npair : 1u);
   if (npair == 0) b.Snp.d = 0;  // no off-diagonal pairs: the symmetrisation loop is empty
+  b.SnP = int(Sn + (Sn & 1u));
   // a multiple of 4 (16-byte rows) that is not a multiple of 32, so the
   // L+1 blocks start on different banks
-  b.LS = int((Sn * Sn + 3) / 4 * 4);
+  b.LS = int((Sn * uint32_t(b.SnP) + 3) / 4 * 4);
   if (b.LS % 32 == 0) b.LS += 4;
   b.vec = (n % 4 == 0) && (Sn % 4 == 0);
   return b;
@@ -419,7 +424,7 @@ size_t bwd_smem(const FeatureDims & fd, const BwdShape & b) {
 }  // namespace
 
 void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
-                        __nv_bfloat16 * Xl, float * norm, cudaStream_t st) {
+                        __nv_bfloat16 * Xl, float * row_scale, cudaStream_t st) {
   if (a.n_centers == 0) return;
   if (!Xh || !Xl) throw Error(RGPU_ERR_INVALID_ARGUMENT, "FP32 power spectrum needs the BF16 outputs");
 #define RGPU_PSF_CASE(LL)                                                                                     \
@@ -427,7 +432,7 @@ void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloa
     const size_t smem = fwd_smem<LL>(a.fd);                                                                   \
     RGPU_CUDA(cudaFuncSetAttribute(ps_fwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
-    ps_fwd_f32_kernel<LL><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, Xh, Xl, norm);                 \
+    ps_fwd_f32_kernel<LL><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, Xh, Xl, row_scale);                 \
     break;                                                                                                    \
   }
   switch (a.fd.L) {
@@ -453,7 +458,7 @@ void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloa
 }
 
 void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh, const __nv_bfloat16 * Xl,
-                        const float * norm, const float * dX, float * dC, cudaStream_t st) {
+                        const float * row_scale, const float * dX, float * dC, cudaStream_t st) {
   if (a.n_centers == 0) return;
   if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
   const BwdShape bs = bwd_shape(a.fd);
@@ -466,7 +471,7 @@ void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 *
                   "species x max_radial too large for the FP32 power-spectrum backward; use FP64");           \
     RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
-    ps_bwd_f32_kernel<LL><<<int(a.n_centers), kThreads, smem, st>>>(a, bs, C, Xh, Xl, norm, dX, dC);          \
+    ps_bwd_f32_kernel<LL><<<int(a.n_centers), kBwdThreads, smem, st>>>(a, bs, C, Xh, Xl, row_scale, dX, dC);          \
     break;                                                                                                    \
   }
   switch (a.fd.L) {

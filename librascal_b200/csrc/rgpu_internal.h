@@ -204,9 +204,11 @@ struct PsArgs {
 // X rows (normalised) and inverse norms.
 void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double * inv_norm,
                         cudaStream_t st);
-// FP32 forward: X (FP32, may be null) and/or its BF16 hi/lo split (may be null).
+// FP32 forward: rows of the unnormalised p (fast column order) as a BF16
+// hi/lo split, optionally also in FP32 (X may be null), and row_scale[row] =
+// 1/|p| (1 without normalisation); x = row_scale * p.
 void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
-                        __nv_bfloat16 * Xl, float * norm, cudaStream_t st);
+                        __nv_bfloat16 * Xl, float * row_scale, cudaStream_t st);
 // Plain-path gradients of the normalised power spectrum for pairs of centres
 // [c0,c1): dX[p - p_base][3][D].
 void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, int64_t c1,
@@ -216,9 +218,9 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
 // Adjoint: dE/dC from dE/dX rows (species-sorted) for all centres, written
 // as dC[i][lm][s*n + n'] (lm = l^2 + m; the (species, radial) index is the
 // fastest so that the centre's 32 consecutive rows store coalesced).
-// x is read back as hi + lo of its BF16 split.
+// x is read back as row_scale * (hi + lo) of the forward's BF16 split.
 void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh,
-                        const __nv_bfloat16 * Xl, const float * norm, const float * dX, float * dC,
+                        const __nv_bfloat16 * Xl, const float * row_scale, const float * dX, float * dC,
                         cudaStream_t st);
 
 // ------------------------------------------------------------------ GAP
@@ -256,7 +258,8 @@ void gemm_tf32(const Tf32GemmArgs & g, cudaStream_t st);
 // A_lo B_hi), FP32 accumulation in TMEM. A [M x K] and B [N x K] are
 // row-major hi/lo BF16 pairs (row strides lda, ldb; 16-byte aligned).
 // epilogue 0: C [M x ldc] FP32; epilogue 1: GAP forward (W_hi/W_lo
-// [M x ldw] BF16, zero for columns >= N; e_part [ceil(N/256)][M]).
+// [M x ldw] BF16, zero for columns >= N; e_part [ceil(N/256)][M]) on
+// k = row_scale[r] (A B^T)[r] when row_scale is given.
 struct Bf16x3Gemm {
   int64_t M, N, K;
   const __nv_bfloat16 * A_hi;
@@ -274,9 +277,13 @@ struct Bf16x3Gemm {
   const float * alpha;
   int zeta;
   float * e_part;
+  const float * row_scale;
 };
 constexpr int kTcTileN = 256;
 void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st);
+// Several GEMMs of the same epilogue kind (up to 16; K may differ) in one
+// persistent launch with a double-buffered TMEM accumulator.
+void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st);
 // 0 when no bounded wait of the tcgen05 GEMM gave up, else where it did.
 int gemm_tc_timeout(bool reset);
 // gemm_bf16x3 reporting a bounded wait that gave up into the caller's device
