@@ -143,7 +143,7 @@ void parse_hypers(const std::string & kind, const std::string & text, Hypers & h
 struct rgpu_calculator {
   Hypers hy;
   RadialSpline spline;
-  DevBuf grid, y, y2h, yf, y2hf, center;
+  DevBuf grid, y, y2h, yf, y2hf, q4f, center;
   SplineDev dev{};
 };
 
@@ -363,7 +363,7 @@ void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, b
       launch_ps_fwd_fp64(pa, s->C64.as<double>(), s->X64.as<double>(), s->invn64.as<double>(), s->st);
     }
   } else {
-    s->C32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.nK + 64);
+    s->C32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.n * row_stride(fd.L) + 64);
     launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), s->st);
     mark(s, 3);
     if (c->hy.kind == "sphericalinvariants") {
@@ -747,6 +747,17 @@ static void calculator_to_device(rgpu_calculator * c) {
       yf[i] = float(sp.y[i]);
       y2hf[i] = float(sp.y2h[i]);
     }
+    // interval table of the FP32 path: one 16-byte load per channel
+    const size_t W = size_t(sp.width);
+    std::vector<float> q4(size_t(std::max(sp.grid_size - 1, 1)) * W * 4, 0.f);
+    for (int k = 0; k + 1 < sp.grid_size; ++k)
+      for (size_t c = 0; c < W; ++c) {
+        float * o = &q4[(size_t(k) * W + c) * 4];
+        o[0] = yf[size_t(k) * W + c];
+        o[1] = y2hf[size_t(k) * W + c];
+        o[2] = yf[size_t(k + 1) * W + c];
+        o[3] = y2hf[size_t(k + 1) * W + c];
+      }
     std::vector<double> center(sp.center.size());
     for (size_t i = 0; i < center.size(); ++i) center[i] = sp.center[i] / std::sqrt(4.0 * kPi);
     auto put = [](DevBuf & b, const void * src, size_t bytes) {
@@ -758,12 +769,14 @@ static void calculator_to_device(rgpu_calculator * c) {
     put(c->y2h, sp.y2h.data(), sizeof(double) * GW);
     put(c->yf, yf.data(), sizeof(float) * GW);
     put(c->y2hf, y2hf.data(), sizeof(float) * GW);
+    put(c->q4f, q4.data(), sizeof(float) * q4.size());
     put(c->center, center.data(), sizeof(double) * center.size());
     c->dev.grid = c->grid.as<double>();
     c->dev.y = c->y.as<double>();
     c->dev.y2h = c->y2h.as<double>();
     c->dev.yf = c->yf.as<float>();
     c->dev.y2hf = c->y2hf.as<float>();
+    c->dev.q4f = c->q4f.as<float4>();
     c->dev.x1 = sp.x1;
     c->dev.h = sp.h;
     c->dev.inv_h = 1.0 / sp.h;
@@ -980,7 +993,9 @@ rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structure
       RGPU_CUDA(cudaMemcpyAsync(dense.data(), src, sizeof(double) * dense.size(), cudaMemcpyDeviceToHost, s->st));
       RGPU_CUDA(cudaStreamSynchronize(s->st));
     } else {
-      std::vector<float> tmp(dense.size());
+      // FP32 expansion rows are padded ([S*n][row_stride(L)])
+      const size_t rs = size_t(row_stride(fd.L));
+      std::vector<float> tmp(ps ? dense.size() : size_t(nc) * fd.S * fd.n * rs);
       const void * src = ps ? s->X32.p : s->C32.p;
       RGPU_CUDA(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, s->st));
       RGPU_CUDA(cudaStreamSynchronize(s->st));
@@ -995,7 +1010,12 @@ rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structure
           for (int d = 0; d < fd.D; ++d)
             dense[size_t(r) * row_len + d] = double(tmp[size_t(r) * row_len + fcol[d]] * scale[r]);
       } else {
-        for (size_t i = 0; i < tmp.size(); ++i) dense[i] = tmp[i];
+        for (int64_t r = 0; r < nc; ++r)
+          for (int row = 0; row < fd.S * fd.n; ++row)
+            for (int l = 0; l <= fd.L; ++l)
+              for (int m = 0; m < 2 * l + 1; ++m)
+                dense[size_t(r) * row_len + size_t(row) * fd.K + l * l + m] =
+                    tmp[(size_t(r) * fd.S * fd.n + row) * rs + offp(l) + m];
       }
     }
     auto blocks = key_blocks(calc, s, n_keys, keys);

@@ -211,6 +211,29 @@ __device__ __forceinline__ void spherical_harmonics(T x, T y, T z, Emit && emit,
 // Cubic-spline evaluation of the radial table at r: index search with the
 // reference's points-per-unit quirk (math/interpolator.cc:214-230), value and
 // derivative formulas of math/interpolator.cc:177-212.
+// Padded coefficient layout of the FP32 path: each l-block of 2l+1 values
+// is padded to a multiple of 4 floats, so every product over m is a few
+// 16-byte loads. Rows ((species, n) pairs) are row_stride(L) floats apart.
+__host__ __device__ constexpr int pad4(int x) { return (x + 3) & ~3; }
+// padded offset of block l: sum_{l' < l} pad4(2l'+1)
+__host__ __device__ constexpr int offp(int l) {
+  int o = 0;
+  for (int i = 0; i < l; ++i) o += pad4(2 * i + 1);
+  return o;
+}
+// the same sum in closed form for a runtime l: blocks of l' = 2k and 2k+1
+// pad to 4(k+1) each
+__host__ __device__ __forceinline__ int offp_rt(int l) {
+  const int k = l >> 1;
+  return 4 * k * (k + 1) + ((l & 1) ? 4 * (k + 1) : 0);
+}
+// row stride of the padded layout: the block sum rounded so that stride/4
+// is odd (conflict-free 16-byte loads across 8 consecutive rows)
+__host__ __device__ constexpr int row_stride(int L) {
+  int s = offp(L + 1);
+  return ((s / 4) % 2 == 1) ? s : s + 4;
+}
+
 struct SplinePos {
   int k;
   double a, b;

@@ -185,6 +185,140 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
   }
 }
 
+
+#ifndef RGPU_PART_FP64
+// FP32 fast path. The same sums, organised for throughput instead of the
+// reference's accumulation order (the FP64 kernel above keeps that order):
+//   (a) lanes = pairs: f_c, the spline interval and Y_lm of one pair each;
+//   (b) lanes = radial channels: f_c RI_c(r_p) for the chunk's pairs one
+//       after the other, one 16-byte load of the interval table per channel;
+//   (c) lanes = lm, n accumulators each (NV >= n registers): per pair of a
+//       species one Y_lm load feeds the n radial products; the sums are
+//       written once into the padded row layout [S*n][row_stride(L)].
+template <int L, int NV>
+__global__ void __launch_bounds__(kWarps * 32)
+expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restrict__ present) {
+  constexpr int K = (L + 1) * (L + 1);
+  constexpr int L1 = L + 1;
+  constexpr int RS = row_stride(L), NPAD = RS - K;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int W = a.fd.W, S = a.fd.S, n = a.fd.n;
+  float * RIf = reinterpret_cast<float *>(smem_raw) + size_t(wid) * (W + K) * kPad;  // [W][kPad]
+  float * Y = RIf + W * kPad;                                                         // [K][kPad]
+  __shared__ float pa_s[kWarps][32], pb_s[kWarps][32], fc_s[kWarps][32];
+  __shared__ int pk_s[kWarps][32];
+  __shared__ uint8_t order_s[kWarps][32];
+  __shared__ uint8_t lofk[K];
+  __shared__ int16_t colk[K];     // padded column of lm: offp(l) + m
+  __shared__ int16_t padc[NPAD];  // the padding columns of a row
+  for (int lm = threadIdx.x; lm < K; lm += blockDim.x) {
+    int l = 0;
+    while ((l + 1) * (l + 1) <= lm) ++l;
+    lofk[lm] = uint8_t(l);
+    colk[lm] = int16_t(offp_rt(l) + (lm - l * l));
+  }
+  if (threadIdx.x == 0) {
+    int j = 0;
+    for (int l = 0; l <= L; ++l)
+      for (int c = 2 * l + 1; c < pad4(2 * l + 1); ++c) padc[j++] = int16_t(offp_rt(l) + c);
+    for (int c = offp(L + 1); c < RS; ++c) padc[j++] = int16_t(c);
+  }
+  __syncthreads();
+  for (int64_t ci = int64_t(blockIdx.x) * kWarps + wid; ci < a.n_centers;
+       ci += int64_t(gridDim.x) * kWarps) {
+    float * Ci = C + size_t(ci) * S * n * RS;
+    const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
+    const int ti = a.species_lut[a.types[a.center_atom[ci]]];
+    uint32_t mask_all = 1u << ti;
+    for (int j = lane; j < NPAD; j += 32) {
+      const int c = padc[j];
+      for (int row = 0; row < S * n; ++row) Ci[row * RS + c] = 0.f;
+    }
+    bool first = true;
+    for (int64_t p0 = p_lo; p0 < p_hi || first; p0 += 32) {
+      const int np = int(max(int64_t(0), min(int64_t(32), p_hi - p0)));
+      int my_sp = 31;
+      if (lane < np) {
+        const int64_t p = p0 + lane;
+        const double r = a.pair_dist[p];
+        my_sp = a.species_lut[a.types[a.pair_j[p]]];
+        const SplinePos q = spline_pos(a.sp, r);
+        pk_s[wid][lane] = q.k;
+        pa_s[wid][lane] = float(q.a);
+        pb_s[wid][lane] = float(q.b);
+        fc_s[wid][lane] = float(fc_cos(r, a.rc, a.sw));
+        const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
+                    dz = float(a.pair_dir[3 * p + 2]);
+        spherical_harmonics<L, false, float>(dx, dy, dz, [&](int lm, float y, float, float, float) {
+          Y[lm * kPad + lane] = y;
+        });
+      }
+      // stable order of the chunk's pairs by species
+      int before = 0;
+      unsigned my_mask = 0;
+      for (int s = 0; s < S; ++s) {
+        unsigned m = __ballot_sync(0xffffffffu, my_sp == s);
+        if (my_sp == s) my_mask = m;
+        if (s < my_sp) before += __popc(m);
+        if (m) mask_all |= 1u << s;
+      }
+      if (lane < np) order_s[wid][before + __popc(my_mask & lanemask_lt())] = uint8_t(lane);
+      __syncwarp();
+      for (int q = 0; q < np; ++q) {
+        const float fa = pa_s[wid][q], fb = pb_s[wid][q], f = fc_s[wid][q];
+        const float ca = fa * fa - 1.f, cb = fb * fb - 1.f;
+        const float4 * row = a.sp.q4f + size_t(pk_s[wid][q]) * W;
+        for (int c = lane; c < W; c += 32) {
+          const float4 t = __ldg(row + c);
+          RIf[c * kPad + q] = f * (fa * (t.x + ca * t.y) + fb * (t.z + cb * t.w));
+        }
+      }
+      __syncwarp();
+      int start = 0;
+      for (int s = 0; s < S; ++s) {
+        const int cnt = __popc(__ballot_sync(0xffffffffu, my_sp == s));
+        if (cnt > 0 || first) {
+          float * Cs = Ci + size_t(s) * n * RS;
+          for (int lm = lane; lm < K; lm += 32) {
+            const float * ri = RIf + lofk[lm] * kPad;  // row nn*L1 + l at + nn*L1*kPad
+            const float * yy = Y + lm * kPad;
+            float acc[NV];
+#pragma unroll
+            for (int nn = 0; nn < NV; ++nn) acc[nn] = 0.f;
+            for (int q = 0; q < cnt; ++q) {
+              const int pl = order_s[wid][start + q];
+              const float y = yy[pl];
+#pragma unroll
+              for (int nn = 0; nn < NV; ++nn)
+                if (nn < n) acc[nn] += ri[nn * L1 * kPad + pl] * y;
+            }
+            float * dst = Cs + colk[lm];
+#pragma unroll
+            for (int nn = 0; nn < NV; ++nn) {
+              if (nn < n) {
+                if (first) {
+                  // centre contribution (calculator_spherical_expansion.hh:2244-2247)
+                  if (s == ti && lm == 0) acc[nn] += float(a.center_contrib[nn]);
+                  dst[nn * RS] = acc[nn];
+                } else {
+                  dst[nn * RS] += acc[nn];
+                }
+              }
+            }
+          }
+        }
+        start += cnt;
+      }
+      __syncwarp();
+      first = false;
+    }
+    if (lane == 0) present[ci] = mask_all;
+    __syncwarp();
+  }
+}
+#endif
+
 // Plain path: grad_j c^i for every non-self pair of centres [c0, c1); each
 // lane streams its pair's 3 x n x K block.
 template <int L>
@@ -294,6 +428,51 @@ void launch_exp(const ExpansionArgs & a, T * C, uint32_t * present, cudaStream_t
   RGPU_CUDA(cudaGetLastError());
 }
 
+#ifndef RGPU_PART_FP64
+void launch_exp_f32(const ExpansionArgs & a, float * C, uint32_t * present, cudaStream_t st) {
+  if (a.n_centers == 0) return;
+  if (a.fd.n > 16) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
+  sph_constants_tu();
+  const size_t smem = size_t(kWarps) * (a.fd.W + a.fd.K) * kPad * sizeof(float);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int grid = int(std::min<int64_t>((a.n_centers + kWarps - 1) / kWarps, int64_t(sms) * 16));
+#define RGPU_EXP_CASE(LL)                                                                   \
+  case LL:                                                                                  \
+    if (a.fd.n <= 8) {                                                                      \
+      RGPU_CUDA(cudaFuncSetAttribute(expansion_f32_kernel<LL, 8>,                           \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+      expansion_f32_kernel<LL, 8><<<grid, kWarps * 32, smem, st>>>(a, C, present);          \
+    } else {                                                                                \
+      RGPU_CUDA(cudaFuncSetAttribute(expansion_f32_kernel<LL, 16>,                          \
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
+      expansion_f32_kernel<LL, 16><<<grid, kWarps * 32, smem, st>>>(a, C, present);         \
+    }                                                                                       \
+    break;
+  switch (a.fd.L) {
+    RGPU_EXP_CASE(0)
+    RGPU_EXP_CASE(1)
+    RGPU_EXP_CASE(2)
+    RGPU_EXP_CASE(3)
+    RGPU_EXP_CASE(4)
+    RGPU_EXP_CASE(5)
+    RGPU_EXP_CASE(6)
+    RGPU_EXP_CASE(7)
+    RGPU_EXP_CASE(8)
+    RGPU_EXP_CASE(9)
+    RGPU_EXP_CASE(10)
+    RGPU_EXP_CASE(11)
+    RGPU_EXP_CASE(12)
+    default:
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
+  }
+#undef RGPU_EXP_CASE
+  RGPU_LAUNCHED();
+  RGPU_CUDA(cudaGetLastError());
+}
+#endif
+
 }  // namespace
 
 // The library compiles this file twice: RGPU_PART_FP64 (with --fmad=false, so
@@ -307,7 +486,7 @@ void launch_expansion_fp64(const ExpansionArgs & a, double * C, uint32_t * prese
 #ifndef RGPU_PART_FP64
 void launch_expansion_fp32(const ExpansionArgs & a, float * C, uint32_t * present,
                            cudaStream_t st) {
-  launch_exp<float>(a, C, present, st);
+  launch_exp_f32(a, C, present, st);
 }
 #endif
 

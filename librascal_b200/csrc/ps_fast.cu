@@ -22,26 +22,6 @@ constexpr int kBwdThreads = 320;  // 16 column groups x 20 row pairs at L = 6, S
 constexpr int kMaxN = 16;  // largest max_radial of the FP32 backward
 constexpr float kSqrt2f = 1.41421356237309504880f;
 
-__host__ __device__ constexpr int pad4(int x) { return (x + 3) & ~3; }
-// padded offset of block l: sum_{l' < l} pad4(2l'+1)
-__host__ __device__ constexpr int offp(int l) {
-  int o = 0;
-  for (int i = 0; i < l; ++i) o += pad4(2 * i + 1);
-  return o;
-}
-// the same sum in closed form for a runtime l: blocks of l' = 2k and 2k+1
-// pad to 4(k+1) each
-__device__ __forceinline__ int offp_rt(int l) {
-  const int k = l >> 1;
-  return 4 * k * (k + 1) + ((l & 1) ? 4 * (k + 1) : 0);
-}
-// row stride of the padded layout: the block sum rounded so that stride/4
-// is odd (conflict-free 16-byte loads across 8 consecutive rows)
-__host__ __device__ constexpr int row_stride(int L) {
-  int s = offp(L + 1);
-  return ((s / 4) % 2 == 1) ? s : s + 4;
-}
-
 struct Keys {
   int8_t ka[kMaxSpecies * (kMaxSpecies + 1) / 2];
   int8_t kb[kMaxSpecies * (kMaxSpecies + 1) / 2];
@@ -73,25 +53,16 @@ __device__ __forceinline__ float block_sum_f(float v, float * red) {
   return red[0];
 }
 
-// Load c^i (S x n x K, K = (L+1)^2) into the padded layout.
+// Copy c^i, already in the padded row layout [S*n][row_stride(L)] of the
+// FP32 expansion, into shared memory. Starts with a barrier so that tables
+// the block wrote before are visible afterwards.
 template <int L>
 __device__ __forceinline__ void load_padded(const float * __restrict__ Ci, float * Cp, int S, int n) {
-  constexpr int K = (L + 1) * (L + 1), RS = row_stride(L);
-  // source index l^2 + m of every padded column, -1 for padding
-  __shared__ int8_t src[RS];
-  if (threadIdx.x < RS) {
-    const int c = threadIdx.x;
-    int l = 0;
-    while (l <= L && c >= offp_rt(l + 1)) ++l;
-    const int m = c - offp_rt(l);
-    src[c] = int8_t((l <= L && m < 2 * l + 1) ? l * l + m : -1);
-  }
+  constexpr int RS = row_stride(L);
   __syncthreads();
-  for (int e = threadIdx.x; e < S * n * RS; e += blockDim.x) {
-    const int row = e / RS, c = e - row * RS;
-    const int s = src[c];
-    Cp[e] = (s >= 0) ? Ci[row * K + s] : 0.f;
-  }
+  const float4 * src = reinterpret_cast<const float4 *>(Ci);
+  float4 * dst = reinterpret_cast<float4 *>(Cp);
+  for (int e = threadIdx.x; e < S * n * (RS / 4); e += blockDim.x) dst[e] = __ldg(src + e);
 }
 
 template <int Q>
@@ -166,7 +137,7 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
   make_keys(kt, S);
   const int64_t ci = blockIdx.x;
   const int64_t row = a.row_of_center[ci];
-  load_padded<L>(C + size_t(ci) * S * fd.nK, Cp, S, n);
+  load_padded<L>(C + size_t(ci) * S * n * RS, Cp, S, n);
   __syncthreads();
   const size_t roff = size_t(row) * fd.Dpad;
   float * Xr = X ? X + roff : nullptr;
@@ -254,7 +225,7 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
   }
   const int64_t ci = blockIdx.x;
   const int64_t row = a.row_of_center[ci];
-  load_padded<L>(C + size_t(ci) * S * fd.nK, Cp, S, n);
+  load_padded<L>(C + size_t(ci) * S * n * RS, Cp, S, n);
   const uint2 * xh = reinterpret_cast<const uint2 *>(Xh + size_t(row) * fd.Dpad);
   const uint2 * xl = reinterpret_cast<const uint2 *>(Xl + size_t(row) * fd.Dpad);
   const float4 * g4 = reinterpret_cast<const float4 *>(dX + size_t(row) * fd.Dpad);

@@ -77,6 +77,7 @@ struct SplineDev {
   const double * y2h;  // [G][W]
   const float * yf;
   const float * y2hf;
+  const float4 * q4f;  // [G-1][W]: (y_k, y2h_k, y_k+1, y2h_k+1) of interval k, FP32
   double x1, h, inv_h, ppu;
   int search_size, W;
 };
@@ -170,6 +171,8 @@ struct ExpansionArgs {
 // C[i][S][n][K] and the per-centre species presence bitmask.
 void launch_expansion_fp64(const ExpansionArgs & a, double * C, uint32_t * present,
                            cudaStream_t st);
+// FP32: C[i][S*n][row_stride(L)], each l-block padded to 4 floats (zeros in
+// the padding; common.cuh), and the presence bitmask.
 void launch_expansion_fp32(const ExpansionArgs & a, float * C, uint32_t * present,
                            cudaStream_t st);
 // Plain-path pair gradients for centres [c0,c1): dCp[p - p_base][3][n][K]
