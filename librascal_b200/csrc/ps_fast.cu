@@ -9,6 +9,8 @@
 // product over m is a few 16-byte loads; work items are ordered with l
 // slowest, so a warp shares l (uniform trip counts, broadcast loads) and the
 // dot products are unrolled per l.
+#include <algorithm>
+
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -119,9 +121,63 @@ __device__ __forceinline__ float fwd_dispatch(int lrt, const float * Cp, const K
   }
 }
 
-// One CTA per centre: p of the centre's row as a BF16 hi/lo split (and in
-// FP32 when X is given), straight from the dot products to HBM, and the
-// row's scale 1/|p| (1 without normalisation).
+// Two consecutive radial indices n1, n1+1 (n1 even) of one (l, n2): each
+// c_b load feeds both dot products, and the two outputs are consecutive
+// columns, stored as packed bf16 pairs (4-byte stores).
+template <int L, int l>
+__device__ __forceinline__ float fwd_task2(const float * Cp, const Keys & kt, int S, int n, int n1, int n2,
+                                           int kstride, int out, float * __restrict__ X,
+                                           __nv_bfloat16 * __restrict__ Xh, __nv_bfloat16 * __restrict__ Xl) {
+  constexpr int RS = row_stride(L), Q = pad4(2 * l + 1) / 4, O = offp(l);
+  const float lf = rsqrtf(float(2 * l + 1));
+  float ss = 0.f;
+  for (int sa = 0; sa < S; ++sa) {
+    float4 ca[Q], cb[Q];
+    const float4 * pa = reinterpret_cast<const float4 *>(Cp + (sa * n + n1) * RS + O);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      ca[q] = pa[q];
+      cb[q] = pa[q + RS / 4];
+    }
+    for (int sb = sa; sb < S; ++sb) {
+      const float4 * p2 = reinterpret_cast<const float4 *>(Cp + (sb * n + n2) * RS + O);
+      float va = 0.f, vb = 0.f;
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const float4 y = p2[q];
+        va += ca[q].x * y.x + ca[q].y * y.y + ca[q].z * y.z + ca[q].w * y.w;
+        vb += cb[q].x * y.x + cb[q].y * y.y + cb[q].z * y.z + cb[q].w * y.w;
+      }
+      const float sc = (sa < sb) ? lf * kSqrt2f : lf;
+      va *= sc;
+      vb *= sc;
+      const int pos = kt.kid[sa][sb] * kstride + out;
+      const __nv_bfloat162 hh = __floats2bfloat162_rn(va, vb);
+      const float2 hf = __bfloat1622float2(hh);
+      *reinterpret_cast<__nv_bfloat162 *>(Xh + pos) = hh;
+      *reinterpret_cast<__nv_bfloat162 *>(Xl + pos) = __floats2bfloat162_rn(va - hf.x, vb - hf.y);
+      if (X) *reinterpret_cast<float2 *>(X + pos) = make_float2(va, vb);
+      ss += va * va + vb * vb;
+    }
+  }
+  return ss;
+}
+
+template <int L, int l>
+__device__ __forceinline__ float fwd_dispatch2(int lrt, const float * Cp, const Keys & kt, int S, int n, int n1,
+                                               int n2, int kstride, int out, float * X, __nv_bfloat16 * Xh,
+                                               __nv_bfloat16 * Xl) {
+  if constexpr (l > L) {
+    return 0.f;
+  } else {
+    if (lrt == l) return fwd_task2<L, l>(Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
+    return fwd_dispatch2<L, l + 1>(lrt, Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
+  }
+}
+
+// p of a centre's row as a BF16 hi/lo split (and in FP32 when X is given),
+// straight from the dot products to HBM, and the row's scale 1/|p| (1
+// without normalisation). Persistent: each block loops over centres.
 template <int L>
 __global__ void __launch_bounds__(kThreads)
 ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X,
@@ -135,30 +191,43 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
   __shared__ Keys kt;
   __shared__ float red[32];
   make_keys(kt, S);
-  const int64_t ci = blockIdx.x;
-  const int64_t row = a.row_of_center[ci];
-  load_padded<L>(C + size_t(ci) * S * n * RS, Cp, S, n);
-  __syncthreads();
-  const size_t roff = size_t(row) * fd.Dpad;
-  float * Xr = X ? X + roff : nullptr;
-  __nv_bfloat16 * hr = Xh + roff;
-  __nv_bfloat16 * lr = Xl + roff;
-  float ss = 0.f;
-  for (int t = threadIdx.x; t < blk; t += blockDim.x) {
-    const int l = t / nn2;
-    const int r = t - l * nn2;
-    const int n2 = r / n, n1 = r - n2 * n;  // consecutive lanes: consecutive n1 and columns
-    ss += fwd_dispatch<L, 0>(l, Cp, kt, S, n, n1, n2, nn2, l * fd.P * nn2 + r, Xr, hr, lr);
-  }
-  for (int d = fd.D + threadIdx.x; d < fd.Dpad; d += blockDim.x) {
-    hr[d] = __float2bfloat16_rn(0.f);
-    lr[d] = __float2bfloat16_rn(0.f);
-    if (Xr) Xr[d] = 0.f;
-  }
-  ss = block_sum_f(ss, red);
-  if (threadIdx.x == 0) {
-    const float nrm = sqrtf(ss);
-    row_scale[row] = (a.normalize && nrm > 0.f) ? 1.f / nrm : 1.f;
+  const bool paired = (n % 2) == 0;
+  const int half = n / 2;
+  for (int64_t ci = blockIdx.x; ci < a.n_centers; ci += gridDim.x) {
+    const int64_t row = a.row_of_center[ci];
+    load_padded<L>(C + size_t(ci) * S * n * RS, Cp, S, n);
+    __syncthreads();
+    const size_t roff = size_t(row) * fd.Dpad;
+    float * Xr = X ? X + roff : nullptr;
+    __nv_bfloat16 * hr = Xh + roff;
+    __nv_bfloat16 * lr = Xl + roff;
+    float ss = 0.f;
+    if (paired) {
+      // tasks (l, n2, n1 pair): consecutive lanes store consecutive pairs
+      for (int t = threadIdx.x; t < L1 * n * half; t += blockDim.x) {
+        const int l = t / (n * half);
+        const int r = t - l * (n * half);
+        const int n2 = r / half, n1 = 2 * (r - n2 * half);
+        ss += fwd_dispatch2<L, 0>(l, Cp, kt, S, n, n1, n2, nn2, l * fd.P * nn2 + n2 * n + n1, Xr, hr, lr);
+      }
+    } else {
+      for (int t = threadIdx.x; t < blk; t += blockDim.x) {
+        const int l = t / nn2;
+        const int r = t - l * nn2;
+        const int n2 = r / n, n1 = r - n2 * n;  // consecutive lanes: consecutive n1 and columns
+        ss += fwd_dispatch<L, 0>(l, Cp, kt, S, n, n1, n2, nn2, l * fd.P * nn2 + r, Xr, hr, lr);
+      }
+    }
+    for (int d = fd.D + threadIdx.x; d < fd.Dpad; d += blockDim.x) {
+      hr[d] = __float2bfloat16_rn(0.f);
+      lr[d] = __float2bfloat16_rn(0.f);
+      if (Xr) Xr[d] = 0.f;
+    }
+    ss = block_sum_f(ss, red);  // ends with a barrier: Cp may be refilled
+    if (threadIdx.x == 0) {
+      const float nrm = sqrtf(ss);
+      row_scale[row] = (a.normalize && nrm > 0.f) ? 1.f / nrm : 1.f;
+    }
   }
 }
 
@@ -223,7 +292,8 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
       pair_n2[p] = int8_t(n2);
     }
   }
-  const int64_t ci = blockIdx.x;
+  // persistent: the tables above serve every centre of this block
+  for (int64_t ci = blockIdx.x; ci < a.n_centers; ci += gridDim.x) {
   const int64_t row = a.row_of_center[ci];
   load_padded<L>(C + size_t(ci) * S * n * RS, Cp, S, n);
   const uint2 * xh = reinterpret_cast<const uint2 *>(Xh + size_t(row) * fd.Dpad);
@@ -363,6 +433,7 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
       }
     }
   }
+  }
 }
 
 template <int L>
@@ -392,6 +463,17 @@ size_t bwd_smem(const FeatureDims & fd, const BwdShape & b) {
   return sizeof(float) * (size_t(fd.S) * fd.n * row_stride(L) + size_t(L + 1) * b.LS);
 }
 
+// Blocks of a persistent kernel: as many as fit on the device at once (at
+// most one per centre).
+template <class Kern>
+int persistent_grid(Kern k, int threads, size_t smem, int64_t n_centers) {
+  int dev = 0, sms = 0, per_sm = 0;
+  RGPU_CUDA(cudaGetDevice(&dev));
+  RGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  RGPU_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, smem));
+  return int(std::max<int64_t>(1, std::min<int64_t>(n_centers, int64_t(sms) * std::max(per_sm, 1))));
+}
+
 }  // namespace
 
 void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
@@ -403,7 +485,8 @@ void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloa
     const size_t smem = fwd_smem<LL>(a.fd);                                                                   \
     RGPU_CUDA(cudaFuncSetAttribute(ps_fwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
-    ps_fwd_f32_kernel<LL><<<int(a.n_centers), kThreads, smem, st>>>(a, C, X, Xh, Xl, row_scale);                 \
+    ps_fwd_f32_kernel<LL><<<persistent_grid(ps_fwd_f32_kernel<LL>, kThreads, smem, a.n_centers), kThreads,   \
+                            smem, st>>>(a, C, X, Xh, Xl, row_scale);                                          \
     break;                                                                                                    \
   }
   switch (a.fd.L) {
@@ -442,7 +525,8 @@ void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 *
                   "species x max_radial too large for the FP32 power-spectrum backward; use FP64");           \
     RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
-    ps_bwd_f32_kernel<LL><<<int(a.n_centers), kBwdThreads, smem, st>>>(a, bs, C, Xh, Xl, row_scale, dX, dC);          \
+    ps_bwd_f32_kernel<LL><<<persistent_grid(ps_bwd_f32_kernel<LL>, kBwdThreads, smem, a.n_centers),           \
+                            kBwdThreads, smem, st>>>(a, bs, C, Xh, Xl, row_scale, dX, dC);                    \
     break;                                                                                                    \
   }
   switch (a.fd.L) {
