@@ -106,6 +106,24 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   d |= uint64_t(2) << 61;            // 128-byte swizzle
   return d;
 }
+// The same descriptor for a K block of BK bf16 per row: 128-byte rows with
+// the 128-byte swizzle (BK = 64) or 64-byte rows with the 64-byte swizzle
+// (BK = 32, 8-row groups 512 bytes apart; layout type 4).
+template <int BK>
+__device__ __forceinline__ uint64_t smem_desc_k(uint32_t addr) {
+  static_assert(BK == 64 || BK == 32, "K block of 32 or 64 bf16");
+  if constexpr (BK == 64) {
+    return smem_desc(addr);
+  } else {
+    uint64_t d = 0;
+    d |= uint64_t((addr >> 4) & 0x3FFF);
+    d |= uint64_t(1) << 16;
+    d |= uint64_t(512 >> 4) << 32;
+    d |= uint64_t(1) << 46;
+    d |= uint64_t(4) << 61;
+    return d;
+  }
+}
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
@@ -151,10 +169,10 @@ struct TcArgs {
   TcStatus * status;
 };
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int BK = kBK>
 struct Smem {
-  static constexpr int A_BYTES = kBM * kBK * 2;  // 16 KB
-  static constexpr int B_BYTES = BN * kBK * 2;
+  static constexpr int A_BYTES = kBM * BK * 2;  // 16 KB at BK = 64
+  static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int TOTAL = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 };
@@ -349,9 +367,9 @@ __device__ __forceinline__ int find_group(const TcGroupedArgs & p, int64_t t) {
   return g;
 }
 
-template <int BN, int STAGES>
+template <int BN, int STAGES, int BK>
 __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __grid_constant__ TcGroupedArgs p) {
-  using SM = Smem<BN, STAGES>;
+  using SM = Smem<BN, STAGES, BK>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char * base = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -395,7 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         const TcGroup & G = p.grp[g];
         const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
         const int m0 = int(mt * kBM), n0 = int(nt * BN);
-        const int nk = int((G.K + kBK - 1) / kBK);
+        const int nk = int((G.K + BK - 1) / BK);
         for (int kb = 0; kb < nk; ++kb) {
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1u;
@@ -405,7 +423,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
           }
           unsigned char * st = base + s * SM::STAGE_BYTES;
           mbar_expect_tx(&full[s], SM::STAGE_BYTES);
-          const int kx = kb * kBK;
+          const int kx = kb * BK;
           tma_load_2d(st, &p.a_hi[g], &full[s], kx, m0);
           tma_load_2d(st + SM::A_BYTES, &p.a_lo[g], &full[s], kx, m0);
           tma_load_2d(st + 2 * SM::A_BYTES, &p.b_hi[g], &full[s], kx, n0);
@@ -426,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
       bool ok = true;
       for (int64_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x, ++i) {
         const int g = find_group(p, t);
-        const int nk = int((p.grp[g].K + kBK - 1) / kBK);
+        const int nk = int((p.grp[g].K + BK - 1) / BK);
         const int b = i & 1;
         const uint32_t use = uint32_t(i >> 1);
         if (!mbar_wait(&tempty[b], (use & 1u) ^ 1u, status, 5)) {
@@ -447,12 +465,12 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
           const uint32_t a_hi = smem_u32(st), a_lo = smem_u32(st + SM::A_BYTES);
           const uint32_t b_hi = smem_u32(st + 2 * SM::A_BYTES), b_lo = smem_u32(st + 2 * SM::A_BYTES + SM::B_BYTES);
 #pragma unroll
-          for (int k = 0; k < kBK / 16; ++k) {
+          for (int k = 0; k < BK / 16; ++k) {
             const uint32_t off = uint32_t(k) * 32u;
             const uint32_t acc0 = (kb > 0 || k > 0) ? 1u : 0u;
-            mma_bf16(acc, smem_desc(a_lo + off), smem_desc(b_hi + off), idesc, acc0);
-            mma_bf16(acc, smem_desc(a_hi + off), smem_desc(b_lo + off), idesc, 1u);
-            mma_bf16(acc, smem_desc(a_hi + off), smem_desc(b_hi + off), idesc, 1u);
+            mma_bf16(acc, smem_desc_k<BK>(a_lo + off), smem_desc_k<BK>(b_hi + off), idesc, acc0);
+            mma_bf16(acc, smem_desc_k<BK>(a_hi + off), smem_desc_k<BK>(b_lo + off), idesc, 1u);
+            mma_bf16(acc, smem_desc_k<BK>(a_hi + off), smem_desc_k<BK>(b_hi + off), idesc, 1u);
           }
           mma_commit(&empty[s]);
           ++it;
@@ -549,17 +567,19 @@ EncodeFn encode_fn() {
 // 2D bf16 tensor map over a row-major [rows x cols] matrix with row stride
 // ld elements; box = box_rows x 64 columns, 128-byte swizzle, zero fill
 // outside the matrix.
-CUtensorMap make_map(const __nv_bfloat16 * ptr, int64_t rows, int64_t cols, int64_t ld, int box_rows) {
+CUtensorMap make_map(const __nv_bfloat16 * ptr, int64_t rows, int64_t cols, int64_t ld, int box_rows,
+                     int box_k = kBK) {
   if ((reinterpret_cast<uintptr_t>(ptr) & 15) != 0 || (ld * 2) % 16 != 0)
     throw Error(RGPU_ERR_INVALID_ARGUMENT, "tensor map: base or stride not 16-byte aligned");
   CUtensorMap m;
   std::memset(&m, 0, sizeof(m));
   cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
   cuuint64_t strides[1] = {cuuint64_t(ld * 2)};
-  cuuint32_t box[2] = {cuuint32_t(kBK), cuuint32_t(box_rows)};
+  cuuint32_t box[2] = {cuuint32_t(box_k), cuuint32_t(box_rows)};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(ptr), dims, strides,
-                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           box_k == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw Error(RGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
   return m;
@@ -661,7 +681,8 @@ void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st)
 
 
 void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
-  constexpr int BN = kTcTileN, STAGES = 2;
+  // K blocks of 32 bf16 (64-byte swizzle): 4 stages of 48 KB in flight
+  constexpr int BN = kTcTileN, STAGES = 4, BK = 32;
   TcGroupedArgs p;
   std::memset(&p, 0, sizeof(p));
   int ng = 0;
@@ -674,10 +695,11 @@ void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
       throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: groups must share the epilogue");
     p.epilogue = g.epilogue;
     p.zeta = g.zeta;
-    p.a_hi[ng] = make_map(g.A_hi, g.M, g.K, g.lda, kBM);
-    p.a_lo[ng] = make_map(g.A_lo, g.M, g.K, g.lda, kBM);
-    p.b_hi[ng] = make_map(g.B_hi, g.N, g.K, g.ldb, BN);
-    p.b_lo[ng] = make_map(g.B_lo, g.N, g.K, g.ldb, BN);
+    if (g.K % BK != 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: K must be a multiple of 32");
+    p.a_hi[ng] = make_map(g.A_hi, g.M, g.K, g.lda, kBM, BK);
+    p.a_lo[ng] = make_map(g.A_lo, g.M, g.K, g.lda, kBM, BK);
+    p.b_hi[ng] = make_map(g.B_hi, g.N, g.K, g.ldb, BN, BK);
+    p.b_lo[ng] = make_map(g.B_lo, g.N, g.K, g.ldb, BN, BK);
     TcGroup & G = p.grp[ng];
     G.M = g.M;
     G.N = g.N;
@@ -702,12 +724,12 @@ void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
   int dev = 0, sms = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-  const size_t smem = Smem<BN, STAGES>::TOTAL;
-  cuda_check(cudaFuncSetAttribute(gemm_tc_grouped_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  int(smem)),
+  const size_t smem = Smem<BN, STAGES, BK>::TOTAL;
+  cuda_check(cudaFuncSetAttribute(gemm_tc_grouped_kernel<BN, STAGES, BK>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
              "cudaFuncSetAttribute(gemm_tc_grouped)");
   const int grid = int(std::min<int64_t>(tiles, sms));
-  gemm_tc_grouped_kernel<BN, STAGES><<<grid, kThreads, smem, st>>>(p);
+  gemm_tc_grouped_kernel<BN, STAGES, BK><<<grid, kThreads, smem, st>>>(p);
   RGPU_LAUNCHED();
   cuda_check(cudaGetLastError(), "gemm_tc_grouped launch");
 }
