@@ -167,7 +167,9 @@ struct rgpu_structures {
   double nl_cutoff{-1};
   NlWork nlw;
   NlOutputs nl;
-  std::vector<int64_t> pair_off_h;
+  std::vector<int64_t> pair_off_h;  // host copy of nl.pair_off, made on demand
+  bool pair_off_h_valid{false};
+  std::vector<int> batch_species;   // sorted atom types present in the batch
   // layout and features
   std::vector<int> species;  // dense layout (sorted)
   DevBuf lut;
@@ -240,6 +242,29 @@ void upload(rgpu_structures * s, DevBuf & dst, const void * src, size_t bytes) {
   RGPU_CUDA(cudaMemcpyAsync(dst.p, p, bytes, cudaMemcpyHostToDevice, s->st));
 }
 
+// Several host -> device copies through one pass of the staging buffer: a
+// single wait for the previous use of the buffer, then one copy per array.
+struct Upload {
+  DevBuf * dst;
+  const void * src;
+  size_t bytes;
+};
+void upload_many(rgpu_structures * s, const std::vector<Upload> & ups) {
+  size_t total = 0;
+  for (const Upload & u : ups) total += (u.bytes + 255) & ~size_t(255);
+  for (const Upload & u : ups) u.dst->ensure(u.bytes);
+  if (total == 0) return;
+  RGPU_CUDA(cudaStreamSynchronize(s->st));  // staging buffer reuse
+  unsigned char * base = static_cast<unsigned char *>(staging(s, total));
+  size_t off = 0;
+  for (const Upload & u : ups) {
+    if (u.bytes == 0) continue;
+    std::memcpy(base + off, u.src, u.bytes);
+    RGPU_CUDA(cudaMemcpyAsync(u.dst->p, base + off, u.bytes, cudaMemcpyHostToDevice, s->st));
+    off += (u.bytes + 255) & ~size_t(255);
+  }
+}
+
 void mark(rgpu_structures * s, int i) {
   if (s->timed) RGPU_CUDA(cudaEventRecord(s->ev[i], s->st));
 }
@@ -260,7 +285,7 @@ FeatureDims make_dims(const Hypers & hy, int S) {
 
 // Choose the dense species layout: batch species plus `extra`.
 void set_layout(rgpu_structures * s, const Hypers & hy, const std::vector<int> & extra) {
-  std::set<int> sp(s->types.begin(), s->types.end());
+  std::set<int> sp(s->batch_species.begin(), s->batch_species.end());
   sp.insert(extra.begin(), extra.end());
   std::vector<int> species(sp.begin(), sp.end());
   if (int(species.size()) > kMaxSpecies)
@@ -291,13 +316,23 @@ void build_nl(rgpu_structures * s, double cutoff) {
   in.center_off = s->center_off_d.as<int64_t>();
   in.atom_struct = s->atom_struct_d.as<int32_t>();
   build_neighbour_list(in, cutoff, s->nlw, s->nl, s->status_d, s->status_h, s->st);
-  s->pair_off_h.resize(s->nl.n_centers + 1);
-  RGPU_CUDA(cudaMemcpyAsync(s->pair_off_h.data(), s->nl.pair_off, sizeof(int64_t) * (s->nl.n_centers + 1),
-                            cudaMemcpyDeviceToHost, s->st));
-  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  s->pair_off_h_valid = false;
   s->nl_valid = true;
   s->nl_cutoff = cutoff;
   s->feat_valid = false;
+}
+
+// Host copy of the neighbour list's centre offsets (for chunking the plain
+// path's gradient passes).
+const std::vector<int64_t> & pair_offsets_host(rgpu_structures * s) {
+  if (!s->pair_off_h_valid) {
+    s->pair_off_h.resize(s->nl.n_centers + 1);
+    RGPU_CUDA(cudaMemcpyAsync(s->pair_off_h.data(), s->nl.pair_off, sizeof(int64_t) * (s->nl.n_centers + 1),
+                              cudaMemcpyDeviceToHost, s->st));
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    s->pair_off_h_valid = true;
+  }
+  return s->pair_off_h;
 }
 
 ExpansionArgs exp_args(const rgpu_calculator * c, const rgpu_structures * s) {
@@ -571,18 +606,19 @@ void gap_plain(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * g
   pa.n_centers = nc;
   pa.normalize = c->hy.normalize;
   pa.row_of_center = s->row_of_center.as<int32_t>();
+  const std::vector<int64_t> & poff = pair_offsets_host(s);
   int64_t c0 = 0;
   while (c0 < nc) {
     int64_t c1 = c0;
     size_t bytes = 0;
     while (c1 < nc) {
-      size_t add = per_pair * size_t(s->pair_off_h[c1 + 1] - s->pair_off_h[c1]) + per_center;
+      size_t add = per_pair * size_t(poff[c1 + 1] - poff[c1]) + per_center;
       if (c1 > c0 && bytes + add > budget) break;
       bytes += add;
       ++c1;
     }
-    const int64_t p_base = s->pair_off_h[c0];
-    const int64_t np = s->pair_off_h[c1] - p_base;
+    const int64_t p_base = poff[c0];
+    const int64_t np = poff[c1] - p_base;
     s->dCp.ensure(sizeof(double) * size_t(np) * 3 * fd.nK + 64);
     s->dCs.ensure(per_center * size_t(c1 - c0) + 64);
     s->dXp.ensure(sizeof(double) * size_t(np) * 3 * fd.D + 64);
@@ -845,9 +881,15 @@ rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const
     s->n_atoms = s->atom_off[n_structures];
     if (s->n_atoms > (int64_t(1) << 31) - 1) throw Error(RGPU_ERR_INVALID_ARGUMENT, "too many atoms");
     s->types.assign(numbers, numbers + s->n_atoms);
-    for (int64_t a = 0; a < s->n_atoms; ++a)
+    bool seen[130] = {false};
+    for (int64_t a = 0; a < s->n_atoms; ++a) {
       if (s->types[a] < 0 || s->types[a] >= 130)
         throw Error(RGPU_ERR_STRUCTURE, "atom types (or atomic numbers) should be in the range [0, 130].");
+      seen[s->types[a]] = true;
+    }
+    s->batch_species.clear();
+    for (int z = 0; z < 130; ++z)
+      if (seen[z]) s->batch_species.push_back(z);
     s->has_mask = false;
     if (center_mask)
       for (int64_t a = 0; a < s->n_atoms; ++a)
@@ -873,15 +915,17 @@ rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const
           if (!center_mask[a]) tag2idx[t++] = int32_t(a);
       }
     }
-    upload(s, s->atom_off_d, s->atom_off.data(), sizeof(int64_t) * (n_structures + 1));
-    upload(s, s->pos_d, positions, sizeof(double) * 3 * s->n_atoms);
-    upload(s, s->types_d, numbers, sizeof(int32_t) * s->n_atoms);
-    upload(s, s->cells_d, cells, sizeof(double) * 9 * n_structures);
-    upload(s, s->pbc_d, pbc, sizeof(int32_t) * 3 * n_structures);
-    upload(s, s->ncent_d, ncent.data(), sizeof(int32_t) * n_structures);
-    upload(s, s->center_off_d, s->center_off_h.data(), sizeof(int64_t) * (n_structures + 1));
-    upload(s, s->atom_struct_d, astruct.data(), sizeof(int32_t) * s->n_atoms);
-    if (s->has_mask) upload(s, s->tag2idx_d, tag2idx.data(), sizeof(int32_t) * s->n_atoms);
+    std::vector<Upload> ups = {
+        {&s->atom_off_d, s->atom_off.data(), sizeof(int64_t) * (n_structures + 1)},
+        {&s->pos_d, positions, sizeof(double) * 3 * s->n_atoms},
+        {&s->types_d, numbers, sizeof(int32_t) * s->n_atoms},
+        {&s->cells_d, cells, sizeof(double) * 9 * n_structures},
+        {&s->pbc_d, pbc, sizeof(int32_t) * 3 * n_structures},
+        {&s->ncent_d, ncent.data(), sizeof(int32_t) * n_structures},
+        {&s->center_off_d, s->center_off_h.data(), sizeof(int64_t) * (n_structures + 1)},
+        {&s->atom_struct_d, astruct.data(), sizeof(int32_t) * s->n_atoms}};
+    if (s->has_mask) ups.push_back({&s->tag2idx_d, tag2idx.data(), sizeof(int32_t) * s->n_atoms});
+    upload_many(s, ups);
     s->nl_valid = false;
     s->feat_valid = false;
   });
@@ -1054,18 +1098,19 @@ rgpu_status rgpu_get_features_gradient(const rgpu_calculator * calc, const rgpu_
     const size_t per_center = sizeof(double) * size_t(fd.S) * 3 * fd.nK;
     const size_t budget = size_t(4) << 30;
     std::vector<double> host;
+    const std::vector<int64_t> & poff = pair_offsets_host(s);
     int64_t c0 = 0;
     while (c0 < nc) {
       int64_t c1 = c0;
       size_t bytes = 0;
       while (c1 < nc) {
-        size_t add = per_pair * size_t(s->pair_off_h[c1 + 1] - s->pair_off_h[c1]) + per_center;
+        size_t add = per_pair * size_t(poff[c1 + 1] - poff[c1]) + per_center;
         if (c1 > c0 && bytes + add > budget) break;
         bytes += add;
         ++c1;
       }
-      const int64_t p_base = s->pair_off_h[c0];
-      const int64_t np = s->pair_off_h[c1] - p_base;
+      const int64_t p_base = poff[c0];
+      const int64_t np = poff[c1] - p_base;
       s->dCp.ensure(sizeof(double) * size_t(np) * 3 * fd.nK + 64);
       s->dCs.ensure(per_center * size_t(c1 - c0) + 64);
       s->dXp.ensure(sizeof(double) * size_t(np) * 3 * fd.D + 64);
@@ -1165,15 +1210,15 @@ rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precis
                                           std::to_string(where) + ")");
     }
     if (energies) {
-      // baseline (models/krr.py:68-90) on the host, FP64
-      std::map<int, double> sc;
-      for (size_t i = 0; i < m->species.size(); ++i) sc[m->species[i]] = m->self_contrib[i];
+      // baseline (models/krr.py:68-90) on the host, FP64: a table over the
+      // atom types (validated to [0, 130) by rgpu_structures_set)
+      double sc[130] = {0.};
+      for (size_t i = 0; i < m->species.size(); ++i)
+        if (m->species[i] >= 0 && m->species[i] < 130) sc[m->species[i]] = m->self_contrib[i];
+      const int32_t * types = s->types.data();
       for (int st = 0; st < s->n_struct; ++st) {
         double y0 = 0.;
-        for (int64_t a = s->atom_off[st]; a < s->atom_off[st + 1]; ++a) {
-          auto it = sc.find(s->types[a]);
-          if (it != sc.end()) y0 += it->second;
-        }
+        for (int64_t a = s->atom_off[st]; a < s->atom_off[st + 1]; ++a) y0 += sc[types[a]];
         energies[st] += y0;
       }
     }
