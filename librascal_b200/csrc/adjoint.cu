@@ -71,8 +71,8 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
       const float ca = aa * aa - 1.f, cb = bb * bb - 1.f;
       const float ea = 3.f * aa * aa - 1.f, eb = 3.f * bb * bb - 1.f;
       const float ih = float(a.sp.inv_h);
-      const float * y0 = a.sp.yf + size_t(q.k) * W;
-      const float * d0 = a.sp.y2hf + size_t(q.k) * W;
+      // interval k of the spline: (y_k, y2h_k, y_k+1, y2h_k+1) per channel
+      const float4 * q4 = a.sp.q4f + size_t(q.k) * W;
       const float * E = dC + size_t(ci) * Sn * K + s * n;
       float rl[NV], pl[NV];
       float sY = 0.f, sd0 = 0.f, sd1 = 0.f, sd2 = 0.f;
@@ -110,11 +110,9 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
 #pragma unroll
             for (int nn = 0; nn < NV; ++nn) {
               if (nn < n) {
-                const int c = nn * L1 + l;
-                const float yy0 = __ldg(y0 + c), yy1 = __ldg(y0 + W + c);
-                const float dd0 = __ldg(d0 + c), dd1 = __ldg(d0 + W + c);
-                const float ri = aa * (yy0 + ca * dd0) + bb * (yy1 + cb * dd1);
-                const float dri = (yy1 - yy0 - ea * dd0 + eb * dd1) * ih;
+                const float4 t = __ldg(q4 + nn * L1 + l);
+                const float ri = aa * (t.x + ca * t.y) + bb * (t.z + cb * t.w);
+                const float dri = (t.z - t.x - ea * t.y + eb * t.w) * ih;
                 rl[nn] = ri;
                 pl[nn] = dri * fc + ri * dfc;
               } else {
