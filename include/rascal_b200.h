@@ -62,7 +62,7 @@ typedef struct rgpu_gap_model rgpu_gap_model;
 /* Arithmetic of a compute call. */
 enum {
   RGPU_PRECISION_FP64 = 0, /* plain path: FP64 everywhere, reference data flow */
-  RGPU_PRECISION_FP32 = 1  /* fast path: FP32 expansion, TF32 tensor-core GEMMs */
+  RGPU_PRECISION_FP32 = 1  /* fast path: FP32 features, BF16x3 tensor-core GEMMs, adjoint forces */
 };
 
 /* ---------------------------------------------------------------------- */
@@ -211,6 +211,16 @@ rgpu_status rgpu_gap_model_destroy(rgpu_gap_model * m);
 rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s,
                              int precision, double * energies,
                              double * forces);
+/* rgpu_gap_predict plus the negative stress of every structure,
+ * neg_stress[n_structures][6] in the Voigt order xx, yy, zz, yz, xz, xy: the
+ * sum over pairs of r_ji (x) dE_i/dr_j divided by the cell volume. Replaces
+ * compute_sparse_kernel_neg_stress (models/sparse_kernel_predict.hh:291-377)
+ * behind KRR.predict_stress, which returns -neg_stress
+ * (bindings/rascal/models/krr.py:168-210). neg_stress must not be NULL;
+ * energies and forces may be. */
+rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s,
+                                    int precision, double * energies,
+                                    double * forces, double * neg_stress);
 
 /* ---------------------------------------------------------------------- */
 /* Timing support: synchronise the structure set's stream; number of kernels

@@ -60,6 +60,8 @@ SIGNATURES = {
     "rgpu_gap_model_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "rgpu_gap_predict": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, c_dbl_p,
                                         c_dbl_p]),
+    "rgpu_gap_predict_stress": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, c_dbl_p,
+                                               c_dbl_p, c_dbl_p]),
     "rgpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "rgpu_kernel_launches": (ctypes.c_int64, [ctypes.c_int]),
     "rgpu_stage_times": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p, ctypes.c_int32]),

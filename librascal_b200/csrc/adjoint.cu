@@ -42,11 +42,14 @@ constexpr int kMaxN = 16;  // largest max_radial of the register-staged path
 // p1 = dRI f_c + RI df_c are staged in registers (NV >= n of them); the
 // spherical-harmonics recurrence then streams (Y, grad Y) for that l.
 // dE/dc of the pair's centre is read as dC[i][lm][s*n + n'], n contiguous
-// values per lm (float4 loads when n == NV).
-template <int L, int NV>
+// values per lm (float4 loads when n == NV). With STRESS, the pair's
+// r_ji (x) g_ij (Voigt xx yy zz yz xz xy, the reference's
+// sparse_kernel_predict.hh:355-366) is summed per structure as well.
+template <int L, int NV, bool STRESS>
 __global__ void __launch_bounds__(kThreads, 4)  // 128 registers, no spills at L = 6
 pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, int64_t n_pairs,
-                    const float * __restrict__ dC, double * __restrict__ F) {
+                    const float * __restrict__ dC, double * __restrict__ F,
+                    const int32_t * __restrict__ center_struct, double * __restrict__ stress) {
   constexpr int K = (L + 1) * (L + 1);
   constexpr int L1 = L + 1;
   const int W = a.fd.W, n = a.fd.n, Sn = a.fd.S * a.fd.n;
@@ -58,6 +61,7 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
     const int64_t p = base + lane;
     const int32_t ci = p < n_pairs ? pair_center[p] : -1;
     float g0 = 0.f, g1 = 0.f, g2 = 0.f;
+    float t6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int32_t j = -1, self_atom = -1;
     // the self pair carries no force of its own: the other pairs' F_i terms do
     if (ci >= 0 && p != a.pair_off[ci]) {
@@ -125,6 +129,15 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
       g0 = dx * sY + fr * sd0;
       g1 = dy * sY + fr * sd1;
       g2 = dz * sY + fr * sd2;
+      if constexpr (STRESS) {
+        const float rf = float(r), rx = -rf * dx, ry = -rf * dy, rz = -rf * dz;
+        t6[0] = rx * g0;
+        t6[1] = ry * g1;
+        t6[2] = rz * g2;
+        t6[3] = ry * g2;
+        t6[4] = rz * g0;
+        t6[5] = rx * g1;
+      }
       atomicAdd(&F[3 * size_t(j) + 0], -double(g0));
       atomicAdd(&F[3 * size_t(j) + 1], -double(g1));
       atomicAdd(&F[3 * size_t(j) + 2], -double(g2));
@@ -154,23 +167,49 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
       atomicAdd(&F[3 * size_t(ia) + 1], double(h1));
       atomicAdd(&F[3 * size_t(ia) + 2], double(h2));
     }
+    if constexpr (STRESS) {
+      // structures are consecutive runs of centres, hence of lanes
+      const int32_t sid = ci >= 0 ? center_struct[ci] : -1;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int32_t su = __shfl_up_sync(0xffffffffu, sid, off);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+          const float u = __shfl_up_sync(0xffffffffu, t6[k], off);
+          if (lane >= off && su == sid) t6[k] += u;
+        }
+      }
+      const int32_t sn = __shfl_down_sync(0xffffffffu, sid, 1);
+      if (sid >= 0 && (lane == 31 || sn != sid))
+#pragma unroll
+        for (int k = 0; k < 6; ++k) atomicAdd(&stress[6 * size_t(sid) + k], double(t6[k]));
+    }
   }
 }
 
 }  // namespace
 
 void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_center, int64_t n_pairs,
-                              const float * dC, double * forces, cudaStream_t st) {
+                              const float * dC, double * forces, cudaStream_t st,
+                              const int32_t * center_struct, double * stress) {
   if (a.n_centers == 0 || n_pairs == 0) return;
   sph_constants_tu();
   if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
   const int grid = int(std::min<int64_t>((n_pairs + kThreads - 1) / kThreads, int64_t(148) * 64));
+#define RGPU_ADJ_LAUNCH(LL, NVV)                                                                     \
+  if (stress)                                                                                        \
+    pair_adjoint_kernel<LL, NVV, true><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces, \
+                                                                   center_struct, stress);           \
+  else                                                                                               \
+    pair_adjoint_kernel<LL, NVV, false><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC,       \
+                                                                    forces, nullptr, nullptr);
 #define RGPU_ADJ_CASE(LL)                                                                            \
   case LL:                                                                                           \
-    if (a.fd.n <= 8)                                                                                 \
-      pair_adjoint_kernel<LL, 8><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces);    \
-    else                                                                                             \
-      pair_adjoint_kernel<LL, 16><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces);   \
+    if (a.fd.n <= 8) {                                                                               \
+      RGPU_ADJ_LAUNCH(LL, 8)                                                                         \
+    } else {                                                                                         \
+      RGPU_ADJ_LAUNCH(LL, 16)                                                                        \
+    }                                                                                                \
     break;
   switch (a.fd.L) {
     RGPU_ADJ_CASE(0)
@@ -190,6 +229,7 @@ void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_cent
       throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
   }
 #undef RGPU_ADJ_CASE
+#undef RGPU_ADJ_LAUNCH
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }

@@ -155,6 +155,7 @@ struct rgpu_structures {
   int64_t n_atoms{0};
   std::vector<int64_t> atom_off;
   std::vector<int32_t> types;
+  std::vector<double> cells_h;  // [n_struct][9], lattice vectors as rows
   std::vector<uint8_t> mask;
   bool has_mask{false};
   std::vector<int64_t> center_off_h;
@@ -182,7 +183,7 @@ struct rgpu_structures {
   bool feat_gradients{false};
   bool feat_valid{false};
   // GAP work
-  DevBuf E_d, F_d, K64, t64, erow64, Wh, Wl, dX32, dC32, epart, Xh, Xl;
+  DevBuf E_d, F_d, S_d, K64, t64, erow64, Wh, Wl, dX32, dC32, epart, Xh, Xl;
   bool feat_x32{false};  // FP32 features also kept unsplit (for export)
   DevBuf dCp, dCs, dXp;
   // status and timing
@@ -558,7 +559,8 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
 
 size_t plain_budget_bytes() { return size_t(24) << 30; }
 
-void gap_plain(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * grad_d, bool forces) {
+void gap_plain(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * grad_d, bool forces,
+               double * stress_d) {
   rgpu_calculator * c = m->calc;
   const FeatureDims & fd = s->fd;
   const int64_t nc = s->nl.n_centers;
@@ -629,7 +631,8 @@ void gap_plain(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * g
                         s->dXp.as<double>(), st);
     launch_force_contract_fp64(fd, c0, c1, p_base, s->nl.pair_off, s->nl.pair_j,
                                s->row_of_center.as<int32_t>(), s->dXp.as<double>(), s->t64.as<double>(),
-                               fd.Dpad, grad_d, st);
+                               fd.Dpad, grad_d, st, s->nl.pair_dist, s->nl.pair_dir, s->nl.center_struct,
+                               stress_d);
     c0 = c1;
   }
   mark(s, 7);
@@ -643,7 +646,8 @@ int64_t eofs_of(const rgpu_structures * s, const rgpu_gap_model * m, int sI) {
   return o;
 }
 
-void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_d, bool forces) {
+void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_d, bool forces,
+              double * stress_d) {
   rgpu_calculator * c = m->calc;
   const FeatureDims & fd = s->fd;
   const int64_t nc = s->nl.n_centers;
@@ -745,10 +749,108 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
                      s->dC32.as<float>(), st);
   mark(s, 7);
   ExpansionArgs ea = exp_args(c, s);
-  launch_pair_adjoint_fp32(ea, s->nl.pair_center, s->nl.n_pairs, s->dC32.as<float>(), F_d, st);
+  launch_pair_adjoint_fp32(ea, s->nl.pair_center, s->nl.n_pairs, s->dC32.as<float>(), F_d, st,
+                           s->nl.center_struct, stress_d);
 }
 
 }  // namespace
+
+// Cell volume as the reference computes it, from the lattice vector lengths
+// and the cosines of the angles between them
+// (structure_managers/atomic_structure.hh:137-155); rows of `cell` are the
+// lattice vectors.
+static double cell_volume(const double * cell) {
+  double len[3], v[3][3];
+  for (int i = 0; i < 3; ++i) {
+    for (int k = 0; k < 3; ++k) v[i][k] = cell[3 * i + k];
+    len[i] = std::sqrt(v[i][0] * v[i][0] + v[i][1] * v[i][1] + v[i][2] * v[i][2]);
+  }
+  auto dot = [&](int a, int b) { return v[a][0] * v[b][0] + v[a][1] * v[b][1] + v[a][2] * v[b][2]; };
+  const double al = std::acos(dot(1, 2) / len[1] / len[2]);
+  const double be = std::acos(dot(0, 2) / len[0] / len[2]);
+  const double ga = std::acos(dot(1, 0) / len[1] / len[0]);
+  const double c0 = std::cos(al), c1 = std::cos(be), c2 = std::cos(ga);
+  return len[0] * len[1] * len[2] * std::sqrt(1 - c0 * c0 - c1 * c1 - c2 * c2 + 2 * c0 * c1 * c2);
+}
+
+extern "C" {
+static void calculator_to_device(rgpu_calculator * c);
+}
+
+// Energies, forces and (optionally) the negative stress of a GAP model: the
+// reference's KRR.predict / predict_forces / predict_stress
+// (bindings/rascal/models/krr.py:92-210) on the GPU.
+static void gap_predict_impl(rgpu_gap_model * m, rgpu_structures * s, int precision, double * energies,
+                             double * forces, double * neg_stress) {
+  {
+    if (!m || !s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    if (s->has_mask)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "Can't compute spherical expansion gradients with masked center atoms",
+                  RGPU_EXC_LOGIC_ERROR);
+    calculator_to_device(m->calc);
+    s->timed = true;
+    mark(s, 0);
+    const bool want_forces = true;
+    // neighbour list, layout, features
+    build_nl(s, m->calc->hy.cutoff);
+    mark(s, 1);
+    compute_features(m->calc, s, precision, want_forces, m->species, /*need_x32=*/false);
+    model_layout(m, s);
+    const int64_t na = s->n_atoms;
+    s->E_d.ensure(sizeof(double) * (s->n_struct + 1));
+    s->F_d.ensure(sizeof(double) * 3 * (na + 1));
+    RGPU_CUDA(cudaMemsetAsync(s->E_d.p, 0, sizeof(double) * s->n_struct, s->st));
+    RGPU_CUDA(cudaMemsetAsync(s->F_d.p, 0, sizeof(double) * 3 * na, s->st));
+    double * stress_d = nullptr;
+    if (neg_stress) {
+      s->S_d.ensure(sizeof(double) * 6 * (s->n_struct + 1));
+      RGPU_CUDA(cudaMemsetAsync(s->S_d.p, 0, sizeof(double) * 6 * s->n_struct, s->st));
+      stress_d = s->S_d.as<double>();
+    }
+    if (precision == RGPU_PRECISION_FP64)
+      gap_plain(m, s, s->E_d.as<double>(), s->F_d.as<double>(), want_forces, stress_d);
+    else
+      gap_fast(m, s, s->E_d.as<double>(), s->F_d.as<double>(), want_forces, stress_d);
+    mark(s, 8);
+    if (energies) {
+      RGPU_CUDA(cudaMemcpyAsync(energies, s->E_d.p, sizeof(double) * s->n_struct, cudaMemcpyDeviceToHost, s->st));
+    }
+    if (forces) {
+      RGPU_CUDA(cudaMemcpyAsync(forces, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s->st));
+    }
+    if (neg_stress) {
+      RGPU_CUDA(cudaMemcpyAsync(neg_stress, s->S_d.p, sizeof(double) * 6 * s->n_struct, cudaMemcpyDeviceToHost,
+                                s->st));
+    }
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    if (precision == RGPU_PRECISION_FP32) {
+      const int where = gemm_tc_timeout(true);
+      if (where)
+        throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM: a bounded pipeline wait gave up (stage " +
+                                          std::to_string(where) + ")");
+    }
+    if (energies) {
+      // baseline (models/krr.py:68-90) on the host, FP64: a table over the
+      // atom types (validated to [0, 130) by rgpu_structures_set)
+      double sc[130] = {0.};
+      for (size_t i = 0; i < m->species.size(); ++i)
+        if (m->species[i] >= 0 && m->species[i] < 130) sc[m->species[i]] = m->self_contrib[i];
+      const int32_t * types = s->types.data();
+      for (int st = 0; st < s->n_struct; ++st) {
+        double y0 = 0.;
+        for (int64_t a = s->atom_off[st]; a < s->atom_off[st + 1]; ++a) y0 += sc[types[a]];
+        energies[st] += y0;
+      }
+    }
+    if (forces && precision == RGPU_PRECISION_FP64)
+      for (int64_t i = 0; i < 3 * na; ++i) forces[i] = -forces[i];
+    if (neg_stress)
+      for (int st = 0; st < s->n_struct; ++st) {
+        const double v = cell_volume(&s->cells_h[9 * size_t(st)]);
+        for (int k = 0; k < 6; ++k) neg_stress[6 * st + k] /= v;
+      }
+  }
+}
 
 // ===================================================================== C ABI
 extern "C" {
@@ -881,6 +983,7 @@ rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const
     s->n_atoms = s->atom_off[n_structures];
     if (s->n_atoms > (int64_t(1) << 31) - 1) throw Error(RGPU_ERR_INVALID_ARGUMENT, "too many atoms");
     s->types.assign(numbers, numbers + s->n_atoms);
+    s->cells_h.assign(cells, cells + 9 * size_t(n_structures));
     bool seen[130] = {false};
     for (int64_t a = 0; a < s->n_atoms; ++a) {
       if (s->types[a] < 0 || s->types[a] >= 130)
@@ -1172,58 +1275,14 @@ rgpu_status rgpu_gap_model_destroy(rgpu_gap_model * m) {
 
 rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precision, double * energies,
                              double * forces) {
+  return guard([&] { gap_predict_impl(m, s, precision, energies, forces, nullptr); });
+}
+
+rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s, int precision, double * energies,
+                                    double * forces, double * neg_stress) {
   return guard([&] {
-    if (!m || !s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
-    if (s->has_mask)
-      throw Error(RGPU_ERR_INVALID_ARGUMENT, "Can't compute spherical expansion gradients with masked center atoms",
-                  RGPU_EXC_LOGIC_ERROR);
-    calculator_to_device(m->calc);
-    s->timed = true;
-    mark(s, 0);
-    const bool want_forces = true;
-    // neighbour list, layout, features
-    build_nl(s, m->calc->hy.cutoff);
-    mark(s, 1);
-    compute_features(m->calc, s, precision, want_forces, m->species, /*need_x32=*/false);
-    model_layout(m, s);
-    const int64_t na = s->n_atoms;
-    s->E_d.ensure(sizeof(double) * (s->n_struct + 1));
-    s->F_d.ensure(sizeof(double) * 3 * (na + 1));
-    RGPU_CUDA(cudaMemsetAsync(s->E_d.p, 0, sizeof(double) * s->n_struct, s->st));
-    RGPU_CUDA(cudaMemsetAsync(s->F_d.p, 0, sizeof(double) * 3 * na, s->st));
-    if (precision == RGPU_PRECISION_FP64)
-      gap_plain(m, s, s->E_d.as<double>(), s->F_d.as<double>(), want_forces);
-    else
-      gap_fast(m, s, s->E_d.as<double>(), s->F_d.as<double>(), want_forces);
-    mark(s, 8);
-    if (energies) {
-      RGPU_CUDA(cudaMemcpyAsync(energies, s->E_d.p, sizeof(double) * s->n_struct, cudaMemcpyDeviceToHost, s->st));
-    }
-    if (forces) {
-      RGPU_CUDA(cudaMemcpyAsync(forces, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s->st));
-    }
-    RGPU_CUDA(cudaStreamSynchronize(s->st));
-    if (precision == RGPU_PRECISION_FP32) {
-      const int where = gemm_tc_timeout(true);
-      if (where)
-        throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM: a bounded pipeline wait gave up (stage " +
-                                          std::to_string(where) + ")");
-    }
-    if (energies) {
-      // baseline (models/krr.py:68-90) on the host, FP64: a table over the
-      // atom types (validated to [0, 130) by rgpu_structures_set)
-      double sc[130] = {0.};
-      for (size_t i = 0; i < m->species.size(); ++i)
-        if (m->species[i] >= 0 && m->species[i] < 130) sc[m->species[i]] = m->self_contrib[i];
-      const int32_t * types = s->types.data();
-      for (int st = 0; st < s->n_struct; ++st) {
-        double y0 = 0.;
-        for (int64_t a = s->atom_off[st]; a < s->atom_off[st + 1]; ++a) y0 += sc[types[a]];
-        energies[st] += y0;
-      }
-    }
-    if (forces && precision == RGPU_PRECISION_FP64)
-      for (int64_t i = 0; i < 3 * na; ++i) forces[i] = -forces[i];
+    if (!neg_stress) throw Error(RGPU_ERR_INVALID_ARGUMENT, "neg_stress output is required");
+    gap_predict_impl(m, s, precision, energies, forces, neg_stress);
   });
 }
 

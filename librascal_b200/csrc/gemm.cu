@@ -325,7 +325,11 @@ __global__ void force_contract_kernel(int64_t p_first, int64_t np, int D, int64_
                                       const int32_t * __restrict__ pair_j,
                                       const int32_t * __restrict__ row_of_center,
                                       const double * __restrict__ dX, const double * __restrict__ t,
-                                      int64_t ldt, double * __restrict__ grad) {
+                                      int64_t ldt, double * __restrict__ grad,
+                                      const double * __restrict__ pair_dist,
+                                      const double * __restrict__ pair_dir,
+                                      const int32_t * __restrict__ center_struct,
+                                      double * __restrict__ stress) {
   int64_t q = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   int lane = threadIdx.x & 31;
   if (q >= np) return;
@@ -346,6 +350,19 @@ __global__ void force_contract_kernel(int64_t p_first, int64_t np, int D, int64_
     int64_t j = pair_j[p];
 #pragma unroll
     for (int c = 0; c < 3; ++c) atomicAdd(&grad[3 * j + c], s[c]);
+    // r_ji (x) dE_i/dr_j, Voigt xx yy zz yz xz xy
+    // (models/sparse_kernel_predict.hh:355-366); the self pair has r_ji = 0
+    if (stress && pair_dist[p] > 0.) {
+      const double r = pair_dist[p];
+      const double rx = -r * pair_dir[3 * p], ry = -r * pair_dir[3 * p + 1], rz = -r * pair_dir[3 * p + 2];
+      double * st = stress + 6 * size_t(center_struct[ci]);
+      atomicAdd(st + 0, rx * s[0]);
+      atomicAdd(st + 4, rz * s[0]);
+      atomicAdd(st + 1, ry * s[1]);
+      atomicAdd(st + 5, rx * s[1]);
+      atomicAdd(st + 2, rz * s[2]);
+      atomicAdd(st + 3, ry * s[2]);
+    }
   }
 }
 
@@ -416,7 +433,8 @@ void launch_energy_reduce(int64_t rows, int n_parts, const float * e_part, int64
 void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, int64_t p_base,
                                 const int64_t * pair_off, const int32_t * pair_j,
                                 const int32_t * row_of_center, const double * dX, const double * t,
-                                int64_t ldt, double * grad, cudaStream_t st) {
+                                int64_t ldt, double * grad, cudaStream_t st, const double * pair_dist,
+                                const double * pair_dir, const int32_t * center_struct, double * stress) {
   if (c1 <= c0) return;
   int64_t p_first = 0, p_last = 0;
   RGPU_CUDA(cudaMemcpyAsync(&p_first, pair_off + c0, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
@@ -430,7 +448,8 @@ void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, 
   RGPU_LAUNCHED();
   force_contract_kernel<<<div_up(np * 32, 256), 256, 0, st>>>(p_first, np, fd.D, p_base,
                                                              pc.as<int64_t>(), pair_j, row_of_center,
-                                                             dX, t, ldt, grad);
+                                                             dX, t, ldt, grad, pair_dist, pair_dir,
+                                                             center_struct, stress);
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }

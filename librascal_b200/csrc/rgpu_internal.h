@@ -309,12 +309,16 @@ void launch_energy_reduce(int64_t rows, int n_parts, const float * e_part, int64
 void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, int64_t p_base,
                                 const int64_t * pair_off, const int32_t * pair_j,
                                 const int32_t * row_of_center, const double * dX,
-                                const double * t, int64_t ldt, double * grad, cudaStream_t st);
+                                const double * t, int64_t ldt, double * grad, cudaStream_t st,
+                                const double * pair_dist = nullptr, const double * pair_dir = nullptr,
+                                const int32_t * center_struct = nullptr, double * stress = nullptr);
 // Adjoint pair kernel: forces from dE/dC (FP32, the layout written by
-// launch_ps_bwd_fp32) and recomputed dC/dr.
+// launch_ps_bwd_fp32) and recomputed dC/dr. With stress, also the unscaled
+// negative stress sum_pairs r_ji (x) g_ij per structure (6 Voigt values).
 void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_center, int64_t n_pairs,
                               const float * dC, double * forces,
-                              cudaStream_t st);
+                              cudaStream_t st, const int32_t * center_struct = nullptr,
+                              double * stress = nullptr);
 
 // ------------------------------------------------------------------ helpers
 void launch_species_sort(int64_t n, const int32_t * types, const int32_t * center_atom,

@@ -176,6 +176,16 @@ class GAPModel:
                                          N.ptr(F, N.c_dbl_p)))
         return E, F
 
+    def predict_stress(self, structures, precision="fp32"):
+        """(energies, forces, negative stress n_structures x 6 in the Voigt
+        order xx, yy, zz, yz, xz, xy) for a StructureSet."""
+        E = np.zeros(structures.n_structures)
+        F = np.zeros((structures.n_atoms, 3))
+        NS = np.zeros((structures.n_structures, 6))
+        N.check(N.lib().rgpu_gap_predict_stress(self._h, structures.handle, _PREC[precision], N.ptr(E, N.c_dbl_p),
+                                                N.ptr(F, N.c_dbl_p), N.ptr(NS, N.c_dbl_p)))
+        return E, F, NS
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and N._lib is not None:
@@ -233,6 +243,20 @@ class KRR:
 
     def predict_energy_forces(self, managers):
         return self._gap().predict(self._structures(managers), self.precision)
+
+    def predict_stress(self, managers, KNM=None):
+        """Stress per structure in the Voigt order xx, yy, zz, yz, xz, xy
+        (bindings/rascal/models/krr.py:168-210): minus the negative stress of
+        compute_sparse_kernel_neg_stress."""
+        if self.kernel.kernel_type != "Sparse":
+            raise NotImplementedError("stress prediction only implemented for kernels with kernel_type=='Sparse'")
+        st = self._structures(managers)
+        if KNM is not None:
+            if 6 * st.n_structures != KNM.shape[0]:
+                raise ValueError("KNM size mismatch {}!={}".format(6 * st.n_structures, KNM.shape[0]))
+            return -np.dot(KNM, self.weights).reshape((st.n_structures, 6))
+        _, _, NS = self._gap().predict_stress(st, self.precision)
+        return -NS
 
     def _baseline(self, managers):
         st = self._structures(managers)

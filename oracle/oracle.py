@@ -63,6 +63,8 @@ def lib():
             getattr(L, f).argtypes = [ctypes.c_void_p, c_dbl_p]
         L.orc_run_gap.argtypes = [ctypes.c_void_p, ctypes.c_int, c_int_p, c_dbl_p, c_dbl_p,
                                   ctypes.c_int, c_dbl_p, c_dbl_p]
+        L.orc_run_gap_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, c_int_p, c_dbl_p, c_dbl_p,
+                                         ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p]
         _lib = L
     return _lib
 
@@ -211,6 +213,21 @@ class Run:
         if lib().orc_run_powerspectrum_grad(self.h, _p(out, c_dbl_p)) != 0:
             raise RuntimeError("gradients were not computed")
         return out
+
+    def gap_stress(self, sparse_species, T, alpha, zeta):
+        """Energies, forces and the negative stress per structure (Voigt xx,
+        yy, zz, yz, xz, xy; the reference's compute_sparse_kernel_neg_stress)."""
+        sps = np.ascontiguousarray(sparse_species, dtype=np.int32)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        al = np.ascontiguousarray(alpha, dtype=np.float64)
+        E = np.zeros(self.n_struct)
+        F = np.zeros((self.n_atoms, 3))
+        NS = np.zeros((self.n_struct, 6))
+        rc = lib().orc_run_gap_stress(self.h, len(sps), _p(sps, c_int_p), _p(T, c_dbl_p), _p(al, c_dbl_p),
+                                      int(zeta), _p(E, c_dbl_p), _p(F, c_dbl_p), _p(NS, c_dbl_p))
+        if rc != 0:
+            raise RuntimeError("the stress needs a run with gradients")
+        return E, F, NS
 
     def gap(self, sparse_species, T, alpha, zeta, forces=True):
         """Energies (per structure, no baseline) and forces (-dE/dr)."""

@@ -1136,8 +1136,27 @@ struct Run {
   std::vector<int> pair_jglobal;     // global atom index of the neighbour
   std::vector<double> C, dC;         // expansion: rows x S*n*K; pairs x S*3*n*K
   std::vector<double> X, dX;         // PS: rows x D; pairs x 3*D
+  std::vector<double> volume;        // cell volume of each structure
   bool grads{false};
 };
+
+// Cell volume as the reference computes it, from the lattice vector lengths
+// and the cosines of the angles between them
+// (structure_managers/atomic_structure.hh:137-155). `cell` holds the lattice
+// vectors as rows.
+static double cell_volume(const double * cell) {
+  double len[3], v[3][3];
+  for (int i = 0; i < 3; ++i) {
+    for (int k = 0; k < 3; ++k) v[i][k] = cell[3 * i + k];
+    len[i] = std::sqrt(v[i][0] * v[i][0] + v[i][1] * v[i][1] + v[i][2] * v[i][2]);
+  }
+  auto dot = [&](int a, int b) { return v[a][0] * v[b][0] + v[a][1] * v[b][1] + v[a][2] * v[b][2]; };
+  const double al = std::acos(dot(1, 2) / len[1] / len[2]);
+  const double be = std::acos(dot(0, 2) / len[0] / len[2]);
+  const double ga = std::acos(dot(1, 0) / len[1] / len[0]);
+  const double c0 = std::cos(al), c1 = std::cos(be), c2 = std::cos(ga);
+  return len[0] * len[1] * len[2] * std::sqrt(1 - c0 * c0 - c1 * c1 - c2 * c2 + 2 * c0 * c1 * c2);
+}
 
 static int species_index(const std::vector<int> & sp, int t) {
   auto it = std::lower_bound(sp.begin(), sp.end(), t);
@@ -1161,8 +1180,10 @@ static void compute_run(Calculator & calc, Run & R, const double * pos,
   SphericalHarmonics sph(L);
   std::vector<double> RI(W), dRI(W), tmp(W);
   R.pair_off.assign(1, 0);
+  R.volume.assign(R.n_struct, 0.);
   for (int s = 0; s < R.n_struct; ++s) {
     long a0 = R.atom_off[s], N = R.atom_off[s + 1] - a0;
+    R.volume[s] = cell_volume(cells + 9 * s);
     StructureNL nl = build_nl(int(N), pos + a0 * 3, types + a0, cells + 9 * s,
                               pbc + 3 * s, mask ? mask + a0 : nullptr, calc.rc);
     long row0 = long(R.center_atom.size());
@@ -1375,14 +1396,21 @@ static double pow_zeta(double v, int zeta) {
   return pow_u(v, size_t(zeta));
 }
 
+// The negative stress (Voigt xx, yy, zz, yz, xz, xy) per structure follows
+// compute_sparse_kernel_neg_stress (models/sparse_kernel_predict.hh:291-377):
+// sum over pairs of r_ji (x) the pair's partial gradient dE_i/dr_j, with the
+// off-diagonals taken as yz <- r_y g_z, xz <- r_z g_x, xy <- r_x g_y, divided
+// by the cell volume.
 static void gap_predict(const Run & R, int M, const int * sp_species,
                         const double * T, const double * alpha, int zeta,
-                        double * energies, double * forces) {
+                        double * energies, double * forces, double * neg_stress = nullptr) {
   long NC = long(R.center_atom.size());
   long NA = R.atom_off[R.n_struct];
   for (int s = 0; s < R.n_struct; ++s) energies[s] = 0.;
   if (forces)
     for (long a = 0; a < 3 * NA; ++a) forces[a] = 0.;
+  if (neg_stress)
+    for (int s = 0; s < 6 * R.n_struct; ++s) neg_stress[s] = 0.;
   std::vector<double> k(M), t(R.D);
   for (long i = 0; i < NC; ++i) {
     const double * Xi = &R.X[size_t(i) * R.D];
@@ -1405,14 +1433,29 @@ static void gap_predict(const Run & R, int M, const int * sp_species,
       for (long p = R.pair_off[i]; p < R.pair_off[i + 1]; ++p) {
         const double * dXp = &R.dX[size_t(p) * 3 * R.D];
         long j = R.pair_jglobal[p];
+        double g[3];
         for (int c = 0; c < 3; ++c) {
-          double g = 0.;
-          for (int d = 0; d < R.D; ++d) g += dXp[c * R.D + d] * t[d];
-          forces[3 * j + c] -= g;
+          g[c] = 0.;
+          for (int d = 0; d < R.D; ++d) g[c] += dXp[c * R.D + d] * t[d];
+          forces[3 * j + c] -= g[c];
+        }
+        if (neg_stress) {
+          const Pair & q = R.pairs[p];
+          double * ns = neg_stress + 6 * R.center_struct[i];
+          const double rji[3] = {-q.dist * q.dir[0], -q.dist * q.dir[1], -q.dist * q.dir[2]};
+          ns[0] += rji[0] * g[0];
+          ns[4] += rji[2] * g[0];
+          ns[1] += rji[1] * g[1];
+          ns[5] += rji[0] * g[1];
+          ns[2] += rji[2] * g[2];
+          ns[3] += rji[1] * g[2];
         }
       }
     }
   }
+  if (neg_stress)
+    for (int s = 0; s < R.n_struct; ++s)
+      for (int k = 0; k < 6; ++k) neg_stress[6 * s + k] /= R.volume[s];
 }
 
 }  // namespace orc
@@ -1583,6 +1626,15 @@ int orc_run_gap(void * r, int M, const int * sp_species, const double * T,
   auto * R = static_cast<orc::Run *>(r);
   if (forces && !R->grads) return -1;
   orc::gap_predict(*R, M, sp_species, T, alpha, zeta, energies, forces);
+  return 0;
+}
+
+int orc_run_gap_stress(void * r, int M, const int * sp_species, const double * T,
+                       const double * alpha, int zeta, double * energies,
+                       double * forces, double * neg_stress) {
+  auto * R = static_cast<orc::Run *>(r);
+  if (!R->grads || !forces || !neg_stress) return -1;
+  orc::gap_predict(*R, M, sp_species, T, alpha, zeta, energies, forces, neg_stress);
   return 0;
 }
 

@@ -312,6 +312,35 @@ def test_gap_forces_periodic_and_fd():
             assert abs(fd - F_ref[a, c]) <= 1e-6 * max(1.0, np.abs(F_ref).max())
 
 
+@pytest.mark.parametrize("which", ["periodic_boxes", "molecule_clusters"])
+def test_gap_neg_stress_parity(which):
+    """Negative stress per structure (Voigt xx, yy, zz, yz, xz, xy) of both
+    GPU paths against the oracle's compute_sparse_kernel_neg_stress
+    restatement; KRR.predict_stress returns its negative."""
+    if which == "periodic_boxes":
+        batch, kw = synthetic.periodic_boxes(n_struct=2, seed=2), dict(rc=4.0, n=6, l=4, sigma=0.3)
+    else:
+        batch, kw = synthetic.molecule_clusters(n_struct=12, seed=5), dict(rc=5.0, n=8, l=6, sigma=0.4)
+    r, T, sps, alpha, species = gap_setup(batch, kw, n_sparse=6)
+    E_ref, F_ref, NS_ref = r.gap_stress(sps, T, alpha, 2)
+    calc = soap(**kw)
+    sp = rb.SparsePoints(calc)
+    sp.add_dense(sps, T, calc.get_keys(species))
+    model = rb.GAPModel(calc, sp, alpha, 2)
+    st = rb.StructureSet(batch)
+    scale = np.abs(NS_ref).max()
+    for prec, tol in [("fp64", 1e-10), ("fp32", 1e-4)]:
+        E, F, NS = model.predict_stress(st, prec)
+        assert NS.shape == NS_ref.shape
+        assert np.abs(NS - NS_ref).max() <= tol * scale, prec
+        assert np.abs(F - F_ref).max() <= tol * np.abs(F_ref).max(), prec
+        E2, F2 = model.predict(st, prec)
+        assert np.array_equal(E, E2) or np.abs(E - E2).max() <= 1e-12 * np.abs(E).max()
+    kernel = rb.Kernel(calc, name="GAP", zeta=2, target_type="Structure", kernel_type="Sparse")
+    krr = rb.KRR(alpha, kernel, sp, {}, precision="fp64")
+    assert np.abs(krr.predict_stress(st) + NS_ref).max() <= 1e-10 * scale
+
+
 def test_empty_and_isolated_atoms():
     frames = [dict(positions=[[5., 5., 5.]], numbers=[1], cell=np.eye(3) * 10., pbc=[False] * 3),
               dict(positions=[[1., 1., 1.], [9., 9., 9.]], numbers=[8, 1], cell=np.eye(3) * 10.,
