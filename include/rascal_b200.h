@@ -179,7 +179,10 @@ rgpu_status rgpu_get_features(const rgpu_calculator * calc,
 /* Dense gradients, 3 rows (x, y, z) per pair including self pairs:
  * get_features_gradient (bind_py_structure_manager.cc:621-668;
  * property_block_sparse.hh:961-987). `out` is 3*n_pairs x (n_keys * inner).
- * Needs a compute with gradients at RGPU_PRECISION_FP64. */
+ * Needs a compute with gradients at RGPU_PRECISION_FP64. For a spherical
+ * expansion the rows are the reference's grad C blocks
+ * (calculator_spherical_expansion.hh:2327-2366): a self pair carries every
+ * centre key, a neighbour pair only the key of its neighbour's species. */
 rgpu_status rgpu_get_features_gradient(const rgpu_calculator * calc,
                                        const rgpu_structures * s,
                                        int32_t n_keys, const int32_t * keys,

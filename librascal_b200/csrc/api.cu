@@ -465,6 +465,72 @@ std::vector<int> key_blocks(const rgpu_calculator * c, const rgpu_structures * s
   return blocks;
 }
 
+// Dense expansion gradients (property_block_sparse.hh:961-987): 3 rows per
+// pair (x, y, z), key blocks of n*K. A pair's gradient has the key of its
+// neighbour's species only; the self pair's has every species
+// (calculator_spherical_expansion.hh:2327-2366).
+void export_expansion_gradient(const rgpu_calculator * calc, rgpu_structures * s, int n_keys,
+                               const std::vector<int> & blocks, double * out) {
+  const FeatureDims & fd = s->fd;
+  const int64_t nc = s->nl.n_centers;
+  const int inner = fd.nK;
+  ExpansionArgs ea = exp_args(calc, s);
+  const std::vector<int64_t> & poff = pair_offsets_host(s);
+  const size_t per_pair = sizeof(double) * 3 * size_t(fd.nK);
+  const size_t per_center = sizeof(double) * size_t(fd.S) * 3 * fd.nK;
+  const size_t budget = size_t(4) << 30;
+  std::map<int, int> sidx;
+  for (int i = 0; i < fd.S; ++i) sidx[s->species[i]] = i;
+  std::vector<double> hp, hs;
+  std::vector<int32_t> pj;
+  int64_t c0 = 0;
+  while (c0 < nc) {
+    int64_t c1 = c0;
+    size_t bytes = 0;
+    while (c1 < nc) {
+      size_t add = per_pair * size_t(poff[c1 + 1] - poff[c1]) + per_center;
+      if (c1 > c0 && bytes + add > budget) break;
+      bytes += add;
+      ++c1;
+    }
+    const int64_t p_base = poff[c0];
+    const int64_t np = poff[c1] - p_base;
+    s->dCp.ensure(per_pair * size_t(np) + 64);
+    s->dCs.ensure(per_center * size_t(c1 - c0) + 64);
+    launch_expansion_grad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), s->st);
+    launch_expansion_selfgrad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), s->dCs.as<double>(), s->st);
+    hp.resize(size_t(np) * 3 * fd.nK);
+    hs.resize(size_t(c1 - c0) * fd.S * 3 * fd.nK);
+    pj.resize(size_t(np));
+    RGPU_CUDA(cudaMemcpyAsync(hp.data(), s->dCp.p, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, s->st));
+    RGPU_CUDA(cudaMemcpyAsync(hs.data(), s->dCs.p, sizeof(double) * hs.size(), cudaMemcpyDeviceToHost, s->st));
+    RGPU_CUDA(cudaMemcpyAsync(pj.data(), s->nl.pair_j + p_base, sizeof(int32_t) * np, cudaMemcpyDeviceToHost,
+                              s->st));
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    for (int64_t ci = c0; ci < c1; ++ci)
+      for (int64_t p = poff[ci]; p < poff[ci + 1]; ++p) {
+        const bool self = (p == poff[ci]);
+        const int sj = self ? -1 : sidx.at(s->types[pj[size_t(p - p_base)]]);
+        for (int c = 0; c < 3; ++c) {
+          double * dst = out + (size_t(p) * 3 + c) * size_t(n_keys) * inner;
+          for (int k = 0; k < n_keys; ++k) {
+            const int b = blocks[k];
+            const double * src = nullptr;
+            if (b >= 0 && self)
+              src = &hs[((size_t(ci - c0) * fd.S + b) * 3 + c) * fd.nK];
+            else if (b >= 0 && b == sj)
+              src = &hp[(size_t(p - p_base) * 3 + c) * fd.nK];
+            if (src)
+              std::memcpy(dst + size_t(k) * inner, src, sizeof(double) * inner);
+            else
+              std::memset(dst + size_t(k) * inner, 0, sizeof(double) * inner);
+          }
+        }
+      }
+    c0 = c1;
+  }
+}
+
 // Device copies of a model's sparse points in the batch's layout.
 void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
   const FeatureDims & fd = s->fd;
@@ -1185,12 +1251,16 @@ rgpu_status rgpu_get_features_gradient(const rgpu_calculator * calc, const rgpu_
     rgpu_structures * s = const_cast<rgpu_structures *>(s_in);
     if (!s->feat_valid || s->feat_calc != calc) throw Error(RGPU_ERR_NOT_COMPUTED, "features have not been computed");
     if (!s->feat_gradients) throw Error(RGPU_ERR_NOT_COMPUTED, "gradients were not requested (compute_gradients)");
-    if (s->feat_precision != RGPU_PRECISION_FP64 || calc->hy.kind != "sphericalinvariants")
-      throw Error(RGPU_ERR_INVALID_ARGUMENT, "dense gradients are exported from the FP64 power spectrum");
+    if (s->feat_precision != RGPU_PRECISION_FP64)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "dense gradients are exported from the FP64 path");
     const FeatureDims & fd = s->fd;
     const int64_t nc = s->nl.n_centers;
-    const int inner = fd.n * fd.n * (fd.L + 1);
     auto blocks = key_blocks(calc, s, n_keys, keys);
+    if (calc->hy.kind == "sphericalexpansion") {
+      export_expansion_gradient(calc, s, n_keys, blocks, out);
+      return;
+    }
+    const int inner = fd.n * fd.n * (fd.L + 1);
     ExpansionArgs ea = exp_args(calc, s);
     PsArgs pa;
     pa.fd = fd;

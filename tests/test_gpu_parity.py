@@ -247,6 +247,36 @@ def test_powerspectrum_gradient_fp64_parity():
     assert info.shape == (r.n_pairs, 5)
 
 
+@pytest.mark.parametrize("which", ["periodic_boxes", "molecule_clusters"])
+def test_expansion_gradient_fp64_parity(which):
+    """Dense spherical-expansion gradients (3 rows per pair, self pairs
+    included; a pair carries only its neighbour's species key, the self pair
+    every key) against the oracle's restatement of
+    calculator_spherical_expansion.hh:2327-2366."""
+    if which == "periodic_boxes":
+        batch, kw = synthetic.periodic_boxes(n_struct=2, seed=4), dict(rc=4.0, n=6, l=4, sigma=0.3)
+    else:
+        batch, kw = synthetic.molecule_clusters(n_struct=6, seed=3), dict(rc=5.0, n=4, l=3, sigma=0.4)
+    calc = rb.SphericalExpansion(interaction_cutoff=kw["rc"], cutoff_smooth_width=0.5, max_radial=kw["n"],
+                                 max_angular=kw["l"], gaussian_sigma_type="Constant",
+                                 gaussian_sigma_constant=kw["sigma"],
+                                 optimization=dict(Spline=dict(accuracy=1e-8)), compute_gradients=True)
+    al = calc.transform(rb.AtomsList(rb.StructureSet(batch)))
+    species = np.unique(batch["numbers"])
+    dC = al.get_features_gradient(calc, keys=calc.get_keys(species))
+    r = O.Run(oracle_calc(**kw), batch, species, gradients=True)
+    ref = r.expansion_gradient()                       # (pairs, S, 3, n, K)
+    ref = np.transpose(ref, (0, 2, 1, 3, 4)).reshape(dC.shape)
+    assert np.abs(dC - ref).max() <= 1e-10 * np.abs(ref).max()
+    C = al.get_features(calc, keys=calc.get_keys(species))
+    C_ref = r.expansion().reshape(C.shape)
+    assert_features_close(C_ref, C)
+    # FP32 expansion rows (padded l-blocks on the device) exported in the same layout
+    al32 = calc.transform(rb.AtomsList(rb.StructureSet(batch)), precision="fp32")
+    C32 = al32.get_features(calc, keys=calc.get_keys(species))
+    assert np.abs(C32 - C_ref).max() <= 1e-5 * np.abs(C_ref).max()
+
+
 def gap_setup(batch, kw, n_sparse=6, seed=0, zeta=2):
     species = np.unique(batch["numbers"])
     oc = oracle_calc(**kw)
