@@ -196,8 +196,9 @@ rgpu_status rgpu_get_features_gradient(const rgpu_calculator * calc,
  * Sparse points are given dense: T [n_sparse x D] FP64 in the power-spectrum
  * layout of `species` (sorted, n_species entries; D = n_species*(n_species+1)/2
  * * n^2 * (l+1)), one row per sparse environment, with its central species in
- * sparse_species [n_sparse]; weights [n_sparse]; self_contributions
- * [n_species] (energy baseline per species, models/krr.py:68-90). */
+ * sparse_species [n_sparse]; weights [n_sparse] (NULL: zero weights, for a
+ * model used only for its kernel matrices); self_contributions [n_species]
+ * (energy baseline per species, models/krr.py:68-90). */
 rgpu_status rgpu_gap_model_create(rgpu_calculator * calc, int32_t n_species,
                                   const int32_t * species, int32_t n_sparse,
                                   const int32_t * sparse_species,
@@ -224,6 +225,34 @@ rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s,
 rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s,
                                     int precision, double * energies,
                                     double * forces, double * neg_stress);
+
+/* Sparse kernel matrices for training a GAP model, FP64 (the reference's
+ * arithmetic). Columns follow the order of the model's sparse points;
+ * weights and self contributions are not used.
+ * K_NM energy rows: SparseKernel::compute with a GAP kernel
+ * (models/sparse_kernels.hh:104-131 for target_atom = 0: out[n_structures]
+ * [n_sparse], the sum over each structure's centres of (X_i . T_m)^zeta for
+ * the sparse points of the centre's species; :165-191 for target_atom = 1:
+ * out[n_centers][n_sparse]), behind Kernel.__call__(managers, sparse_points)
+ * (bindings/rascal/models/kernels.py:122-164). */
+rgpu_status rgpu_sparse_kernel(rgpu_gap_model * m, rgpu_structures * s,
+                               int32_t target_atom, double * out);
+/* K_NM gradient rows: SparseKernel::compute_derivative
+ * (models/sparse_kernels.hh:258-499, 577-619) behind
+ * Kernel.__call__(managers, sparse_points, grad=(True, False),
+ * compute_neg_stress) (bindings/rascal/models/kernels.py:150-156).
+ * out[3 * n_centers (+ 6 * n_structures if neg_stress)][n_sparse]: row
+ * 3a + c is d/dr_a[c] of the structure's summed kernel; the stress rows
+ * (Voigt xx, yy, zz, yz, xz, xy, divided by the cell volume) follow. As in
+ * the reference, a structure none of whose centre species has sparse points
+ * ends the computation: its rows and those of all later structures are 0.
+ * Centre masks are rejected, as with gradients in the reference. */
+rgpu_status rgpu_sparse_kernel_derivative(rgpu_gap_model * m, rgpu_structures * s,
+                                          int32_t neg_stress, double * out);
+/* K_MM: SparseKernel::compute(sparse_points) (models/sparse_kernels.hh:
+ * 141-156, models/sparse_points.hh:144-170): out[n_sparse][n_sparse] =
+ * (T_a . T_b)^zeta for points of one species, 0 across species. */
+rgpu_status rgpu_sparse_kernel_mm(rgpu_gap_model * m, double * out);
 
 /* ---------------------------------------------------------------------- */
 /* Timing support: synchronise the structure set's stream; number of kernels

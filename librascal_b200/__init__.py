@@ -10,11 +10,12 @@ plus StructureSet / GAPModel (direct handles on the C ABI) and gap_energy
 (torch.autograd.Function over the adjoint force path).
 """
 from ._native import LIB_PATH, lib  # noqa: F401
-from .models import (KRR, GAPModel, Kernel, SparsePoints, compute_sparse_kernel_gradients,  # noqa: F401
-                     gap_energy)
+from .models import (KRR, GAPModel, Kernel, SparsePoints, compute_KNM, compute_sparse_kernel_gradients,  # noqa: F401
+                     gap_energy, train_gap_model)
 from .neighbourlist import AtomsList, StructureSet, frames_to_batch  # noqa: F401
 from .representations import SphericalExpansion, SphericalInvariants  # noqa: F401
 
 __all__ = ["SphericalInvariants", "SphericalExpansion", "AtomsList", "StructureSet", "SparsePoints",
-           "Kernel", "KRR", "GAPModel", "compute_sparse_kernel_gradients", "gap_energy",
+           "Kernel", "KRR", "GAPModel", "compute_sparse_kernel_gradients", "compute_KNM", "train_gap_model",
+           "gap_energy",
            "frames_to_batch"]

@@ -62,6 +62,9 @@ SIGNATURES = {
                                         c_dbl_p]),
     "rgpu_gap_predict_stress": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, c_dbl_p,
                                                c_dbl_p, c_dbl_p]),
+    "rgpu_sparse_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, c_dbl_p]),
+    "rgpu_sparse_kernel_derivative": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, c_dbl_p]),
+    "rgpu_sparse_kernel_mm": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p]),
     "rgpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "rgpu_kernel_launches": (ctypes.c_int64, [ctypes.c_int]),
     "rgpu_stage_times": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p, ctypes.c_int32]),

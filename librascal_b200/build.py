@@ -33,6 +33,7 @@ SOURCES = [
     ("gemm_tc.cu", [], "gemm_tc"),
     ("noalloc.cu", [], "noalloc"),
     ("adjoint.cu", [], "adjoint"),
+    ("training.cu", [], "training"),
     ("api.cu", [], "api"),
     ("radial_gto.cpp", ["-Xcompiler", "-ffp-contract=off"], "radial_gto"),
     ("json_lite.cpp", [], "json_lite"),

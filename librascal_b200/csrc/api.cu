@@ -186,6 +186,7 @@ struct rgpu_structures {
   DevBuf E_d, F_d, S_d, K64, t64, erow64, Wh, Wl, dX32, dC32, epart, Xh, Xl;
   bool feat_x32{false};  // FP32 features also kept unsplit (for export)
   DevBuf dCp, dCs, dXp;
+  DevBuf knm, W64, plist;  // sparse kernel matrices for training
   // status and timing
   DevStatus * status_d{nullptr};
   DevStatus * status_h{nullptr};
@@ -209,6 +210,7 @@ struct rgpu_gap_model {
   std::vector<GapSpecies> segs;  // per batch species
   DevBuf T64, alpha64, Th, Tl, Tth, Ttl, alpha32;
   std::vector<int64_t> tt_off;  // per batch species offset into Tt32
+  DevBuf ucol;                  // caller's index of each sparse point in layout order
 };
 
 namespace {
@@ -551,6 +553,7 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
   std::vector<double> T(size_t(m->M) * fd.Dpad, 0.), al(m->M);
   int pos = 0;
   int64_t tt_total = 0;
+  std::vector<int32_t> user(size_t(std::max(m->M, 1)), 0);
   m->tt_off.assign(fd.S, 0);
   for (int sI = 0; sI < fd.S; ++sI) {
     GapSpecies & g = m->segs[sI];
@@ -560,6 +563,7 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
     m->tt_off[sI] = tt_total;
     tt_total += int64_t(g.Mpad) * fd.Dpad;
     for (int r : rows[sI]) {
+      user[pos] = r;
       al[pos] = m->alpha[r];
       const double * src = &m->T[size_t(r) * fm.D];
       double * dst = &T[size_t(pos) * fd.Dpad];
@@ -618,6 +622,7 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
   upload(s, m->alpha32, al32.data(), sizeof(float) * al32.size());
   upload(s, m->Tth, Tth.data(), sizeof(uint16_t) * Tth.size());
   upload(s, m->Ttl, Ttl.data(), sizeof(uint16_t) * Ttl.size());
+  upload(s, m->ucol, user.data(), sizeof(int32_t) * user.size());
   RGPU_CUDA(cudaStreamSynchronize(s->st));
   m->layout_species = s->species;
   m->layout_D = fd.D;
@@ -916,6 +921,239 @@ static void gap_predict_impl(rgpu_gap_model * m, rgpu_structures * s, int precis
         for (int k = 0; k < 6; ++k) neg_stress[6 * st + k] /= v;
       }
   }
+}
+
+// ---------------------------------------------------------------- training
+// Sparse kernel matrices of a GAP model (models/sparse_kernels.hh), FP64.
+// Their columns follow the order in which the sparse points were given.
+static void kernel_features(rgpu_gap_model * m, rgpu_structures * s, bool grads) {
+  if (!m || !s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (grads && s->has_mask)
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, "Can't compute spherical expansion gradients with masked center atoms",
+                RGPU_EXC_LOGIC_ERROR);
+  calculator_to_device(m->calc);
+  s->timed = false;
+  build_nl(s, m->calc->hy.cutoff);
+  compute_features(m->calc, s, RGPU_PRECISION_FP64, grads, m->species, /*need_x32=*/false);
+  model_layout(m, s);
+}
+
+// K = X_s T_s^T of species sI into s->K64 (rows x M).
+static void species_dots(rgpu_gap_model * m, rgpu_structures * s, int sI, int64_t row0) {
+  const FeatureDims & fd = s->fd;
+  const GapSpecies & g = m->segs[sI];
+  const int64_t rows = s->species_count[sI];
+  s->K64.ensure(sizeof(double) * size_t(std::max<int64_t>(rows, 1)) * std::max(g.M, 1) + 64);
+  gemm_nt_fp64(rows, g.M, fd.D, s->X64.as<double>() + size_t(row0) * fd.Dpad, fd.Dpad,
+               m->T64.as<double>() + size_t(g.m0) * fd.Dpad, fd.Dpad, s->K64.as<double>(), g.M, s->st);
+}
+
+// K_NM energy rows: SparseKernelImpl<GAP>::compute for target Structure
+// (models/sparse_kernels.hh:104-131) or Atom (:165-191).
+static void sparse_kernel_impl(rgpu_gap_model * m, rgpu_structures * s, bool atom_target, double * out) {
+  kernel_features(m, s, false);
+  const FeatureDims & fd = s->fd;
+  const int64_t rows_out = atom_target ? s->nl.n_centers : s->n_struct;
+  const size_t bytes = sizeof(double) * size_t(rows_out) * m->M;
+  s->knm.ensure(bytes + 64);
+  RGPU_CUDA(cudaMemsetAsync(s->knm.p, 0, bytes, s->st));
+  int64_t row0 = 0;
+  for (int sI = 0; sI < fd.S; ++sI) {
+    const int64_t rows = s->species_count[sI];
+    const GapSpecies & g = m->segs[sI];
+    if (rows > 0 && g.M > 0) {
+      species_dots(m, s, sI, row0);
+      launch_knm_rows(rows, g.M, s->K64.as<double>(), m->zeta, s->center_of_row.as<int32_t>(), row0,
+                      s->nl.center_struct, atom_target, m->ucol.as<int32_t>() + g.m0, s->knm.as<double>(), m->M,
+                      s->st);
+    }
+    row0 += rows;
+  }
+  if (bytes) RGPU_CUDA(cudaMemcpyAsync(out, s->knm.p, bytes, cudaMemcpyDeviceToHost, s->st));
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+}
+
+// K_NM gradient rows: SparseKernelImpl<GAP>::compute_derivative
+// (models/sparse_kernels.hh:258-499). dX/dr is materialised chunk by chunk
+// as in the plain prediction path and contracted with the sparse points of
+// each central species by one gathered GEMM per species and chunk.
+static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * s, bool neg_stress,
+                                          double * out) {
+  kernel_features(m, s, true);
+  rgpu_calculator * c = m->calc;
+  const FeatureDims & fd = s->fd;
+  const int64_t nc = s->nl.n_centers;
+  const int M = m->M;
+  cudaStream_t st = s->st;
+  const int64_t rows_out = 3 * nc + (neg_stress ? 6 * int64_t(s->n_struct) : 0);
+  const size_t bytes = sizeof(double) * size_t(rows_out) * M;
+  s->knm.ensure(bytes + 64);
+  RGPU_CUDA(cudaMemsetAsync(s->knm.p, 0, bytes, st));
+  if (M == 0 || nc == 0) {
+    RGPU_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  // zeta (X_i . T_m)^(zeta-1) of every row, species by species
+  std::vector<int64_t> woff(fd.S + 1, 0), srow0(fd.S + 1, 0);
+  for (int sI = 0; sI < fd.S; ++sI) {
+    woff[sI + 1] = woff[sI] + s->species_count[sI] * m->segs[sI].M;
+    srow0[sI + 1] = srow0[sI] + s->species_count[sI];
+  }
+  s->W64.ensure(sizeof(double) * size_t(std::max<int64_t>(woff[fd.S], 1)) + 64);
+  for (int sI = 0; sI < fd.S; ++sI) {
+    const int64_t rows = s->species_count[sI];
+    const GapSpecies & g = m->segs[sI];
+    if (rows == 0 || g.M == 0) continue;
+    gemm_nt_fp64(rows, g.M, fd.D, s->X64.as<double>() + size_t(srow0[sI]) * fd.Dpad, fd.Dpad,
+                 m->T64.as<double>() + size_t(g.m0) * fd.Dpad, fd.Dpad, s->W64.as<double>() + woff[sI], g.M, st);
+    launch_kernel_weight(rows * g.M, s->W64.as<double>() + woff[sI], m->zeta, st);
+  }
+  // The reference returns from its loop over structures at the first one
+  // whose centre species have no sparse points (models/sparse_kernels.hh:
+  // 347-349): that structure and all later ones keep zero rows.
+  std::vector<int> sp_index(130, -1);
+  for (int sI = 0; sI < fd.S; ++sI) sp_index[s->species[sI]] = sI;
+  int64_t c_stop = nc;
+  for (int st_i = 0; st_i < s->n_struct; ++st_i) {
+    bool shared = false;
+    for (int64_t a = s->atom_off[st_i]; a < s->atom_off[st_i + 1] && !shared; ++a)
+      shared = m->segs[sp_index[s->types[a]]].M > 0;
+    if (!shared) {
+      c_stop = s->atom_off[st_i];  // centres are the atoms (no centre mask with gradients)
+      break;
+    }
+  }
+  const std::vector<int64_t> & poff = pair_offsets_host(s);
+  const size_t per_pair = sizeof(double) * (3 * size_t(fd.D) + 3 * size_t(fd.nK));
+  const size_t per_center = sizeof(double) * size_t(fd.S) * 3 * fd.nK;
+  const size_t budget = plain_budget_bytes();
+  ExpansionArgs ea = exp_args(c, s);
+  PsArgs pa;
+  pa.fd = fd;
+  pa.n_centers = nc;
+  pa.normalize = c->hy.normalize;
+  pa.row_of_center = s->row_of_center.as<int32_t>();
+  std::vector<std::vector<int32_t>> lists(fd.S);
+  int64_t c0 = 0;
+  while (c0 < c_stop) {
+    int64_t c1 = c0;
+    size_t used = 0;
+    while (c1 < c_stop) {
+      size_t add = per_pair * size_t(poff[c1 + 1] - poff[c1]) + per_center;
+      if (c1 > c0 && used + add > budget) break;
+      used += add;
+      ++c1;
+    }
+    const int64_t p_base = poff[c0];
+    const int64_t np = poff[c1] - p_base;
+    // pairs of the chunk listed by the species of their centre: (pair - p_base, centre)
+    for (auto & l : lists) l.clear();
+    for (int64_t ci = c0; ci < c1; ++ci) {
+      std::vector<int32_t> & l = lists[sp_index[s->types[ci]]];
+      for (int64_t p = poff[ci]; p < poff[ci + 1]; ++p) {
+        l.push_back(int32_t(p - p_base));
+        l.push_back(int32_t(ci));
+      }
+    }
+    std::vector<int32_t> flat;
+    std::vector<int64_t> loff(fd.S + 1, 0);
+    for (int sI = 0; sI < fd.S; ++sI) {
+      loff[sI] = int64_t(flat.size()) / 2;
+      flat.insert(flat.end(), lists[sI].begin(), lists[sI].end());
+    }
+    loff[fd.S] = int64_t(flat.size()) / 2;
+    upload(s, s->plist, flat.data(), sizeof(int32_t) * flat.size());
+    s->dCp.ensure(sizeof(double) * size_t(np) * 3 * fd.nK + 64);
+    s->dCs.ensure(per_center * size_t(c1 - c0) + 64);
+    s->dXp.ensure(sizeof(double) * size_t(np) * 3 * fd.D + 64);
+    launch_expansion_grad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), st);
+    launch_expansion_selfgrad_fp64(ea, c0, c1, p_base, s->dCp.as<double>(), s->dCs.as<double>(), st);
+    launch_ps_grad_fp64(pa, ea, c0, c1, p_base, s->C64.as<double>(), s->X64.as<double>(), s->invn64.as<double>(),
+                        s->dCp.as<double>(), s->dCs.as<double>(), s->dXp.as<double>(), st);
+    for (int sI = 0; sI < fd.S; ++sI) {
+      const GapSpecies & g = m->segs[sI];
+      const int64_t n_list = loff[sI + 1] - loff[sI];
+      if (n_list == 0 || g.M == 0) continue;
+      KnmDerArgs a{};
+      a.list = s->plist.as<int32_t>() + 2 * loff[sI];
+      a.n_list = n_list;
+      a.p_base = p_base;
+      a.dX = s->dXp.as<double>();
+      a.D = fd.D;
+      a.T = m->T64.as<double>() + size_t(g.m0) * fd.Dpad;
+      a.ldt = fd.Dpad;
+      a.M = g.M;
+      a.W = s->W64.as<double>() + woff[sI];
+      a.row0 = srow0[sI];
+      a.row_of_center = s->row_of_center.as<int32_t>();
+      a.pair_j = s->nl.pair_j;
+      a.ucol = m->ucol.as<int32_t>() + g.m0;
+      a.out = s->knm.as<double>();
+      a.ldo = M;
+      if (neg_stress) {
+        a.pair_dist = s->nl.pair_dist;
+        a.pair_dir = s->nl.pair_dir;
+        a.center_struct = s->nl.center_struct;
+        a.stress_row0 = 3 * nc;
+      }
+      launch_knm_derivative(a, st);
+    }
+    c0 = c1;
+  }
+  RGPU_CUDA(cudaMemcpyAsync(out, s->knm.p, bytes, cudaMemcpyDeviceToHost, st));
+  RGPU_CUDA(cudaStreamSynchronize(st));
+  if (neg_stress)
+    for (int st_i = 0; st_i < s->n_struct; ++st_i) {
+      const double v = cell_volume(&s->cells_h[9 * size_t(st_i)]);
+      double * r = out + size_t(3 * nc + 6 * int64_t(st_i)) * M;
+      for (int k = 0; k < 6 * M; ++k) r[k] /= v;
+    }
+}
+
+// K_MM: SparseKernel::compute(sparse_points) (models/sparse_kernels.hh:
+// 141-156, models/sparse_points.hh:144-170), one FP64 T_s T_s^T per species.
+static void sparse_kernel_mm_impl(rgpu_gap_model * m, double * out) {
+  if (!m) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+  const int M = m->M;
+  if (M == 0) return;
+  const int Sm = int(m->species.size());
+  const FeatureDims fm = make_dims(m->calc->hy, Sm);
+  std::vector<int32_t> order;
+  std::vector<int> m0(Sm + 1, 0);
+  for (int a = 0; a < Sm; ++a) {
+    m0[a] = int(order.size());
+    for (int r = 0; r < M; ++r)
+      if (m->sp_species[r] == m->species[a]) order.push_back(r);
+  }
+  m0[Sm] = int(order.size());
+  std::vector<double> T(size_t(M) * fm.D);
+  for (int k = 0; k < M; ++k)
+    std::memcpy(&T[size_t(k) * fm.D], &m->T[size_t(order[k]) * fm.D], sizeof(double) * fm.D);
+  int Mmax = 0;
+  for (int a = 0; a < Sm; ++a) Mmax = std::max(Mmax, m0[a + 1] - m0[a]);
+  cudaStream_t st = nullptr;
+  RGPU_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+  } guard_st{st};
+  DevBuf Td, Kd, Od, Ud;
+  Td.ensure(sizeof(double) * T.size());
+  Kd.ensure(sizeof(double) * size_t(Mmax) * Mmax + 64);
+  Od.ensure(sizeof(double) * size_t(M) * M);
+  Ud.ensure(sizeof(int32_t) * order.size());
+  RGPU_CUDA(cudaMemcpyAsync(Td.p, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice, st));
+  RGPU_CUDA(cudaMemcpyAsync(Ud.p, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice, st));
+  RGPU_CUDA(cudaMemsetAsync(Od.p, 0, sizeof(double) * size_t(M) * M, st));
+  for (int a = 0; a < Sm; ++a) {
+    const int Ms = m0[a + 1] - m0[a];
+    if (Ms == 0) continue;
+    const double * Ts = Td.as<double>() + size_t(m0[a]) * fm.D;
+    gemm_nt_fp64(Ms, Ms, fm.D, Ts, fm.D, Ts, fm.D, Kd.as<double>(), Ms, st);
+    launch_kmm_scatter(Ms, Kd.as<double>(), m->zeta, Ud.as<int32_t>() + m0[a], Od.as<double>(), M, st);
+  }
+  RGPU_CUDA(cudaMemcpyAsync(out, Od.p, sizeof(double) * size_t(M) * M, cudaMemcpyDeviceToHost, st));
+  RGPU_CUDA(cudaStreamSynchronize(st));
 }
 
 // ===================================================================== C ABI
@@ -1331,7 +1569,10 @@ rgpu_status rgpu_gap_model_create(rgpu_calculator * calc, int32_t n_species, con
         throw Error(RGPU_ERR_INVALID_ARGUMENT, "sparse point species missing from the model species");
     FeatureDims fm = make_dims(calc->hy, n_species);
     m->T.assign(T, T + size_t(n_sparse) * fm.D);
-    m->alpha.assign(weights, weights + n_sparse);
+    if (weights)
+      m->alpha.assign(weights, weights + n_sparse);
+    else
+      m->alpha.assign(size_t(n_sparse), 0.);  // kernel matrices only
     m->zeta = zeta;
     m->self_contrib.assign(n_species, 0.);
     if (self_contributions) m->self_contrib.assign(self_contributions, self_contributions + n_species);
@@ -1353,6 +1594,28 @@ rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s, int
   return guard([&] {
     if (!neg_stress) throw Error(RGPU_ERR_INVALID_ARGUMENT, "neg_stress output is required");
     gap_predict_impl(m, s, precision, energies, forces, neg_stress);
+  });
+}
+
+rgpu_status rgpu_sparse_kernel(rgpu_gap_model * m, rgpu_structures * s, int32_t target_atom, double * out) {
+  return guard([&] {
+    if (!out) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    sparse_kernel_impl(m, s, target_atom != 0, out);
+  });
+}
+
+rgpu_status rgpu_sparse_kernel_derivative(rgpu_gap_model * m, rgpu_structures * s, int32_t neg_stress,
+                                          double * out) {
+  return guard([&] {
+    if (!out) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    sparse_kernel_derivative_impl(m, s, neg_stress != 0, out);
+  });
+}
+
+rgpu_status rgpu_sparse_kernel_mm(rgpu_gap_model * m, double * out) {
+  return guard([&] {
+    if (!out) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    sparse_kernel_mm_impl(m, out);
   });
 }
 

@@ -40,6 +40,22 @@ __device__ __forceinline__ float to_tf32(float x) {
 
 inline int div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }
 
+// v^zeta of the GAP kernel (models/kernels.hh:48-61)
+__device__ __forceinline__ double pow_zeta_d(double v, int z) {
+  if (z == 0) return 1.;
+  if (z == 1) return v;
+  if (z == 2) return v * v;
+  if (z == 3) return v * v * v;
+  double r = 1., x = v;
+  int n = z;
+  do {
+    if (n & 1) r *= x;
+    n >>= 1;
+    x *= x;
+  } while (n);
+  return r;
+}
+
 // Spherical-harmonics constants per (l, m), double and float copies:
 // coeff_a, coeff_b (math/spherical_harmonics.cc:54-64), sqrt(2l+1) and
 // -sqrt(1 + 1/(2l)) (:67-71), and the ladder factors sqrt((l-m)(l+m+1))

@@ -85,21 +85,6 @@ gemm_fp64_kernel(int64_t M, int64_t N, int64_t K, const double * __restrict__ A,
     }
 }
 
-__device__ __forceinline__ double pow_zeta_d(double v, int z) {
-  // models/kernels.hh:48-61 (zeta 1, 2, 3 special cases, else repeated product)
-  if (z == 0) return 1.;
-  if (z == 1) return v;
-  if (z == 2) return v * v;
-  if (z == 3) return v * v * v;
-  double r = 1., x = v;
-  int n = z;
-  do {
-    if (n & 1) r *= x;
-    n >>= 1;
-    x *= x;
-  } while (n);
-  return r;
-}
 __device__ __forceinline__ float pow_zeta_f(float v, int z) {
   float r = 1.f;
   for (int i = 0; i < z; ++i) r *= v;

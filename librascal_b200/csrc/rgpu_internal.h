@@ -312,6 +312,41 @@ void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, 
                                 const double * t, int64_t ldt, double * grad, cudaStream_t st,
                                 const double * pair_dist = nullptr, const double * pair_dir = nullptr,
                                 const int32_t * center_struct = nullptr, double * stress = nullptr);
+// ------------------------------------------------------------------ training
+// K_NM energy rows from K = X_s T_s^T (rows x M): k^zeta into row
+// center_of_row[row0 + r] (atom target) or added into its structure's row.
+void launch_knm_rows(int64_t rows, int M, const double * K, int zeta, const int32_t * center_of_row,
+                     int64_t row0, const int32_t * center_struct, bool atom_target, const int32_t * ucol,
+                     double * out, int64_t ldo, cudaStream_t st);
+// K <- zeta K^(zeta-1) (1 for zeta = 1), in place.
+void launch_kernel_weight(int64_t n, double * K, int zeta, cudaStream_t st);
+// K_MM block of one species: out[ucol[a]][ucol[b]] = K[a][b]^zeta.
+void launch_kmm_scatter(int M, const double * K, int zeta, const int32_t * ucol, double * out, int64_t ldo,
+                        cudaStream_t st);
+// Gradient block of one central species over one chunk of pairs.
+struct KnmDerArgs {
+  const int32_t * list;  // [n_list][2]: pair index relative to p_base, centre
+  int64_t n_list, p_base;
+  const double * dX;  // materialised dX/dr of the chunk, [pair][3][D]
+  int D;
+  const double * T;  // sparse points of the species, M rows of stride ldt
+  int64_t ldt;
+  int M;
+  const double * W;  // zeta k^(zeta-1) of the species' rows, [row - row0][M]
+  int64_t row0;
+  const int32_t * row_of_center;
+  const int32_t * pair_j;
+  const int32_t * ucol;  // output column of each sparse point
+  double * out;
+  int64_t ldo;
+  // negative-stress rows (pair_dist == nullptr: none)
+  const double * pair_dist;
+  const double * pair_dir;
+  const int32_t * center_struct;
+  int64_t stress_row0;
+};
+void launch_knm_derivative(const KnmDerArgs & a, cudaStream_t st);
+
 // Adjoint pair kernel: forces from dE/dC (FP32, the layout written by
 // launch_ps_bwd_fp32) and recomputed dC/dr. With stress, also the unscaled
 // negative stress sum_pairs r_ji (x) g_ij per structure (6 Voigt values).

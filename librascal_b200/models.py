@@ -21,7 +21,7 @@ import ctypes
 import numpy as np
 
 from . import _native as N
-from .neighbourlist import AtomsList, StructureSet, frames_to_batch
+from .neighbourlist import AtomsList, StructureSet, _frame_arrays, frames_to_batch
 
 _PREC = {"fp64": N.PRECISION_FP64, "fp32": N.PRECISION_FP32}
 
@@ -37,6 +37,14 @@ class SparsePoints:
         self._representation = representation
         self.species = []       # central species of each point
         self.values = []        # dict key -> vector, per point
+
+    def _group_by_species(self):
+        """Points of one species together, species ascending, insertion
+        order inside a species: the column order of the reference's
+        SparsePointsBlockSparse (offset(sp) + index, sparse_points.hh:341-417)."""
+        order = sorted(range(len(self.species)), key=lambda i: self.species[i])
+        self.species = [self.species[i] for i in order]
+        self.values = [self.values[i] for i in order]
 
     def size(self):
         return len(self.species)
@@ -72,6 +80,7 @@ class SparsePoints:
                 self.values.append(v)
                 self.species.append(int(info[r, 2]))
             row0 += n_c
+        self._group_by_species()
 
     def add_dense(self, species, T, keys):
         """Add points from a dense matrix with the given key layout."""
@@ -84,6 +93,7 @@ class SparsePoints:
                     v[(int(key[0]), int(key[1]))] = np.array(blk, dtype=float)
             self.values.append(v)
             self.species.append(int(s))
+        self._group_by_species()
 
     def get_species(self):
         sp = set(self.species)
@@ -109,40 +119,64 @@ class SparsePoints:
 
 
 class Kernel:
-    """GAP kernel description (models/kernels.py:16-164), Sparse only."""
+    """GAP kernel (models/kernels.py:16-164), Sparse only. Every matrix is
+    computed on the GPU in FP64 through a GAP model handle with zero
+    weights:
+
+      kernel(sparse_points)                     K_MM
+      kernel(managers, sparse_points)           K_NM energy rows
+      kernel(managers, sparse_points, grad=(True, False), compute_neg_stress)
+                                                K_NM gradient (+ stress) rows
+    """
 
     def __init__(self, representation, name="GAP", kernel_type="Sparse", target_type="Structure", zeta=2,
                  **kwargs):
+        if name not in ("GAP", "Cosine"):
+            raise RuntimeError("Kernel name must be one of: Cosine, GAP.")
+        if not (isinstance(zeta, (int, np.integer)) and zeta > 0):
+            raise ValueError("The given zeta has to be a positive integer.")
         if name != "GAP" or kernel_type != "Sparse":
             raise NotImplementedError("only the sparse GAP kernel is on the B200 path")
+        if target_type not in ("Structure", "Atom"):
+            raise RuntimeError("Given target_type " + str(target_type) + " is not known."
+                               " It is either 'Structure' or 'Atom')")
         self._representation = representation
         self.name = name
         self.kernel_type = kernel_type
         self.target_type = target_type
         self.zeta = int(zeta)
 
-    def __call__(self, X, Y=None, grad=(False, False)):
-        """K_NM between the structures of an AtomsList and sparse points
-        (models/sparse_kernels.hh:104-191), FP64 on the host from the GPU
-        features."""
-        if grad != (False, False):
-            raise NotImplementedError("kernel gradients: use KRR.predict_forces")
+    def _model(self, sparse_points):
+        return GAPModel(self._representation, sparse_points, None, self.zeta)
+
+    def __call__(self, X, Y=None, grad=(False, False), compute_neg_stress=False):
+        if Y is None and grad == (False, False):
+            if not isinstance(X, SparsePoints):
+                raise NotImplementedError("the sparse kernel of a single argument needs SparsePoints")
+            model = self._model(X)
+            out = np.zeros((X.size(), X.size()))
+            if X.size():
+                N.check(N.lib().rgpu_sparse_kernel_mm(model.handle, N.ptr(out, N.c_dbl_p)))
+            return out
         if not isinstance(Y, SparsePoints):
             raise NotImplementedError("the sparse kernel needs SparsePoints as its second argument")
-        calc = self._representation
-        species = sorted(set(X.get_species()) | set(Y.get_species()))
-        keys = calc.get_keys(species)
-        feats = X.get_features(calc, keys=keys)
-        T = Y.dense(species)
-        info = X.get_representation_info()
-        k = (feats @ T.T)
-        same = info[:, 2][:, None] == np.asarray(Y.species)[None, :]
-        k = np.where(same, k ** self.zeta, 0.)
-        if self.target_type == "Atom":
-            return k
-        K = np.zeros((len(X), Y.size()))
-        np.add.at(K, info[:, 0], k)
-        return K
+        st = X.structures if isinstance(X, AtomsList) else X
+        model = self._model(Y)
+        if grad == (True, False):
+            n_c = X.n_centers() if isinstance(X, AtomsList) else st.n_atoms
+            rows = 3 * n_c + (6 * st.n_structures if compute_neg_stress else 0)
+            out = np.zeros((rows, Y.size()))
+            N.check(N.lib().rgpu_sparse_kernel_derivative(model.handle, st.handle, int(bool(compute_neg_stress)),
+                                                          N.ptr(out, N.c_dbl_p)))
+            return out
+        if grad == (False, False):
+            atom = self.target_type == "Atom"
+            rows = (X.n_centers() if isinstance(X, AtomsList) else st.n_atoms) if atom else st.n_structures
+            out = np.zeros((rows, Y.size()))
+            N.check(N.lib().rgpu_sparse_kernel(model.handle, st.handle, int(atom), N.ptr(out, N.c_dbl_p)))
+            return out
+        raise NotImplementedError("The configuration: {} is not implemented for kernel {} in {} mode.".format(
+            grad, self.name, self.kernel_type))
 
 
 class GAPModel:
@@ -152,9 +186,11 @@ class GAPModel:
         self.representation = representation
         self.species = sparse_points.get_species()
         T = N.f64(sparse_points.dense(self.species))
-        w = N.f64(np.asarray(weights).reshape(-1))
-        if len(w) != sparse_points.size():
-            raise ValueError("weights size mismatch {}!={}".format(len(w), sparse_points.size()))
+        w = None
+        if weights is not None:
+            w = N.f64(np.asarray(weights).reshape(-1))
+            if len(w) != sparse_points.size():
+                raise ValueError("weights size mismatch {}!={}".format(len(w), sparse_points.size()))
         sp = N.i32(self.species)
         sps = N.i32(sparse_points.species)
         sc = N.f64([(self_contributions or {}).get(s, 0.) for s in self.species])
@@ -276,6 +312,73 @@ def compute_sparse_kernel_gradients(representation, kernel, managers, sparse_poi
     st = managers.structures if isinstance(managers, AtomsList) else managers
     _, F = model.predict(st, precision, energies=False)
     return -F
+
+
+def _frame_numbers(frame):
+    return _frame_arrays(frame)[1]
+
+
+def compute_KNM(frames, X_sparse, kernel, soap):
+    """Energy rows of the kernel (one per structure) stacked over its
+    gradient rows (three per atom, structure after structure)
+    (bindings/rascal/models/krr.py:246-343). All frames go through one
+    batched call of each kernel on the GPU. A frame none of whose species
+    has sparse points keeps zero rows: the reference computes each frame
+    separately, so its early return for such a frame
+    (models/sparse_kernels.hh:347-349) touches no other frame."""
+    frames = list(getattr(frames, "iterable", frames))
+    n_at = np.array([len(_frame_numbers(f)) for f in frames], dtype=np.int64)
+    n_struct = len(frames)
+    stride = np.concatenate([[0], np.cumsum(3 * n_at)]) + n_struct
+    KNM = np.zeros((n_struct + int(3 * n_at.sum()), X_sparse.size()))
+    sparse_species = set(X_sparse.species)
+    good = [i for i, f in enumerate(frames) if sparse_species & set(int(z) for z in _frame_numbers(f))]
+    if not good:
+        return KNM
+    feat = soap.transform([frames[i] for i in good])
+    en = kernel(feat, X_sparse)
+    grad = kernel(feat, X_sparse, grad=(True, False))
+    g0 = 0
+    for k, i in enumerate(good):
+        KNM[i] = en[k]
+        KNM[stride[i]:stride[i + 1]] = grad[g0:g0 + 3 * n_at[i]]
+        g0 += 3 * n_at[i]
+    return KNM
+
+
+def train_gap_model(kernel, frames, KNM_, X_sparse, y_train, self_contributions, grad_train=None,
+                    lambdas=None, jitter=1e-8):
+    """Sparse GAP (subset of regressors) fit (bindings/rascal/models/krr.py:
+    346-477): weights = lstsq(K_MM + K_NM^T K_NM, K_NM^T y) with K_NM and y
+    scaled by the regularisation lambdas[0] / std(y) * sqrt(n_atoms) for
+    the energy rows and lambdas[1] / std(y) for the gradient rows, after the
+    self contributions are taken from y. K_MM comes from the GPU; the
+    normal equations are solved on the host in FP64, as in the reference."""
+    KMM = kernel(X_sparse)
+    Y = np.array(y_train, dtype=float).reshape((-1, 1))
+    KNM = np.array(KNM_, dtype=float)
+    n_struct = Y.shape[0]
+    n_atoms = np.zeros(n_struct)
+    Y0 = np.zeros((n_struct, 1))
+    for i, frame in enumerate(frames):
+        z = _frame_numbers(frame)
+        n_atoms[i] = len(z)
+        for sp in z:
+            Y0[i] += self_contributions[int(sp)]
+    Y = Y - Y0
+    delta = np.std(Y)
+    scale = lambdas[0] / delta * np.sqrt(n_atoms)[:, None]
+    KNM[:n_struct] /= scale
+    Y /= scale
+    if grad_train is not None:
+        KNM[n_struct:] /= lambdas[1] / delta
+        F = np.array(grad_train, dtype=float).reshape((-1, 1)) / (lambdas[1] / delta)
+        Y = np.vstack([Y, F])
+    KMM[np.diag_indices_from(KMM)] += jitter
+    K = KMM + KNM.T @ KNM
+    Y = KNM.T @ Y
+    weights = np.linalg.lstsq(K, Y, rcond=None)[0]
+    return KRR(weights, kernel, X_sparse, self_contributions)
 
 
 def gap_energy(positions, model, structures):

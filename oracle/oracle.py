@@ -65,6 +65,11 @@ def lib():
                                   ctypes.c_int, c_dbl_p, c_dbl_p]
         L.orc_run_gap_stress.argtypes = [ctypes.c_void_p, ctypes.c_int, c_int_p, c_dbl_p, c_dbl_p,
                                          ctypes.c_int, c_dbl_p, c_dbl_p, c_dbl_p]
+        L.orc_run_kernel_nm.argtypes = [ctypes.c_void_p, ctypes.c_int, c_int_p, c_dbl_p, ctypes.c_int,
+                                         ctypes.c_int, c_dbl_p]
+        L.orc_run_kernel_nm_derivative.argtypes = [ctypes.c_void_p, ctypes.c_int, c_int_p, c_dbl_p,
+                                                    ctypes.c_int, ctypes.c_int, c_dbl_p]
+        L.orc_kernel_mm.argtypes = [ctypes.c_int, ctypes.c_int, c_int_p, c_dbl_p, ctypes.c_int, c_dbl_p]
         _lib = L
     return _lib
 
@@ -241,3 +246,35 @@ class Run:
         if rc != 0:
             raise RuntimeError("forces need a run with gradients")
         return (E, F) if forces else E
+
+    def kernel_nm(self, sparse_species, T, zeta, target_type="Structure"):
+        """K_NM energy rows: per structure, or per centre for target "Atom"."""
+        sps = np.ascontiguousarray(sparse_species, dtype=np.int32)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        atom = target_type == "Atom"
+        out = np.zeros((self.n_centers if atom else self.n_struct, len(sps)))
+        lib().orc_run_kernel_nm(self.h, len(sps), _p(sps, c_int_p), _p(T, c_dbl_p), int(zeta), int(atom),
+                                _p(out, c_dbl_p))
+        return out
+
+    def kernel_nm_derivative(self, sparse_species, T, zeta, compute_neg_stress=False):
+        """K_NM gradient rows: 3 per centre (x, y, z), then 6 negative-stress
+        rows per structure (Voigt xx, yy, zz, yz, xz, xy) when asked."""
+        sps = np.ascontiguousarray(sparse_species, dtype=np.int32)
+        T = np.ascontiguousarray(T, dtype=np.float64)
+        rows = 3 * self.n_centers + (6 * self.n_struct if compute_neg_stress else 0)
+        out = np.zeros((rows, len(sps)))
+        rc = lib().orc_run_kernel_nm_derivative(self.h, len(sps), _p(sps, c_int_p), _p(T, c_dbl_p), int(zeta),
+                                                int(compute_neg_stress), _p(out, c_dbl_p))
+        if rc != 0:
+            raise RuntimeError("kernel gradients need a run with gradients")
+        return out
+
+
+def kernel_mm(sparse_species, T, zeta):
+    """K_MM: (T_a . T_b)^zeta within a species, 0 across species."""
+    sps = np.ascontiguousarray(sparse_species, dtype=np.int32)
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    out = np.zeros((len(sps), len(sps)))
+    lib().orc_kernel_mm(len(sps), T.shape[1], _p(sps, c_int_p), _p(T, c_dbl_p), int(zeta), _p(out, c_dbl_p))
+    return out

@@ -1458,6 +1458,118 @@ static void gap_predict(const Run & R, int M, const int * sp_species,
       for (int k = 0; k < 6; ++k) neg_stress[6 * s + k] /= R.volume[s];
 }
 
+// Sparse kernel matrices for training.
+//
+// K_NM energy rows (models/sparse_kernels.hh:104-131 for target "Structure",
+// :165-191 for target "Atom"): k(X_i, T_m) = (X_i . T_m)^zeta for the sparse
+// points of the centre's species and 0 for the others, summed over the
+// centres of each structure or kept per centre.
+static void kernel_nm(const Run & R, int M, const int * sp_species, const double * T, int zeta,
+                      bool atom_target, double * out) {
+  const long NC = long(R.center_atom.size());
+  const long rows = atom_target ? NC : long(R.n_struct);
+  std::fill(out, out + size_t(rows) * M, 0.);
+  for (long i = 0; i < NC; ++i) {
+    const double * Xi = &R.X[size_t(i) * R.D];
+    double * row = out + size_t(atom_target ? i : R.center_struct[i]) * M;
+    for (int m = 0; m < M; ++m) {
+      if (sp_species[m] != R.center_type[i]) continue;
+      const double * Tm = T + size_t(m) * R.D;
+      double dot = 0.;
+      for (int d = 0; d < R.D; ++d) dot += Xi[d] * Tm[d];
+      row[m] += pow_zeta(dot, zeta);
+    }
+  }
+}
+
+// K_NM gradient rows (models/sparse_kernels.hh:258-499): three rows (x, y, z)
+// per centre, row 3a+c = d/dr_a[c] of sum_i k(X_i, T_m) over the centres i of
+// a's structure, accumulated pair by pair as
+//   dk[j][c][m] += (dX_i/dr_j[c] . T_m) * zeta (X_i . T_m)^(zeta-1)
+// with j the neighbour's real atom. With `neg_stress`, six rows per structure
+// follow all centre rows: sum over pairs of r_ji[a] times the pair term for
+// component b, in the Voigt order xx, yy, zz, yz (r_y, z), xz (r_z, x),
+// xy (r_x, y), divided by the cell volume (:405-425, :470-482).
+// A structure none of whose centre species has sparse points ends the loop
+// over structures, as the early return at :347-349 does: its rows and those
+// of every later structure stay zero.
+static void kernel_nm_derivative(const Run & R, int M, const int * sp_species, const double * T,
+                                 int zeta, bool neg_stress, double * out) {
+  const long NC = long(R.center_atom.size());
+  const long rows = 3 * NC + (neg_stress ? 6L * R.n_struct : 0L);
+  std::fill(out, out + size_t(rows) * M, 0.);
+  const long NA = R.atom_off[R.n_struct];
+  std::vector<long> row_of_atom(size_t(NA), -1);
+  for (long i = 0; i < NC; ++i) row_of_atom[size_t(R.center_atom[i])] = i;
+  std::set<int> sparse_sp(sp_species, sp_species + M);
+  std::vector<double> w(static_cast<size_t>(M), 0.);
+  long i = 0;
+  for (int s = 0; s < R.n_struct; ++s) {
+    long i_end = i;
+    bool shared = false;
+    while (i_end < NC && R.center_struct[i_end] == s) {
+      if (sparse_sp.count(R.center_type[i_end])) shared = true;
+      ++i_end;
+    }
+    if (!shared) break;
+    double * st = neg_stress ? out + size_t(3 * NC + 6L * s) * M : nullptr;
+    for (; i < i_end; ++i) {
+      const double * Xi = &R.X[size_t(i) * R.D];
+      for (int m = 0; m < M; ++m) {
+        w[m] = 0.;
+        if (sp_species[m] != R.center_type[i]) continue;
+        if (zeta > 1) {
+          const double * Tm = T + size_t(m) * R.D;
+          double dot = 0.;
+          for (int d = 0; d < R.D; ++d) dot += Xi[d] * Tm[d];
+          w[m] = double(zeta) * pow_zeta(dot, zeta - 1);
+        } else {
+          w[m] = 1.;
+        }
+      }
+      for (long p = R.pair_off[i]; p < R.pair_off[i + 1]; ++p) {
+        const double * dXp = &R.dX[size_t(p) * 3 * R.D];
+        const long rj = row_of_atom[size_t(R.pair_jglobal[p])];
+        const Pair & q = R.pairs[p];
+        const double rji[3] = {-q.dist * q.dir[0], -q.dist * q.dir[1], -q.dist * q.dir[2]};
+        for (int m = 0; m < M; ++m) {
+          if (sp_species[m] != R.center_type[i]) continue;
+          const double * Tm = T + size_t(m) * R.D;
+          for (int c = 0; c < 3; ++c) {
+            double v = 0.;
+            for (int d = 0; d < R.D; ++d) v += dXp[c * R.D + d] * Tm[d];
+            v *= w[m];
+            if (rj >= 0) out[size_t(3 * rj + c) * M + m] += v;
+            if (st) {
+              // xx yy zz from r_ji[c]; then xz (c = x, r_z), xy (c = y, r_x), yz (c = z, r_y)
+              static const int voigt_row[3] = {4, 5, 3}, voigt_dim[3] = {2, 0, 1};
+              st[size_t(c) * M + m] += rji[c] * v;
+              st[size_t(voigt_row[c]) * M + m] += rji[voigt_dim[c]] * v;
+            }
+          }
+        }
+      }
+    }
+    if (st)
+      for (int k = 0; k < 6 * M; ++k) st[k] /= R.volume[s];
+  }
+}
+
+// K_MM (models/sparse_kernels.hh:141-156 with sparse_points.hh:144-170):
+// (T_a . T_b)^zeta for two sparse points of one species, 0 across species.
+static void kernel_mm(int M, int D, const int * sp_species, const double * T, int zeta, double * out) {
+  for (int a = 0; a < M; ++a)
+    for (int b = 0; b < M; ++b) {
+      double v = 0.;
+      if (sp_species[a] == sp_species[b]) {
+        double dot = 0.;
+        for (int d = 0; d < D; ++d) dot += T[size_t(a) * D + d] * T[size_t(b) * D + d];
+        v = pow_zeta(dot, zeta);
+      }
+      out[size_t(a) * M + b] = v;
+    }
+}
+
 }  // namespace orc
 
 /* ======================================================================== */
@@ -1635,6 +1747,26 @@ int orc_run_gap_stress(void * r, int M, const int * sp_species, const double * T
   auto * R = static_cast<orc::Run *>(r);
   if (!R->grads || !forces || !neg_stress) return -1;
   orc::gap_predict(*R, M, sp_species, T, alpha, zeta, energies, forces, neg_stress);
+  return 0;
+}
+
+
+int orc_run_kernel_nm(void * r, int M, const int * sp_species, const double * T, int zeta,
+                      int atom_target, double * out) {
+  orc::kernel_nm(*static_cast<orc::Run *>(r), M, sp_species, T, zeta, atom_target != 0, out);
+  return 0;
+}
+
+int orc_run_kernel_nm_derivative(void * r, int M, const int * sp_species, const double * T, int zeta,
+                                 int neg_stress, double * out) {
+  auto * R = static_cast<orc::Run *>(r);
+  if (!R->grads) return -1;
+  orc::kernel_nm_derivative(*R, M, sp_species, T, zeta, neg_stress != 0, out);
+  return 0;
+}
+
+int orc_kernel_mm(int M, int D, const int * sp_species, const double * T, int zeta, double * out) {
+  orc::kernel_mm(M, D, sp_species, T, zeta, out);
   return 0;
 }
 

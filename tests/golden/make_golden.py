@@ -16,6 +16,11 @@ Written files:
   expansion_reference.npz  GTO + ShiftedCosine subset of spherical_expansion_reference.ubjson
   kernel_reference.npz     PowerSpectrum subset of kernel_reference.ubjson
   structures.json          test input structures (ASE-db json subset)
+  sparse_kernel_inputs.json  parameters of the reference's sparse-kernel
+                           gradient tests (tests/test_sparse_kernels.cc:129-220)
+
+`python tests/golden/make_golden.py <ref> sparse_kernel_inputs` rewrites only
+the last file.
 """
 import json
 import os
@@ -42,6 +47,29 @@ def read_ase_db(path, start=0, length=None):
                            numbers=[int(x) for x in e["numbers"]],
                            cell=cell.tolist(), pbc=[bool(x) for x in pbc]))
     return frames
+
+
+def sparse_kernel_inputs(ref_root):
+    """The cases of reference_data/tests_only/sparse_kernel_inputs.json, with
+    each structure file named by its key in structures.json."""
+    td = os.path.join(ref_root, "reference_data", "tests_only")
+    cases = []
+    for e in json.load(open(os.path.join(td, "sparse_kernel_inputs.json"))):
+        hy = e["calculator"]
+        f = os.path.basename(e["filename"])
+        n = int(e["n_structures"])
+        key = f if f != "small_molecules-20.json" else "%s:0:%d" % (f, n)
+        cases.append(dict(
+            structure=key, n_structures=n,
+            cutoff=float(hy["cutoff_function"]["cutoff"]["value"]),
+            smooth_width=float(hy["cutoff_function"]["smooth_width"]["value"]),
+            sigma=float(hy["gaussian_density"]["gaussian_sigma"]["value"]),
+            max_radial=int(hy["max_radial"]), max_angular=int(hy["max_angular"]),
+            normalize=bool(hy["normalize"]),
+            spline="Spline" in hy["radial_contribution"].get("optimization", {}),
+            zeta=int(e["kernel"]["zeta"]), target_type=e["kernel"]["target_type"],
+            h=float(e["h"]), selected_ids=e["selected_ids"]))
+    json.dump(cases, open(os.path.join(HERE, "sparse_kernel_inputs.json"), "w"), indent=1)
 
 
 def main(ref_root):
@@ -138,4 +166,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if sys.argv[2:] != ["sparse_kernel_inputs"]:
+        main(root)
+    sparse_kernel_inputs(root)
