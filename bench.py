@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=40, help="clusters in the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", default="gap", choices=["gap", "training"],
+                   help="gap: E+F prediction (the headline); training: sparse-kernel K_NM energy and "
+                        "gradient rows for GAP fitting")
     return p.parse_args()
 
 
@@ -245,11 +248,104 @@ def run_reference_arm(args):
     return 0
 
 
+TRAINING_METRIC = "GAP training K_NM rows (energy + position gradients) atoms/s on 1 B200, FP64"
+FP64_NOMINAL_TFLOPS = 37.0  # no measured FP64 peak on this pool; B200 nominal FP64 (CUDA cores)
+
+
+def run_training(args):
+    """One step = the K_NM energy rows and gradient rows of compute_KNM for a
+    batch of clusters against 4 000 sparse points, FP64, through the C ABI."""
+    import torch
+    import librascal_b200 as rb
+    from librascal_b200 import _native as N, synthetic
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    n_struct = min(args.n_struct, 1000)
+    batch = synthetic.molecule_clusters(n_struct=n_struct, seed=args.seed + rank)
+    n_atoms = int(batch["atom_offsets"][-1])
+    calc = rb.SphericalInvariants(**HYPERS)
+    sp, alpha, species, T_sel, sps_sel = sparse_selection(rb, calc, batch, args.n_sparse, args.seed)
+    kern = rb.Kernel(calc, name="GAP", zeta=2, target_type="Structure", kernel_type="Sparse")
+    model = kern._model(sp)
+    st = rb.StructureSet(batch)
+    lib = rb.lib()
+    M = sp.size()
+    K_e = np.zeros((n_struct, M))
+    K_g = np.zeros((3 * n_atoms, M))
+
+    def step():
+        st.invalidate()
+        N.check(lib.rgpu_sparse_kernel(model.handle, st.handle, 0, N.ptr(K_e, N.c_dbl_p)))
+        N.check(lib.rgpu_sparse_kernel_derivative(model.handle, st.handle, 0, N.ptr(K_g, N.c_dbl_p)))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    l0 = lib.rgpu_kernel_launches(0)
+    dev_ms, wall = [], []
+    with Clocks(torch.cuda.current_device()) as clk:
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            step()
+            wall.append(time.perf_counter() - t)
+            dev_ms.append(st.stage_times()[0])
+    launches = int(lib.rgpu_kernel_launches(0) - l0)
+    # FP64 flops of the gradient block's GEMM: 2 * 3 * pairs_s * D * M_s per species
+    nl = st.neighbour_list()
+    npc = np.diff(nl["pair_offsets"])
+    zc = batch["numbers"][nl["center_atom"]]
+    D = T_sel.shape[1]
+    msp = {int(z): int(np.sum(np.asarray(sp.species) == z)) for z in set(sp.species)}
+    flops = sum(2.0 * 3 * float(npc[zc == z].sum()) * D * m for z, m in msp.items())
+    ms = float(np.mean(dev_ms))
+    achieved = flops / (ms * 1e-3) / 1e12
+    value = n_atoms / (ms * 1e-3)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        ns = 10
+        off = batch["atom_offsets"]
+        sub = dict(atom_offsets=off[:ns + 1], positions=batch["positions"][:off[ns]],
+                   numbers=batch["numbers"][:off[ns]], cells=batch["cells"][:ns], pbc=batch["pbc"][:ns])
+        oc = O.Calculator(HYPERS["interaction_cutoff"], HYPERS["cutoff_smooth_width"], HYPERS["max_radial"],
+                          HYPERS["max_angular"], HYPERS["gaussian_sigma_constant"], spline=True, accuracy=1e-8)
+        t = time.perf_counter()
+        r = O.Run(oc, sub, species, gradients=True)
+        r.kernel_nm(sps_sel, T_sel, 2)
+        r.kernel_nm_derivative(sps_sel, T_sel, 2)
+        secs = time.perf_counter() - t
+        cpu = dict(value=float(off[ns]) / secs, unit="atoms/s", cores=1, kind="port",
+                   sample="first %d clusters (%d atoms), K_NM energy + gradient rows, CPU FP64 restatement, "
+                          "1 thread, %.1f s" % (ns, int(off[ns]), secs))
+    line = dict(metric=TRAINING_METRIC, value=value, unit="atoms/s", n_gpus=1, steps=args.steps,
+                warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f64", data="synthetic",
+                config=dict(workload="molecule_clusters: first %d of the seeded 3-29 atom clusters, rc 5.0, n 8, "
+                                     "l 6, GTO spline, %d sparse points, zeta 2; K_NM energy rows + 3 gradient "
+                                     "rows per atom" % (n_struct, M),
+                            n_atoms=n_atoms, output_gb=K_g.nbytes / 1e9,
+                            l2="inputs larger than L2: dX/dr chunks of up to 24 GB"),
+                roofline=dict(bound="fp64", kernel="gathered FP64 tile GEMM of the gradient block (dgemm.cuh), "
+                              "with the materialised dX/dr chunks in the same timed stage",
+                              achieved=achieved, peak=FP64_NOMINAL_TFLOPS, unit="TFLOP/s",
+                              frac=achieved / FP64_NOMINAL_TFLOPS, traffic=None,
+                              peak_kind="nominal FP64 (no measured FP64 peak on this pool)",
+                              flops_per_step=flops),
+                cpu_baseline=cpu,
+                e2e=dict(value=n_atoms / float(np.mean(wall)), unit="atoms/s", h2d_bytes_per_step=0,
+                         d2h_bytes_per_step=int(K_e.nbytes + K_g.nbytes), ms_per_step=1e3 * float(np.mean(wall))),
+                gpu_launches=launches, clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "training":
+        return run_training(args)
     import torch
     import librascal_b200 as rb
     from librascal_b200 import sharding, synthetic

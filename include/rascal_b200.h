@@ -263,7 +263,10 @@ int64_t rgpu_kernel_launches(int reset);
  * CUDA events on the structure set's stream: 0 = whole call, 1 = neighbour
  * list, 2 = expansion, 3 = power spectrum, 4 = forward GEMMs, 5 = backward
  * GEMMs, 6 = power-spectrum backward (plain path: the materialised gradient
- * chunks and their contraction), 7 = pair adjoint. */
+ * chunks and their contraction), 7 = pair adjoint. After
+ * rgpu_sparse_kernel_derivative: 0 = its device time after the features and
+ * before the copy to the host, 4 = the zeta k^(zeta-1) GEMMs, 6 = the
+ * gradient chunks (materialised dX/dr and the gathered GEMMs). */
 rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out,
                              int32_t n_stages);
 

@@ -186,7 +186,7 @@ struct rgpu_structures {
   DevBuf E_d, F_d, S_d, K64, t64, erow64, Wh, Wl, dX32, dC32, epart, Xh, Xl;
   bool feat_x32{false};  // FP32 features also kept unsplit (for export)
   DevBuf dCp, dCs, dXp;
-  DevBuf knm, W64, plist;  // sparse kernel matrices for training
+  DevBuf knm, W64, plist, Vvir;  // sparse kernel matrices for training
   // status and timing
   DevStatus * status_d{nullptr};
   DevStatus * status_h{nullptr};
@@ -211,6 +211,9 @@ struct rgpu_gap_model {
   DevBuf T64, alpha64, Th, Tl, Tth, Ttl, alpha32;
   std::vector<int64_t> tt_off;  // per batch species offset into Tt32
   DevBuf ucol;                  // caller's index of each sparse point in layout order
+  std::vector<double> T_layout, alpha_layout;  // host copies in the batch layout
+  int64_t tt_total{0};
+  bool layout_bf16{false};
 };
 
 namespace {
@@ -533,10 +536,16 @@ void export_expansion_gradient(const rgpu_calculator * calc, rgpu_structures * s
   }
 }
 
-// Device copies of a model's sparse points in the batch's layout.
-void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
+void model_layout_bf16(rgpu_gap_model * m, rgpu_structures * s);
+
+// Device copies of a model's sparse points in the batch's layout: FP64
+// always, the BF16 splits of the tensor-core path only when `bf16` asks.
+void model_layout(rgpu_gap_model * m, rgpu_structures * s, bool bf16) {
   const FeatureDims & fd = s->fd;
-  if (m->layout_species == s->species && m->layout_D == fd.D) return;
+  if (m->layout_species == s->species && m->layout_D == fd.D) {
+    if (bf16 && !m->layout_bf16) model_layout_bf16(m, s);
+    return;
+  }
   const int Sm = int(m->species.size());
   FeatureDims fm = make_dims(m->calc->hy, Sm);
   std::map<int, int> bidx;
@@ -577,8 +586,26 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
       ++pos;
     }
   }
-  // BF16 hi/lo splits of T (rows = sparse points) and of T^T per species
-  // (rows = feature index, padded to Mpad columns) for the tensor-core GEMMs
+  upload(s, m->T64, T.data(), sizeof(double) * T.size());
+  upload(s, m->alpha64, al.data(), sizeof(double) * al.size());
+  upload(s, m->ucol, user.data(), sizeof(int32_t) * user.size());
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  m->T_layout.swap(T);
+  m->alpha_layout.swap(al);
+  m->tt_total = tt_total;
+  m->layout_species = s->species;
+  m->layout_D = fd.D;
+  m->layout_bf16 = false;
+  if (bf16) model_layout_bf16(m, s);
+}
+
+// BF16 hi/lo splits of T (rows = sparse points) and of T^T per species
+// (rows = feature index, padded to Mpad columns) for the tensor-core GEMMs.
+void model_layout_bf16(rgpu_gap_model * m, rgpu_structures * s) {
+  const FeatureDims & fd = s->fd;
+  const std::vector<double> & T = m->T_layout;
+  const std::vector<double> & al = m->alpha_layout;
+  const int64_t tt_total = m->tt_total;
   auto f2bf = [](float f) -> uint16_t {
     uint32_t u;
     std::memcpy(&u, &f, 4);
@@ -615,17 +642,13 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s) {
         Ttl[dst] = Tl[src];
       }
   }
-  upload(s, m->T64, T.data(), sizeof(double) * T.size());
-  upload(s, m->alpha64, al.data(), sizeof(double) * al.size());
   upload(s, m->Th, Th.data(), sizeof(uint16_t) * Th.size());
   upload(s, m->Tl, Tl.data(), sizeof(uint16_t) * Tl.size());
   upload(s, m->alpha32, al32.data(), sizeof(float) * al32.size());
   upload(s, m->Tth, Tth.data(), sizeof(uint16_t) * Tth.size());
   upload(s, m->Ttl, Ttl.data(), sizeof(uint16_t) * Ttl.size());
-  upload(s, m->ucol, user.data(), sizeof(int32_t) * user.size());
   RGPU_CUDA(cudaStreamSynchronize(s->st));
-  m->layout_species = s->species;
-  m->layout_D = fd.D;
+  m->layout_bf16 = true;
 }
 
 size_t plain_budget_bytes() { return size_t(24) << 30; }
@@ -866,7 +889,7 @@ static void gap_predict_impl(rgpu_gap_model * m, rgpu_structures * s, int precis
     build_nl(s, m->calc->hy.cutoff);
     mark(s, 1);
     compute_features(m->calc, s, precision, want_forces, m->species, /*need_x32=*/false);
-    model_layout(m, s);
+    model_layout(m, s, precision == RGPU_PRECISION_FP32);
     const int64_t na = s->n_atoms;
     s->E_d.ensure(sizeof(double) * (s->n_struct + 1));
     s->F_d.ensure(sizeof(double) * 3 * (na + 1));
@@ -935,7 +958,7 @@ static void kernel_features(rgpu_gap_model * m, rgpu_structures * s, bool grads)
   s->timed = false;
   build_nl(s, m->calc->hy.cutoff);
   compute_features(m->calc, s, RGPU_PRECISION_FP64, grads, m->species, /*need_x32=*/false);
-  model_layout(m, s);
+  model_layout(m, s, false);
 }
 
 // K = X_s T_s^T of species sI into s->K64 (rows x M).
@@ -980,6 +1003,8 @@ static void sparse_kernel_impl(rgpu_gap_model * m, rgpu_structures * s, bool ato
 static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * s, bool neg_stress,
                                           double * out) {
   kernel_features(m, s, true);
+  s->timed = true;
+  for (int k = 0; k < 4; ++k) mark(s, k);
   rgpu_calculator * c = m->calc;
   const FeatureDims & fd = s->fd;
   const int64_t nc = s->nl.n_centers;
@@ -1000,6 +1025,7 @@ static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * 
     srow0[sI + 1] = srow0[sI] + s->species_count[sI];
   }
   s->W64.ensure(sizeof(double) * size_t(std::max<int64_t>(woff[fd.S], 1)) + 64);
+  mark(s, 4);
   for (int sI = 0; sI < fd.S; ++sI) {
     const int64_t rows = s->species_count[sI];
     const GapSpecies & g = m->segs[sI];
@@ -1008,6 +1034,8 @@ static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * 
                  m->T64.as<double>() + size_t(g.m0) * fd.Dpad, fd.Dpad, s->W64.as<double>() + woff[sI], g.M, st);
     launch_kernel_weight(rows * g.M, s->W64.as<double>() + woff[sI], m->zeta, st);
   }
+  mark(s, 5);
+  mark(s, 6);
   // The reference returns from its loop over structures at the first one
   // whose centre species have no sparse points (models/sparse_kernels.hh:
   // 347-349): that structure and all later ones keep zero rows.
@@ -1025,7 +1053,8 @@ static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * 
   }
   const std::vector<int64_t> & poff = pair_offsets_host(s);
   const size_t per_pair = sizeof(double) * (3 * size_t(fd.D) + 3 * size_t(fd.nK));
-  const size_t per_center = sizeof(double) * size_t(fd.S) * 3 * fd.nK;
+  const size_t per_center =
+      sizeof(double) * (size_t(fd.S) * 3 * fd.nK + (neg_stress ? 6 * size_t(fd.D) : 0));
   const size_t budget = plain_budget_bytes();
   ExpansionArgs ea = exp_args(c, s);
   PsArgs pa;
@@ -1033,7 +1062,7 @@ static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * 
   pa.n_centers = nc;
   pa.normalize = c->hy.normalize;
   pa.row_of_center = s->row_of_center.as<int32_t>();
-  std::vector<std::vector<int32_t>> lists(fd.S);
+  std::vector<std::vector<int32_t>> lists(fd.S), centres(fd.S);
   int64_t c0 = 0;
   while (c0 < c_stop) {
     int64_t c1 = c0;
@@ -1048,21 +1077,32 @@ static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * 
     const int64_t np = poff[c1] - p_base;
     // pairs of the chunk listed by the species of their centre: (pair - p_base, centre)
     for (auto & l : lists) l.clear();
+    for (auto & l : centres) l.clear();
     for (int64_t ci = c0; ci < c1; ++ci) {
-      std::vector<int32_t> & l = lists[sp_index[s->types[ci]]];
+      const int sI = sp_index[s->types[ci]];
+      std::vector<int32_t> & l = lists[sI];
+      centres[sI].push_back(int32_t(ci));
       for (int64_t p = poff[ci]; p < poff[ci + 1]; ++p) {
         l.push_back(int32_t(p - p_base));
         l.push_back(int32_t(ci));
       }
     }
+    // one upload: [pair lists of all species][centre lists of all species]
     std::vector<int32_t> flat;
-    std::vector<int64_t> loff(fd.S + 1, 0);
+    std::vector<int64_t> loff(fd.S + 1, 0), coff(fd.S + 1, 0);
     for (int sI = 0; sI < fd.S; ++sI) {
       loff[sI] = int64_t(flat.size()) / 2;
       flat.insert(flat.end(), lists[sI].begin(), lists[sI].end());
     }
     loff[fd.S] = int64_t(flat.size()) / 2;
+    const int64_t cbase = int64_t(flat.size());
+    for (int sI = 0; sI < fd.S; ++sI) {
+      coff[sI] = int64_t(flat.size()) - cbase;
+      flat.insert(flat.end(), centres[sI].begin(), centres[sI].end());
+    }
+    coff[fd.S] = int64_t(flat.size()) - cbase;
     upload(s, s->plist, flat.data(), sizeof(int32_t) * flat.size());
+    if (neg_stress) s->Vvir.ensure(sizeof(double) * 6 * size_t(fd.D) * size_t(c1 - c0) + 64);
     s->dCp.ensure(sizeof(double) * size_t(np) * 3 * fd.nK + 64);
     s->dCs.ensure(per_center * size_t(c1 - c0) + 64);
     s->dXp.ensure(sizeof(double) * size_t(np) * 3 * fd.D + 64);
@@ -1090,16 +1130,36 @@ static void sparse_kernel_derivative_impl(rgpu_gap_model * m, rgpu_structures * 
       a.ucol = m->ucol.as<int32_t>() + g.m0;
       a.out = s->knm.as<double>();
       a.ldo = M;
-      if (neg_stress) {
-        a.pair_dist = s->nl.pair_dist;
-        a.pair_dir = s->nl.pair_dir;
-        a.center_struct = s->nl.center_struct;
-        a.stress_row0 = 3 * nc;
-      }
       launch_knm_derivative(a, st);
+      if (neg_stress) {
+        KnmStressArgs b{};
+        b.centres = s->plist.as<int32_t>() + cbase + coff[sI];
+        b.n_centres = coff[sI + 1] - coff[sI];
+        b.p_base = p_base;
+        b.pair_off = s->nl.pair_off;
+        b.pair_dist = s->nl.pair_dist;
+        b.pair_dir = s->nl.pair_dir;
+        b.dX = s->dXp.as<double>();
+        b.D = fd.D;
+        b.V = s->Vvir.as<double>();
+        b.T = a.T;
+        b.ldt = a.ldt;
+        b.M = g.M;
+        b.W = a.W;
+        b.row0 = a.row0;
+        b.row_of_center = a.row_of_center;
+        b.center_struct = s->nl.center_struct;
+        b.ucol = a.ucol;
+        b.out = a.out;
+        b.ldo = M;
+        b.stress_row0 = 3 * nc;
+        launch_knm_stress(b, st);
+      }
     }
     c0 = c1;
   }
+  mark(s, 7);
+  mark(s, 8);
   RGPU_CUDA(cudaMemcpyAsync(out, s->knm.p, bytes, cudaMemcpyDeviceToHost, st));
   RGPU_CUDA(cudaStreamSynchronize(st));
   if (neg_stress)

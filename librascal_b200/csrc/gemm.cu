@@ -7,7 +7,8 @@
 // models/sparse_kernel_predict.hh:141-143, done for all centres at once).
 //
 // Two implementations:
-//  * FP64 SIMT tiles for the plain path (the reference's arithmetic);
+//  * FP64 SIMT tiles for the plain path (the reference's arithmetic,
+//    dgemm.cuh);
 //  * TF32 tensor-core tiles (mma.sync m16n8k8) with FP32 accumulation for
 //    the fast path, optionally as a 3-term split (hi*hi + hi*lo + lo*hi) that
 //    carries ~21 mantissa bits. The forward epilogue fuses k^zeta, the
@@ -15,75 +16,10 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "dgemm.cuh"
 
 namespace rgpu {
 namespace {
-
-// ----------------------------------------------------------- FP64 SIMT GEMM
-constexpr int kT = 64, kBK = 16;
-
-template <bool NT>
-__global__ void __launch_bounds__(256)
-gemm_fp64_kernel(int64_t M, int64_t N, int64_t K, const double * __restrict__ A, int64_t lda,
-                 const double * __restrict__ B, int64_t ldb, double * __restrict__ C, int64_t ldc) {
-  __shared__ double As[kBK][kT + 1];
-  __shared__ double Bs[kBK][kT + 1];
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int64_t r0 = int64_t(blockIdx.y) * kT, c0 = int64_t(blockIdx.x) * kT;
-  double acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.;
-  for (int64_t k0 = 0; k0 < K; k0 += kBK) {
-    // A tile: 64 rows x 16 k, 4 loads per thread
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      int idx = threadIdx.x + q * 256;
-      int r = idx / kBK, k = idx % kBK;
-      int64_t gr = r0 + r, gk = k0 + k;
-      As[k][r] = (gr < M && gk < K) ? A[gr * lda + gk] : 0.;
-    }
-    if (NT) {
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        int idx = threadIdx.x + q * 256;
-        int c = idx / kBK, k = idx % kBK;
-        int64_t gc = c0 + c, gk = k0 + k;
-        Bs[k][c] = (gc < N && gk < K) ? B[gc * ldb + gk] : 0.;
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        int idx = threadIdx.x + q * 256;
-        int k = idx / kT, c = idx % kT;
-        int64_t gc = c0 + c, gk = k0 + k;
-        Bs[k][c] = (gc < N && gk < K) ? B[gk * ldb + gc] : 0.;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kBK; ++k) {
-      double a[4], b[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[k][ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[k][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += a[i] * b[j];
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      int64_t gr = r0 + ty + 16 * i, gc = c0 + tx + 16 * j;
-      if (gr < M && gc < N) C[gr * ldc + gc] = acc[i][j];
-    }
-}
 
 __device__ __forceinline__ float pow_zeta_f(float v, int z) {
   float r = 1.f;
@@ -363,19 +299,11 @@ __global__ void pair_center2_kernel(int64_t c0, int64_t c1, const int64_t * __re
 
 void gemm_nt_fp64(int64_t M, int64_t N, int64_t K, const double * A, int64_t lda, const double * B,
                   int64_t ldb, double * C, int64_t ldc, cudaStream_t st) {
-  if (M <= 0 || N <= 0) return;
-  dim3 grid(div_up(N, kT), div_up(M, kT));
-  gemm_fp64_kernel<true><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc);
-  RGPU_LAUNCHED();
-  RGPU_CUDA(cudaGetLastError());
+  launch_dgemm<true>(M, int(N), int(K), A, DgPlainRows{lda}, B, ldb, DgStoreC{C, ldc}, st);
 }
 void gemm_nn_fp64(int64_t M, int64_t N, int64_t K, const double * A, int64_t lda, const double * B,
                   int64_t ldb, double * C, int64_t ldc, cudaStream_t st) {
-  if (M <= 0 || N <= 0) return;
-  dim3 grid(div_up(N, kT), div_up(M, kT));
-  gemm_fp64_kernel<false><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc);
-  RGPU_LAUNCHED();
-  RGPU_CUDA(cudaGetLastError());
+  launch_dgemm<false>(M, int(N), int(K), A, DgPlainRows{lda}, B, ldb, DgStoreC{C, ldc}, st);
 }
 
 void launch_gap_pointwise_fp64(int64_t rows, int M, const double * Kmat, int64_t ldk,

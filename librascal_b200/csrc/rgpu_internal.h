@@ -339,13 +339,31 @@ struct KnmDerArgs {
   const int32_t * ucol;  // output column of each sparse point
   double * out;
   int64_t ldo;
-  // negative-stress rows (pair_dist == nullptr: none)
-  const double * pair_dist;
-  const double * pair_dir;
-  const int32_t * center_struct;
-  int64_t stress_row0;
 };
 void launch_knm_derivative(const KnmDerArgs & a, cudaStream_t st);
+// Negative-stress rows of one central species over one chunk: 6 virial rows
+// per centre into V, contracted with the sparse points.
+struct KnmStressArgs {
+  const int32_t * centres;  // centres of the species in the chunk
+  int64_t n_centres, p_base;
+  const int64_t * pair_off;
+  const double * pair_dist;
+  const double * pair_dir;
+  const double * dX;  // chunk [pair][3][D]
+  int D;
+  double * V;  // [n_centres][6][D] scratch
+  const double * T;
+  int64_t ldt;
+  int M;
+  const double * W;
+  int64_t row0;
+  const int32_t * row_of_center;
+  const int32_t * center_struct;
+  const int32_t * ucol;
+  double * out;
+  int64_t ldo, stress_row0;
+};
+void launch_knm_stress(const KnmStressArgs & a, cudaStream_t st);
 
 // Adjoint pair kernel: forces from dE/dC (FP32, the layout written by
 // launch_ps_bwd_fp32) and recomputed dC/dr. With stress, also the unscaled

@@ -7,17 +7,18 @@
 //   K_MM                models/sparse_kernels.hh:141-156 with
 //                       models/sparse_points.hh:144-170.
 //
-// The dot products X T^T and T T^T run through the FP64 tile GEMM of
-// gemm.cu. The gradient block is one gathered GEMM per central species and
-// chunk of pairs: its A rows are the materialised dX_i/dr_j[c] (3 rows per
-// pair, pairs listed by the species of their centre), its B rows the sparse
-// points of that species. The epilogue scales each entry by
-// zeta (X_i . T_m)^(zeta-1), adds it into row 3j + c of the output and, for
-// the stress rows, reduces r_ji (x) entry over the tile's rows of one
-// structure before one atomic add per (structure, Voigt entry, column).
+// All products run through the FP64 tile GEMM of dgemm.cuh. The gradient
+// block is one gathered GEMM per central species and chunk of pairs: its A
+// rows are the materialised dX_i/dr_j[c] (3 rows per pair, pairs listed by
+// the species of their centre), its B rows the sparse points of that
+// species; the epilogue scales each entry by zeta (X_i . T_m)^(zeta-1) and
+// adds it into row 3j + c of the output. The stress rows come from a second,
+// smaller GEMM over 6 virial rows per centre (sum over its pairs of r_ji
+// times dX_i/dr_j), whose epilogue adds into the centre's structure.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "dgemm.cuh"
 
 namespace rgpu {
 namespace {
@@ -56,133 +57,103 @@ __global__ void kmm_scatter_kernel(int M, const double * __restrict__ K, int zet
   out[int64_t(ucol[a]) * ldo + ucol[b]] = pow_zeta_d(K[i], zeta);
 }
 
-constexpr int kDT = 64, kDK = 16;
+// A rows of the gradient block: row 3k + c is dX_i/dr_j[c] of pair list[2k].
+struct PairRows {
+  const int32_t * list;
+  int D;
+  __device__ __forceinline__ int64_t operator()(int64_t r) const {
+    const int64_t k = r / 3;
+    return (int64_t(list[2 * k]) * 3 + (r - 3 * k)) * D;
+  }
+};
 
-// Gathered GEMM of the gradient block: tile of 64 (pair, component) rows x
-// 64 sparse points, 256 threads with a 4 x 4 register tile each.
-template <bool STRESS>
+// Entry (3k + c, m): scaled by zeta k_im^(zeta-1) and added into row 3j + c.
+struct PairScatter {
+  const int32_t * list;
+  int64_t p_base, row0;
+  const int32_t * row_of_center;
+  const double * W;
+  int M;
+  const int32_t * pair_j;
+  const int32_t * ucol;
+  double * out;
+  int64_t ldo;
+  __device__ __forceinline__ void operator()(int64_t r, int m, double v) const {
+    const int64_t k = r / 3;
+    const int c = int(r - 3 * k);
+    const int64_t ci = list[2 * k + 1];
+    const double w = W[(int64_t(row_of_center[ci]) - row0) * M + m];
+    const int64_t j = pair_j[p_base + list[2 * k]];
+    atomicAdd(&out[(3 * j + c) * ldo + ucol[m]], v * w);
+  }
+};
+
+// Entry (6k + e, m) of the stress GEMM: scaled like the pair entries and
+// added into Voigt row e of the centre's structure.
+struct StressScatter {
+  const int32_t * centres;
+  int64_t row0, stress_row0;
+  const int32_t * row_of_center;
+  const double * W;
+  int M;
+  const int32_t * center_struct;
+  const int32_t * ucol;
+  double * out;
+  int64_t ldo;
+  __device__ __forceinline__ void operator()(int64_t r, int m, double v) const {
+    const int64_t k = r / 6;
+    const int e = int(r - 6 * k);
+    const int64_t ci = centres[k];
+    const double w = W[(int64_t(row_of_center[ci]) - row0) * M + m];
+    atomicAdd(&out[(stress_row0 + 6 * int64_t(center_struct[ci]) + e) * ldo + ucol[m]], v * w);
+  }
+};
+
+// Virial rows of a centre i: V[e][d] = sum over its pairs of r_ji[a_e] *
+// dX_i/dr_j[b_e][d], Voigt e = xx, yy, zz, yz, xz, xy with (a, b) = (x, x),
+// (y, y), (z, z), (y, z), (z, x), (x, y) (models/sparse_kernels.hh:405-425).
+// Contracting V with T_m gives the stress entries of the centre, since the
+// scale zeta k_im^(zeta-1) is the same for all its pairs.
 __global__ void __launch_bounds__(256)
-knm_derivative_kernel(const KnmDerArgs a) {
-  // As/Bs during the main loop; the scaled 64 x 64 tile in the stress epilogue
-  __shared__ double sm[kDT * (kDT + 1)];
-  __shared__ int64_t a_off[kDT];
-  __shared__ int32_t r_struct[kDT];
-  __shared__ double r_vec[kDT][3];
-  double (*As)[kDT + 1] = reinterpret_cast<double (*)[kDT + 1]>(sm);
-  double (*Bs)[kDT + 1] = reinterpret_cast<double (*)[kDT + 1]>(sm + kDK * (kDT + 1));
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int64_t n_rows = 3 * a.n_list;
-  const int64_t r0 = int64_t(blockIdx.x) * kDT;
-  const int c0 = int(blockIdx.y) * kDT;
-  if (threadIdx.x < kDT) {
-    const int64_t gr = r0 + threadIdx.x;
-    int64_t off = -1;
-    if (gr < n_rows) {
-      const int64_t k = gr / 3;
-      const int c = int(gr - 3 * k);
-      const int64_t pl = a.list[2 * k];
-      off = (pl * 3 + c) * int64_t(a.D);
-      if (STRESS) {
-        const int64_t p = a.p_base + pl;
-        const double r = a.pair_dist[p];
-        // r_ji = r_i - r_j = -r * dir
-        r_vec[threadIdx.x][0] = -r * a.pair_dir[3 * p];
-        r_vec[threadIdx.x][1] = -r * a.pair_dir[3 * p + 1];
-        r_vec[threadIdx.x][2] = -r * a.pair_dir[3 * p + 2];
-        r_struct[threadIdx.x] = a.center_struct[a.list[2 * k + 1]];
-      }
-    }
-    a_off[threadIdx.x] = off;
-  }
-  __syncthreads();
-  double acc[4][4];
+virial_rows_kernel(const int32_t * __restrict__ centres, int64_t n, const int64_t * __restrict__ pair_off,
+                   int64_t p_base, const double * __restrict__ pair_dist, const double * __restrict__ pair_dir,
+                   const double * __restrict__ dX, int D, double * __restrict__ V) {
+  constexpr int kMaxP = 64;
+  __shared__ double rv[kMaxP][3];
+  const int64_t k = blockIdx.x;
+  if (k >= n) return;
+  const int64_t ci = centres[k];
+  const int64_t p0 = pair_off[ci], p1 = pair_off[ci + 1];
+  double * out = V + k * 6 * int64_t(D);
+  for (int d = threadIdx.x; d < D; d += blockDim.x)
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = 0.;
-  for (int k0 = 0; k0 < a.D; k0 += kDK) {
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int idx = threadIdx.x + q * 256;
-      const int r = idx / kDK, k = idx % kDK;
-      const int64_t off = a_off[r];
-      As[k][r] = (off >= 0 && k0 + k < a.D) ? a.dX[off + k0 + k] : 0.;
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int idx = threadIdx.x + q * 256;
-      const int c = idx / kDK, k = idx % kDK;
-      const int gc = c0 + c;
-      Bs[k][c] = (gc < a.M && k0 + k < a.D) ? a.T[int64_t(gc) * a.ldt + k0 + k] : 0.;
+    for (int e = 0; e < 6; ++e) out[int64_t(e) * D + d] = 0.;
+  for (int64_t q0 = p0; q0 < p1; q0 += kMaxP) {
+    const int np = p1 - q0 < kMaxP ? int(p1 - q0) : kMaxP;
+    __syncthreads();
+    if (threadIdx.x < np) {
+      const int64_t p = q0 + threadIdx.x;
+      const double r = pair_dist[p];
+      rv[threadIdx.x][0] = -r * pair_dir[3 * p];
+      rv[threadIdx.x][1] = -r * pair_dir[3 * p + 1];
+      rv[threadIdx.x][2] = -r * pair_dir[3 * p + 2];
     }
     __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kDK; ++k) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) av[i] = As[k][ty + 16 * i];
-#pragma unroll
-      for (int j = 0; j < 4; ++j) bv[j] = Bs[k][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] += av[i] * bv[j];
-    }
-    __syncthreads();
-  }
-  // epilogue: scale by W, add into the atom rows, keep the tile for the stress
-  double (*V)[kDT + 1] = reinterpret_cast<double (*)[kDT + 1]>(sm);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int rl = ty + 16 * i;
-    const int64_t gr = r0 + rl;
-    const bool row_ok = gr < n_rows;
-    int64_t k = 0, ci = 0, wrow = 0, j = 0;
-    int c = 0;
-    if (row_ok) {
-      k = gr / 3;
-      c = int(gr - 3 * k);
-      ci = a.list[2 * k + 1];
-      wrow = int64_t(a.row_of_center[ci]) - a.row0;
-      j = a.pair_j[a.p_base + a.list[2 * k]];
-    }
-#pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      const int cl = tx + 16 * jj;
-      const int gc = c0 + cl;
-      double v = 0.;
-      if (row_ok && gc < a.M) {
-        v = acc[i][jj] * a.W[wrow * a.M + gc];
-        atomicAdd(&a.out[(3 * j + c) * a.ldo + a.ucol[gc]], v);
+    for (int d = threadIdx.x; d < D; d += blockDim.x) {
+      double v[6] = {0., 0., 0., 0., 0., 0.};
+      for (int q = 0; q < np; ++q) {
+        const double * g = dX + (q0 + q - p_base) * 3 * int64_t(D) + d;
+        const double gx = g[0], gy = g[D], gz = g[2 * int64_t(D)];
+        v[0] += rv[q][0] * gx;
+        v[1] += rv[q][1] * gy;
+        v[2] += rv[q][2] * gz;
+        v[3] += rv[q][1] * gz;
+        v[4] += rv[q][2] * gx;
+        v[5] += rv[q][0] * gy;
       }
-      if (STRESS) V[rl][cl] = v;
+#pragma unroll
+      for (int e = 0; e < 6; ++e) out[int64_t(e) * D + d] += v[e];
     }
-  }
-  if (!STRESS) return;
-  __syncthreads();
-  // Voigt xx, yy, zz, yz, xz, xy: entry e takes component c_of[e] of the
-  // pair term times r_ji[d_of[e]] (models/sparse_kernels.hh:405-425)
-  const int64_t rem = n_rows - r0;
-  const int rows_here = rem < kDT ? int(rem) : kDT;
-  for (int t = threadIdx.x; t < 6 * kDT; t += blockDim.x) {
-    const int cl = t % kDT, e = t / kDT;
-    const int gc = c0 + cl;
-    if (gc >= a.M) continue;
-    const int c_of = e < 3 ? e : (e == 3 ? 2 : (e == 4 ? 0 : 1));
-    const int d_of = e < 3 ? e : (e == 3 ? 1 : (e == 4 ? 2 : 0));
-    double sum = 0.;
-    int cur = -1;
-    for (int rl = 0; rl < rows_here; ++rl) {
-      if (int((r0 + rl) % 3) != c_of) continue;
-      const int sidx = r_struct[rl];
-      if (sidx != cur) {
-        if (cur >= 0) atomicAdd(&a.out[(a.stress_row0 + 6 * int64_t(cur) + e) * a.ldo + a.ucol[gc]], sum);
-        cur = sidx;
-        sum = 0.;
-      }
-      sum += r_vec[rl][d_of] * V[rl][cl];
-    }
-    if (cur >= 0) atomicAdd(&a.out[(a.stress_row0 + 6 * int64_t(cur) + e) * a.ldo + a.ucol[gc]], sum);
   }
 }
 
@@ -215,17 +186,19 @@ void launch_kmm_scatter(int M, const double * K, int zeta, const int32_t * ucol,
 
 void launch_knm_derivative(const KnmDerArgs & a, cudaStream_t st) {
   if (a.n_list <= 0 || a.M <= 0) return;
-  const int64_t row_tiles = (3 * a.n_list + kDT - 1) / kDT;
-  const int col_tiles = div_up(a.M, kDT);
-  if (row_tiles > 0x7fffffff || col_tiles > 65535)
-    throw Error(RGPU_ERR_CAPACITY, "kernel gradient block: too many rows or sparse points for one launch");
-  const dim3 grid{static_cast<unsigned>(row_tiles), static_cast<unsigned>(col_tiles), 1u};
-  if (a.pair_dist)
-    knm_derivative_kernel<true><<<grid, 256, 0, st>>>(a);
-  else
-    knm_derivative_kernel<false><<<grid, 256, 0, st>>>(a);
+  PairScatter epi{a.list, a.p_base, a.row0, a.row_of_center, a.W, a.M, a.pair_j, a.ucol, a.out, a.ldo};
+  launch_dgemm<true>(3 * a.n_list, a.M, a.D, a.dX, PairRows{a.list, a.D}, a.T, a.ldt, epi, st);
+}
+
+void launch_knm_stress(const KnmStressArgs & a, cudaStream_t st) {
+  if (a.n_centres <= 0 || a.M <= 0) return;
+  virial_rows_kernel<<<unsigned(a.n_centres), 256, 0, st>>>(a.centres, a.n_centres, a.pair_off, a.p_base,
+                                                          a.pair_dist, a.pair_dir, a.dX, a.D, a.V);
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
+  StressScatter epi{a.centres, a.row0, a.stress_row0, a.row_of_center, a.W, a.M, a.center_struct, a.ucol,
+                    a.out, a.ldo};
+  launch_dgemm<true>(6 * a.n_centres, a.M, a.D, a.V, DgPlainRows{a.D}, a.T, a.ldt, epi, st);
 }
 
 }  // namespace rgpu

@@ -37,6 +37,7 @@ class SparsePoints:
         self._representation = representation
         self.species = []       # central species of each point
         self.values = []        # dict key -> vector, per point
+        self._models = {}       # zeta -> GAPModel with zero weights (kernel matrices)
 
     def _group_by_species(self):
         """Points of one species together, species ascending, insertion
@@ -45,6 +46,7 @@ class SparsePoints:
         order = sorted(range(len(self.species)), key=lambda i: self.species[i])
         self.species = [self.species[i] for i in order]
         self.values = [self.values[i] for i in order]
+        self._models = {}  # device copies made by Kernel, now stale
 
     def size(self):
         return len(self.species)
@@ -147,7 +149,14 @@ class Kernel:
         self.zeta = int(zeta)
 
     def _model(self, sparse_points):
-        return GAPModel(self._representation, sparse_points, None, self.zeta)
+        """A zero-weight model holding the sparse points on the device, kept
+        with the sparse points until they change."""
+        key = (id(self._representation), self.zeta)
+        model = sparse_points._models.get(key)
+        if model is None:
+            model = GAPModel(self._representation, sparse_points, None, self.zeta)
+            sparse_points._models[key] = model
+        return model
 
     def __call__(self, X, Y=None, grad=(False, False), compute_neg_stress=False):
         if Y is None and grad == (False, False):
