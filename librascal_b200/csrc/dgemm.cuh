@@ -40,8 +40,10 @@ dgemm_kernel(int64_t M, int N, int K, const double * __restrict__ A, ARows arows
   __shared__ int64_t a_off[kDgBM];
   const int t = threadIdx.x;
   const int tx = t & 15, ty = t >> 4;
-  const int64_t r0 = int64_t(blockIdx.x) * kDgBM;
-  const int c0 = int(blockIdx.y) * kDgBN;
+  // column tiles vary fastest: the blocks that share an A row tile run
+  // together, so A comes from DRAM once and the others read it from L2
+  const int64_t r0 = int64_t(blockIdx.y) * kDgBM;
+  const int c0 = int(blockIdx.x) * kDgBN;
   if (t < kDgBM) a_off[t] = (r0 + t < M) ? arows(r0 + t) : int64_t(-1);
   __syncthreads();
   // global -> register loaders: A and B_NT tiles, 2 threads per row, 4 k each
@@ -135,9 +137,9 @@ void launch_dgemm(int64_t M, int N, int K, const double * A, ARows arows, const 
   if (M <= 0 || N <= 0) return;
   const int64_t row_tiles = (M + kDgBM - 1) / kDgBM;
   const int col_tiles = div_up(N, kDgBN);
-  if (row_tiles > 0x7fffffff || col_tiles > 65535)
-    throw Error(RGPU_ERR_CAPACITY, "FP64 GEMM: too many rows or columns for one launch");
-  const dim3 grid{static_cast<unsigned>(row_tiles), static_cast<unsigned>(col_tiles), 1u};
+  if (row_tiles > 65535 || col_tiles > 0x7fffffff)
+    throw Error(RGPU_ERR_CAPACITY, "FP64 GEMM: too many rows for one launch");
+  const dim3 grid{static_cast<unsigned>(col_tiles), static_cast<unsigned>(row_tiles), 1u};
   dgemm_kernel<B_NT><<<grid, 256, 0, st>>>(M, N, K, A, arows, B, ldb, epi);
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
