@@ -69,7 +69,14 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
       const double r = a.pair_dist[p];
       j = a.pair_j[p];
       const int s = a.species_lut[a.types[j]];
-      const float fc = fc_cos_f(r, a.rc, a.sw), dfc = dfc_cos_f(r, a.rc, a.sw);
+      float fc = fc_cos_f(r, a.rc, a.sw), dfc = dfc_cos_f(r, a.rc, a.sw);
+      if (a.rs.on) {
+        const double u = rs_value(a.rs, r);
+        const double cosw = 0.5 * (1. + cos(3.14159265358979323846264338327950288 * (r - a.rc + a.sw) / a.sw));
+        const double sr = (r <= a.rc - a.sw) ? 1.0 : (r > a.rc ? 0.0 : cosw);
+        dfc = float(rs_grad(a.rs, r) * sr + u * double(dfc));
+        fc = float(u * sr);
+      }
       const SplinePos q = spline_pos(a.sp, r);
       const float aa = float(q.a), bb = float(q.b);
       const float ca = aa * aa - 1.f, cb = bb * bb - 1.f;

@@ -103,12 +103,20 @@ void parse_hypers(const std::string & kind, const std::string & text, Hypers & h
   }
   const Json & fc = j.at("cutoff_function");
   std::string fct = fc.at("type").as_string();
-  if (fct != "ShiftedCosine")
+  if (fct != "ShiftedCosine" && fct != "RadialScaling")
     throw Error(RGPU_ERR_INVALID_ARGUMENT,
                 "Requested cutoff function type '" + fct + "' is not on the B200 path. Supported: "
-                                                          "'ShiftedCosine'.");
+                                                          "'ShiftedCosine', 'RadialScaling'.");
   h.cutoff = fc.at("cutoff").at("value").as_number();
   h.smooth_width = fc.at("smooth_width").at("value").as_number();
+  h.radial_scaling = fct == "RadialScaling";
+  if (h.radial_scaling) {
+    // representations/cutoff_functions.hh:243-253
+    h.rs_rate = fc.at("rate").at("value").as_number();
+    if (h.rs_rate < 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "RadialScaling's rate should be positive");
+    h.rs_exponent = fc.at("exponent").at("value").as_number();
+    h.rs_scale = fc.at("scale").at("value").as_number();
+  }
   const Json & gd = j.at("gaussian_density");
   std::string gt = gd.at("type").as_string();
   if (gt != "Constant")
@@ -349,6 +357,10 @@ ExpansionArgs exp_args(const rgpu_calculator * c, const rgpu_structures * s) {
   a.species_lut = s->lut.as<int8_t>();
   a.rc = c->hy.cutoff;
   a.sw = c->hy.smooth_width;
+  a.rs.on = c->hy.radial_scaling ? 1 : 0;
+  a.rs.rate = c->hy.rs_rate;
+  a.rs.exponent = c->hy.rs_exponent;
+  a.rs.scale = c->hy.rs_scale;
   a.n_centers = s->nl.n_centers;
   a.center_atom = s->nl.center_atom;
   a.pair_off = s->nl.pair_off;

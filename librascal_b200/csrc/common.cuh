@@ -40,6 +40,24 @@ __device__ __forceinline__ float to_tf32(float x) {
 
 inline int div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }
 
+// Radial factor u(r) of the RadialScaling cutoff and its derivative
+// (representations/cutoff_functions.hh:178-280): c / (c + (r/r0)^m), or
+// (r/r0)^-m when c is zero (|c| <= 100 eps, the reference's test), or 1 when
+// m is zero. It multiplies the shifted cosine; the products below follow the
+// reference's order: f_c = u * s, df_c = u' * s + u * s'.
+__device__ __forceinline__ double rs_value(const RadialScalingDev & p, double r) {
+  if (fabs(p.rate) <= 100.0 * 2.220446049250313e-16) return 1.0 / pow(r / p.scale, p.exponent);
+  if (p.exponent == 0.0) return 1.0;
+  return p.rate / (p.rate + pow(r / p.scale, p.exponent));
+}
+__device__ __forceinline__ double rs_grad(const RadialScalingDev & p, double r) {
+  if (fabs(p.rate) <= 100.0 * 2.220446049250313e-16) return -p.exponent / r / pow(r / p.scale, p.exponent);
+  if (p.exponent == 0.0) return 0.0;
+  const double ff = pow(r / p.scale, p.exponent);
+  const double d = p.rate + ff;
+  return -p.rate * p.exponent * ff / r / (d * d);
+}
+
 // v^zeta of the GAP kernel (models/kernels.hh:48-61)
 __device__ __forceinline__ double pow_zeta_d(double v, int z) {
   if (z == 0) return 1.;

@@ -68,6 +68,23 @@ __device__ __forceinline__ double dfc_cos(double r, double rc, double sw) {
   double rs = 3.14159265358979323846264338327950288 * (r - rc + sw) / sw;
   return -0.5 * 3.14159265358979323846264338327950288 / sw * sin(rs);
 }
+// the cutoff function of the calculator: shifted cosine, times the
+// RadialScaling factor when that is the cutoff type
+__device__ __forceinline__ double cutoff_fc(const ExpansionArgs & a, double r) {
+  const double s = fc_cos(r, a.rc, a.sw);
+  return a.rs.on ? rs_value(a.rs, r) * s : s;
+}
+__device__ __forceinline__ void cutoff_fc_dfc(const ExpansionArgs & a, double r, double & fc, double & dfc) {
+  const double s = fc_cos(r, a.rc, a.sw), ds = dfc_cos(r, a.rc, a.sw);
+  if (a.rs.on) {
+    const double u = rs_value(a.rs, r);
+    fc = u * s;
+    dfc = rs_grad(a.rs, r) * s + u * ds;
+  } else {
+    fc = s;
+    dfc = ds;
+  }
+}
 
 // Evaluate RI (and optionally dRI) of all W channels at r into smem columns.
 template <typename T, bool DER>
@@ -136,7 +153,7 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
         const int64_t p = p0 + lane;
         const double r = a.pair_dist[p];
         my_sp = a.species_lut[a.types[a.pair_j[p]]];
-        FC[lane] = T(fc_cos(r, a.rc, a.sw));
+        FC[lane] = T(cutoff_fc(a, r));
         spline_eval<T, false>(a.sp, r, RI + lane, nullptr, kPad);
         const T dx = T(a.pair_dir[3 * p]), dy = T(a.pair_dir[3 * p + 1]),
                 dz = T(a.pair_dir[3 * p + 2]);
@@ -247,7 +264,7 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
         pk_s[wid][lane] = q.k;
         pa_s[wid][lane] = float(q.a);
         pb_s[wid][lane] = float(q.b);
-        fc_s[wid][lane] = float(fc_cos(r, a.rc, a.sw));
+        fc_s[wid][lane] = float(cutoff_fc(a, r));
         const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
                     dz = float(a.pair_dir[3 * p + 2]);
         spherical_harmonics<L, false, float>(dx, dy, dz, [&](int lm, float y, float, float, float) {
@@ -337,7 +354,8 @@ expansion_grad_kernel(ExpansionArgs a, int64_t c0, int64_t c1, int64_t p_base,
     const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
     for (int64_t p = p_lo + lane; p < p_hi; p += 32) {
       const double r = a.pair_dist[p];
-      const double fc = fc_cos(r, a.rc, a.sw), dfc = dfc_cos(r, a.rc, a.sw);
+      double fc, dfc;
+      cutoff_fc_dfc(a, r, fc, dfc);
       spline_eval<double, true>(a.sp, r, RI + lane, P1 + lane, 32);
       for (int c = 0; c < W; ++c) {
         // p1 = dRI f_c + RI df_c

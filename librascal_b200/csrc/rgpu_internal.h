@@ -40,6 +40,10 @@ struct Hypers {
   std::string soap_type{"PowerSpectrum"};
   int max_radial{0}, max_angular{0};
   double cutoff{0}, smooth_width{0}, sigma{0};
+  // cutoff_function "RadialScaling": u(r) = c / (c + (r/r0)^m) times the
+  // shifted cosine (rate c, scale r0, exponent m)
+  bool radial_scaling{false};
+  double rs_rate{0}, rs_scale{1}, rs_exponent{0};
   bool spline{true};
   double spline_accuracy{1e-8};
   bool normalize{true};
@@ -154,9 +158,15 @@ struct FeatureDims {
   int Dpad;   // D rounded up to 32
 };
 
+// RadialScaling cutoff parameters (on = 0: plain shifted cosine).
+struct RadialScalingDev {
+  int on;
+  double rate, exponent, scale;
+};
 struct ExpansionArgs {
   FeatureDims fd;
   SplineDev sp;
+  RadialScalingDev rs;
   const double * center_contrib;  // [n] / sqrt(4 pi) already applied
   const int8_t * species_lut;     // [130] -> species index or -1
   double rc, sw;

@@ -38,6 +38,7 @@ def lib():
         L.orc_calc_new.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int] * 3 + [
             ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]
         L.orc_calc_free.argtypes = [ctypes.c_void_p]
+        L.orc_calc_set_radial_scaling.argtypes = [ctypes.c_void_p] + [ctypes.c_double] * 3
         L.orc_calc_spline_size.argtypes = [ctypes.c_void_p]
         L.orc_calc_spline_table.argtypes = [ctypes.c_void_p, c_dbl_p, c_dbl_p, c_dbl_p]
         L.orc_calc_gto.argtypes = [ctypes.c_void_p, c_dbl_p, c_dbl_p, c_dbl_p]
@@ -97,7 +98,9 @@ class Calculator:
 
     def __init__(self, interaction_cutoff, cutoff_smooth_width, max_radial,
                  max_angular, gaussian_sigma_constant, spline=True,
-                 accuracy=1e-8, normalize=True):
+                 accuracy=1e-8, normalize=True, radial_scaling=None):
+        """radial_scaling: None for the shifted cosine, or a dict with rate,
+        scale and exponent for the RadialScaling cutoff."""
         self.rc = float(interaction_cutoff)
         self.n = int(max_radial)
         self.l = int(max_angular)
@@ -107,6 +110,9 @@ class Calculator:
                                     int(spline), float(accuracy), int(normalize), err, 512)
         if not self.h:
             raise RuntimeError(err.value.decode())
+        if radial_scaling is not None:
+            lib().orc_calc_set_radial_scaling(self.h, float(radial_scaling["rate"]),
+                                              float(radial_scaling["scale"]), float(radial_scaling["exponent"]))
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:

@@ -834,6 +834,29 @@ struct Calculator {
   double rc, sw, sigma, accuracy;
   int nmax, lmax;
   bool use_spline, normalize;
+  // RadialScaling cutoff (representations/cutoff_functions.hh:178-280):
+  // f_c(r) = u(r) * shifted cosine, u = c / (c + (r/r0)^m)
+  bool radial_scaling{false};
+  double rs_rate{0.}, rs_scale{1.}, rs_exponent{0.};
+  double rs_value(double r) const {
+    if (std::abs(rs_rate) <= DBL_FTOL) return 1. / std::pow(r / rs_scale, rs_exponent);
+    if (rs_exponent == 0) return 1.;
+    return rs_rate / (rs_rate + std::pow(r / rs_scale, rs_exponent));
+  }
+  double rs_grad(double r) const {
+    if (std::abs(rs_rate) <= DBL_FTOL) return -rs_exponent / r / std::pow(r / rs_scale, rs_exponent);
+    if (rs_exponent == 0) return 0.;
+    double ff = std::pow(r / rs_scale, rs_exponent);
+    return -rs_rate * rs_exponent * ff / r / pow_u(rs_rate + ff, 2);
+  }
+  // the calculator's cutoff function and its derivative (:258-272)
+  double f_c(double r) const {
+    return radial_scaling ? rs_value(r) * fc_cos(r, rc, sw) : fc_cos(r, rc, sw);
+  }
+  double df_c(double r) const {
+    if (!radial_scaling) return dfc_cos(r, rc, sw);
+    return rs_grad(r) * fc_cos(r, rc, sw) + rs_value(r) * dfc_cos(r, rc, sw);
+  }
   GTO gto;
   Spline * spline{nullptr};
   std::vector<double> center_final;  // ortho_norm^T * center (spline mode)
@@ -1229,7 +1252,7 @@ static void compute_run(Calculator & calc, Run & R, const double * pos,
       int tj = species_index(R.species, pr.j_type);
       sph.calc(pr.dir, R.grads);
       calc.radial(pr.dist, RI.data(), R.grads ? dRI.data() : nullptr);
-      double f_c = fc_cos(pr.dist, calc.rc, calc.sw);
+      double f_c = calc.f_c(pr.dist);
       double * Cij = Ci + tj * nK;
       int lb = 0;
       for (int l = 0; l < L1; ++l) {
@@ -1239,7 +1262,7 @@ static void compute_run(Calculator & calc, Run & R, const double * pos,
         lb += 2 * l + 1;
       }
       if (R.grads) {
-        double df_c = dfc_cos(pr.dist, calc.rc, calc.sw);
+        double df_c = calc.df_c(pr.dist);
         double * dCp = &R.dC[size_t(p) * S * 3 * nK] + size_t(tj) * 3 * nK;
         double * dCs = dCself + size_t(tj) * 3 * nK;
         bool not_image_of_center = R.pair_jglobal[p] != center_real;
@@ -1620,6 +1643,14 @@ void * orc_calc_new(double rc, double sw, double sigma, int nmax, int lmax,
 }
 
 void orc_calc_free(void * c) { delete static_cast<orc::Calculator *>(c); }
+
+void orc_calc_set_radial_scaling(void * c, double rate, double scale, double exponent) {
+  auto * C = static_cast<orc::Calculator *>(c);
+  C->radial_scaling = true;
+  C->rs_rate = rate;
+  C->rs_scale = scale;
+  C->rs_exponent = exponent;
+}
 
 int orc_calc_spline_size(void * c) {
   auto * calc = static_cast<orc::Calculator *>(c);

@@ -92,7 +92,7 @@ def main(ref_root):
                         alps=np.array([np.asarray(e["alps"]) for e in s]))
 
     structures = {}
-    # --- spherical expansion goldens: keep GTO + ShiftedCosine, no RDR
+    # --- spherical expansion goldens: GTO with the ShiftedCosine or RadialScaling cutoff, no RDR
     se = ubjson_reader.load(os.path.join(td, "spherical_expansion_reference.ubjson"))
     files = [os.path.basename(f) for f in se["filenames"]]
     for f in files:
@@ -107,8 +107,13 @@ def main(ref_root):
                 hy = e["hypers"]
                 rcontrib = hy["radial_contribution"]
                 opt = list(rcontrib.get("optimization", {}).keys())
-                if rcontrib["type"] != "GTO" or hy["cutoff_function"]["type"] != "ShiftedCosine":
+                cf = hy["cutoff_function"]
+                if rcontrib["type"] != "GTO" or cf["type"] not in ("ShiftedCosine", "RadialScaling"):
                     continue
+                rs = None
+                if cf["type"] == "RadialScaling":
+                    rs = dict(rate=float(cf["rate"]["value"]), scale=float(cf["scale"]["value"]),
+                              exponent=float(cf["exponent"]["value"]))
                 if "RadialDimReduction" in opt:
                     continue
                 spline = "Spline" in opt
@@ -118,7 +123,7 @@ def main(ref_root):
                     smooth_width=float(hy["cutoff_function"]["smooth_width"]["value"]),
                     sigma=float(hy["gaussian_density"]["gaussian_sigma"]["value"]),
                     max_radial=int(hy["max_radial"]), max_angular=int(hy["max_angular"]),
-                    spline=spline, accuracy=float(acc),
+                    spline=spline, accuracy=float(acc), radial_scaling=rs,
                     features=np.asarray(e["feature_matrix"], dtype=float)))
     np.savez_compressed(
         os.path.join(HERE, "expansion_reference.npz"),

@@ -22,17 +22,20 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def soap(rc=3.5, sw=0.5, n=4, l=3, sigma=0.4, spline=True, grads=False, normalize=True):
+def soap(rc=3.5, sw=0.5, n=4, l=3, sigma=0.4, spline=True, grads=False, normalize=True, rs=None):
+    """rs: None for the shifted cosine, or dict(rate, scale, exponent) for
+    the RadialScaling cutoff."""
     opt = dict(Spline=dict(accuracy=1e-8)) if spline else {}
+    cut = dict(cutoff_function_type="RadialScaling", cutoff_function_parameters=dict(rs)) if rs else {}
     return rb.SphericalInvariants(interaction_cutoff=rc, cutoff_smooth_width=sw, max_radial=n,
                                   max_angular=l, gaussian_sigma_type="Constant",
                                   gaussian_sigma_constant=sigma, optimization=opt,
-                                  compute_gradients=grads, normalize=normalize)
+                                  compute_gradients=grads, normalize=normalize, **cut)
 
 
-def oracle_calc(rc=3.5, sw=0.5, n=4, l=3, sigma=0.4, spline=True, normalize=True):
+def oracle_calc(rc=3.5, sw=0.5, n=4, l=3, sigma=0.4, spline=True, normalize=True, rs=None):
     return O.Calculator(rc, sw, n, l, sigma, spline=spline, normalize=normalize,
-                        accuracy=1e-8 if spline else 1e-8)
+                        accuracy=1e-8 if spline else 1e-8, radial_scaling=rs)
 
 
 def subset(batch, idx):
@@ -201,10 +204,12 @@ def test_expansion_golden_on_gpu():
     for i, m in enumerate(meta):
         batch = batch_from_frames(structs[m["structure"]])
         opt = dict(Spline=dict(accuracy=m["accuracy"])) if m["spline"] else {}
+        rs = m["radial_scaling"]
+        cut = dict(cutoff_function_type="RadialScaling", cutoff_function_parameters=dict(rs)) if rs else {}
         calc = rb.SphericalExpansion(interaction_cutoff=m["cutoff"], cutoff_smooth_width=m["smooth_width"],
                                      max_radial=m["max_radial"], max_angular=m["max_angular"],
                                      gaussian_sigma_type="Constant", gaussian_sigma_constant=m["sigma"],
-                                     optimization=opt)
+                                     optimization=opt, **cut)
         al = calc.transform(rb.AtomsList(rb.StructureSet(batch)))
         C = al.get_features(calc, keys=calc.get_keys(np.unique(batch["numbers"])))
         ref = z["features_%d" % i]
@@ -378,3 +383,41 @@ def test_empty_and_isolated_atoms():
     batch = batch_from_frames(frames)
     X, Xo, *_ = features_vs_oracle(batch, dict(rc=3.0, n=4, l=3, sigma=0.4))
     assert_features_close(Xo, X)
+
+
+RS = dict(rate=1.0, scale=4.5, exponent=4.0)
+
+
+@pytest.mark.parametrize("which", ["periodic_boxes", "molecule_clusters"])
+def test_radial_scaling_parity(which):
+    """The RadialScaling cutoff (the one of the reference's serialised GAP
+    model) on every GPU path: FP64 and FP32 features, FP64 power-spectrum
+    gradients, and GAP energies, forces and negative stress at both
+    precisions, against the oracle."""
+    if which == "periodic_boxes":
+        batch, kw = synthetic.periodic_boxes(n_struct=2, seed=6), dict(rc=4.5, n=6, l=4, sigma=0.4, rs=RS)
+    else:
+        batch, kw = synthetic.molecule_clusters(n_struct=12, seed=8), dict(rc=5.0, n=6, l=4, sigma=0.5, rs=RS)
+    X, Xo, al, calc, r0 = features_vs_oracle(batch, kw)
+    assert_features_close(Xo, X)
+    species = np.unique(batch["numbers"])
+    al32 = calc.transform(rb.AtomsList(rb.StructureSet(batch)), precision="fp32")
+    X32 = al32.get_features(calc, keys=calc.get_keys(species))
+    assert np.abs(X32 - Xo).max() <= 1e-5 * np.abs(Xo).max()
+    cg = soap(grads=True, **kw)
+    alg = cg.transform(rb.AtomsList(rb.StructureSet(batch)))
+    dX = alg.get_features_gradient(cg, keys=cg.get_keys(species))
+    r = O.Run(oracle_calc(**kw), batch, species, gradients=True)
+    ref = r.power_spectrum_gradient().reshape(dX.shape)
+    assert np.abs(dX - ref).max() <= 1e-10 * np.abs(ref).max()
+    rr, T, sps, alpha, _ = gap_setup(batch, kw, n_sparse=5)
+    E_ref, F_ref, NS_ref = rr.gap_stress(sps, T, alpha, 2)
+    sp = rb.SparsePoints(calc)
+    sp.add_dense(sps, T, calc.get_keys(species))
+    model = rb.GAPModel(calc, sp, alpha, 2)
+    st = rb.StructureSet(batch)
+    for prec, tol in [("fp64", 1e-10), ("fp32", 1e-4)]:
+        E, F, NS = model.predict_stress(st, prec)
+        assert np.abs(E - E_ref).max() <= tol * np.abs(E_ref).max(), prec
+        assert np.abs(F - F_ref).max() <= tol * np.abs(F_ref).max(), prec
+        assert np.abs(NS - NS_ref).max() <= tol * np.abs(NS_ref).max(), prec

@@ -82,11 +82,14 @@ def test_expansion_golden():
     z = np.load(os.path.join(GOLDEN, "expansion_reference.npz"))
     meta = json.loads(str(z["meta"]))
     structs = load_structures()
-    assert len(meta) == 16
+    # 16 ShiftedCosine and 16 RadialScaling cases, direct and spline
+    assert len(meta) == 32
+    assert sum(m["radial_scaling"] is not None for m in meta) == 16
     for i, m in enumerate(meta):
         b = batch_from_frames(structs[m["structure"]])
         calc = O.Calculator(m["cutoff"], m["smooth_width"], m["max_radial"], m["max_angular"],
-                            m["sigma"], spline=m["spline"], accuracy=m["accuracy"] or 1e-8)
+                            m["sigma"], spline=m["spline"], accuracy=m["accuracy"] or 1e-8,
+                            radial_scaling=m["radial_scaling"])
         r = O.Run(calc, b, np.unique(b["numbers"]))
         C = r.expansion().reshape(r.n_centers, -1)
         ref = z["features_%d" % i]
