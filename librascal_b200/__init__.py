@@ -14,8 +14,10 @@ from .models import (KRR, GAPModel, Kernel, SparsePoints, compute_KNM, compute_s
                      gap_energy, train_gap_model)
 from .neighbourlist import AtomsList, StructureSet, frames_to_batch  # noqa: F401
 from .representations import SphericalExpansion, SphericalInvariants  # noqa: F401
+from .io import dump_obj, load_obj, read_ase_json, read_extxyz  # noqa: F401
+from .genericmd import GenericMDCalculator  # noqa: F401
 
 __all__ = ["SphericalInvariants", "SphericalExpansion", "AtomsList", "StructureSet", "SparsePoints",
            "Kernel", "KRR", "GAPModel", "compute_sparse_kernel_gradients", "compute_KNM", "train_gap_model",
-           "gap_energy",
+           "gap_energy", "dump_obj", "load_obj", "read_ase_json", "read_extxyz", "GenericMDCalculator",
            "frames_to_batch"]

@@ -119,6 +119,57 @@ class SparsePoints:
     def get_features(self):
         return self.dense(self.get_species())
 
+    # --- serialisation in the reference's format (models/sparse_points.py,
+    # models/sparse_points.hh:456-498): per central species, per key, the
+    # rows of the points that have the key, with their index in the species
+    def _get_init_params(self):
+        return dict(representation=self._representation)
+
+    def _get_data(self):
+        inner = self._representation.inner_size()
+        species = sorted(set(self.species))
+        counters = [[z, 0] for z in range(130)]
+        values, indices, keys_sp, all_keys = [], [], [], set()
+        for sp in species:
+            points = [i for i, s in enumerate(self.species) if s == sp]
+            counters[sp][1] = len(points)
+            per_key = {}
+            for local, i in enumerate(points):
+                for key, blk in self.values[i].items():
+                    idx, val = per_key.setdefault(tuple(int(k) for k in key), ([], []))
+                    idx.append(local)
+                    val.extend(float(x) for x in blk)
+            ks = sorted(per_key)
+            all_keys.update(ks)
+            values.append([sp, [[list(k), per_key[k][1]] for k in ks]])
+            indices.append([sp, [[list(k), per_key[k][0]] for k in ks]])
+            keys_sp.append([sp, [list(k) for k in ks]])
+        return dict(sparse_points=dict(
+            name="rascal::SparsePointsBlockSparse<rascal::CalculatorSphericalInvariants>",
+            values=values, indices=indices, counters=counters, inner_size=inner, center_species=species,
+            keys=[list(k) for k in sorted(all_keys)], keys_sp=keys_sp))
+
+    def _set_data(self, data):
+        d = data["sparse_points"]
+        inner = int(d["inner_size"])
+        if inner != self._representation.inner_size():
+            raise RuntimeError("sparse points of inner size %d do not match the representation (%d)"
+                               % (inner, self._representation.inner_size()))
+        counts = {int(z): int(c) for z, c in d["counters"]}
+        indices = {int(sp): v for sp, v in d["indices"]}
+        self.species, self.values = [], []
+        for sp, per_key in sorted((int(sp), v) for sp, v in d["values"]):
+            points = [dict() for _ in range(counts.get(sp, 0))]
+            idx_of = {tuple(int(x) for x in k): idx for k, idx in indices[sp]}
+            for key, flat in per_key:
+                key = tuple(int(x) for x in key)
+                flat = np.asarray(flat, dtype=float).reshape(-1, inner)
+                for r, local in enumerate(idx_of[key]):
+                    points[int(local)][key] = flat[r].copy()
+            self.species.extend([sp] * len(points))
+            self.values.extend(points)
+        self._models = {}
+
 
 class Kernel:
     """GAP kernel (models/kernels.py:16-164), Sparse only. Every matrix is
@@ -147,6 +198,16 @@ class Kernel:
         self.kernel_type = kernel_type
         self.target_type = target_type
         self.zeta = int(zeta)
+
+    def _get_init_params(self):
+        return dict(representation=self._representation, name=self.name, kernel_type=self.kernel_type,
+                    target_type=self.target_type, zeta=self.zeta)
+
+    def _get_data(self):
+        return dict()
+
+    def _set_data(self, data):
+        pass
 
     def _model(self, sparse_points):
         """A zero-weight model holding the sparse points on the device, kept
@@ -255,6 +316,20 @@ class KRR:
         self.units.setdefault("length", "AA")
         self.precision = precision
         self._model = None
+
+    def _get_init_params(self):
+        return dict(weights=self.weights, kernel=self.kernel, X_train=self.X_train,
+                    self_contributions=self.self_contributions, description=self.description,
+                    units=self.units.copy())
+
+    def _get_data(self):
+        return dict()
+
+    def _set_data(self, data):
+        pass
+
+    def get_representation_calculator(self):
+        return self.kernel._representation
 
     def _gap(self):
         if self._model is None:

@@ -165,6 +165,30 @@ class SphericalInvariants(_Calculator):
         species = sorted(set(int(s) for s in species))
         return np.array([[a, b] for i, a in enumerate(species) for b in species[i:]], dtype=np.int32)
 
+    def _get_init_params(self):
+        """Constructor arguments, as the reference serialises them
+        (spherical_invariants.py:451-480)."""
+        gd, cf, rc = self.hypers["gaussian_density"], self.hypers["cutoff_function"], \
+            self.hypers["radial_contribution"]
+        p = dict(interaction_cutoff=cf["cutoff"]["value"], cutoff_smooth_width=cf["smooth_width"]["value"],
+                 max_radial=self.hypers["max_radial"], max_angular=self.hypers["max_angular"],
+                 soap_type=self.hypers["soap_type"], inversion_symmetry=self.hypers["inversion_symmetry"],
+                 normalize=self.hypers["normalize"],
+                 expansion_by_species_method=self.hypers["expansion_by_species_method"],
+                 global_species=self.hypers["global_species"], compute_gradients=self.hypers["compute_gradients"],
+                 gaussian_sigma_type=gd["type"], gaussian_sigma_constant=gd["gaussian_sigma"]["value"],
+                 cutoff_function_type=cf["type"], radial_basis=rc["type"], optimization=rc["optimization"],
+                 cutoff_function_parameters=self.cutoff_function_parameters)
+        if "coefficient_subselection" in self.hypers:
+            p["coefficient_subselection"] = self.hypers["coefficient_subselection"]
+        return p
+
+    def _get_data(self):
+        return dict()
+
+    def _set_data(self, data):
+        pass
+
 
 class SphericalExpansion(_Calculator):
     """Density expansion coefficients c^i_{a n lm} on the B200 path."""
@@ -177,6 +201,7 @@ class SphericalExpansion(_Calculator):
         self.name = "sphericalexpansion"
         if global_species is None:
             global_species = []
+        self.cutoff_function_parameters = deepcopy(cutoff_function_parameters)
         cutoff_function_parameters = dict(cutoff_function_parameters)
         cutoff_function_parameters.update(interaction_cutoff=interaction_cutoff,
                                           cutoff_smooth_width=cutoff_smooth_width)
@@ -209,3 +234,22 @@ class SphericalExpansion(_Calculator):
     def get_keys(self, species):
         species = sorted(set(int(s) for s in species))
         return np.array([[a, a] for a in species], dtype=np.int32)
+
+    def _get_init_params(self):
+        h = self.hypers
+        return dict(interaction_cutoff=h["interaction_cutoff"], cutoff_smooth_width=h["cutoff_smooth_width"],
+                    max_radial=h["max_radial"], max_angular=h["max_angular"],
+                    gaussian_sigma_type=h["gaussian_sigma_type"],
+                    gaussian_sigma_constant=h["gaussian_sigma_constant"],
+                    cutoff_function_type=h["cutoff_function"]["type"],
+                    radial_basis=h["radial_contribution"]["type"],
+                    optimization=h["radial_contribution"]["optimization"],
+                    expansion_by_species_method=h["expansion_by_species_method"],
+                    global_species=h["global_species"], compute_gradients=h["compute_gradients"],
+                    cutoff_function_parameters=self.cutoff_function_parameters)
+
+    def _get_data(self):
+        return dict()
+
+    def _set_data(self, data):
+        pass

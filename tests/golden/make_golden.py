@@ -19,8 +19,13 @@ Written files:
   sparse_kernel_inputs.json  parameters of the reference's sparse-kernel
                            gradient tests (tests/test_sparse_kernels.cc:129-220)
 
+  simple_gap_model.json, methane_dimer_sample.xyz
+                           the reference's serialised GAP model and its
+                           structures, copied unchanged
+                           (tests/python/md_calculator_test.py)
+
 `python tests/golden/make_golden.py <ref> sparse_kernel_inputs` rewrites only
-the last file.
+the sparse-kernel inputs, `... <ref> model_files` only the model files.
 """
 import json
 import os
@@ -70,6 +75,14 @@ def sparse_kernel_inputs(ref_root):
             zeta=int(e["kernel"]["zeta"]), target_type=e["kernel"]["target_type"],
             h=float(e["h"]), selected_ids=e["selected_ids"]))
     json.dump(cases, open(os.path.join(HERE, "sparse_kernel_inputs.json"), "w"), indent=1)
+
+
+def model_files(ref_root):
+    import shutil
+    shutil.copyfile(os.path.join(ref_root, "reference_data", "tests_only", "simple_gap_model.json"),
+                    os.path.join(HERE, "simple_gap_model.json"))
+    shutil.copyfile(os.path.join(ref_root, "reference_data", "inputs", "methane_dimer_sample.xyz"),
+                    os.path.join(HERE, "methane_dimer_sample.xyz"))
 
 
 def main(ref_root):
@@ -172,6 +185,10 @@ def main(ref_root):
 
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    if sys.argv[2:] != ["sparse_kernel_inputs"]:
+    only = sys.argv[2:]
+    if not only:
         main(root)
-    sparse_kernel_inputs(root)
+    if not only or only == ["sparse_kernel_inputs"]:
+        sparse_kernel_inputs(root)
+    if not only or only == ["model_files"]:
+        model_files(root)
