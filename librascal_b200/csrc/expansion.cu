@@ -21,6 +21,10 @@ namespace {
 
 constexpr int kWarps = 4;
 constexpr int kPad = 33;  // shared row stride of the per-pair tiles
+// The FP32 kernel takes pairs 16 at a time (most centres of the molecular
+// benchmark have fewer than 16 pairs), which halves its per-warp tiles and
+// doubles the warps that fit on an SM.
+constexpr int kChunkF = 16, kPadF = 17;
 
 template <typename T>
 struct Tab;
@@ -221,8 +225,8 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int W = a.fd.W, S = a.fd.S, n = a.fd.n;
-  float * RIf = reinterpret_cast<float *>(smem_raw) + size_t(wid) * (W + K) * kPad;  // [W][kPad]
-  float * Y = RIf + W * kPad;                                                         // [K][kPad]
+  float * RIf = reinterpret_cast<float *>(smem_raw) + size_t(wid) * (W + K) * kPadF;  // [W][kPadF]
+  float * Y = RIf + W * kPadF;                                                         // [K][kPadF]
   __shared__ float pa_s[kWarps][32], pb_s[kWarps][32], fc_s[kWarps][32];
   __shared__ int pk_s[kWarps][32];
   __shared__ uint8_t order_s[kWarps][32];
@@ -253,8 +257,8 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
       for (int row = 0; row < S * n; ++row) Ci[row * RS + c] = 0.f;
     }
     bool first = true;
-    for (int64_t p0 = p_lo; p0 < p_hi || first; p0 += 32) {
-      const int np = int(max(int64_t(0), min(int64_t(32), p_hi - p0)));
+    for (int64_t p0 = p_lo; p0 < p_hi || first; p0 += kChunkF) {
+      const int np = int(max(int64_t(0), min(int64_t(kChunkF), p_hi - p0)));
       int my_sp = 31;
       if (lane < np) {
         const int64_t p = p0 + lane;
@@ -268,7 +272,7 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
         const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
                     dz = float(a.pair_dir[3 * p + 2]);
         spherical_harmonics<L, false, float>(dx, dy, dz, [&](int lm, float y, float, float, float) {
-          Y[lm * kPad + lane] = y;
+          Y[lm * kPadF + lane] = y;
         });
       }
       // stable order of the chunk's pairs by species
@@ -288,7 +292,7 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
         const float4 * row = a.sp.q4f + size_t(pk_s[wid][q]) * W;
         for (int c = lane; c < W; c += 32) {
           const float4 t = __ldg(row + c);
-          RIf[c * kPad + q] = f * (fa * (t.x + ca * t.y) + fb * (t.z + cb * t.w));
+          RIf[c * kPadF + q] = f * (fa * (t.x + ca * t.y) + fb * (t.z + cb * t.w));
         }
       }
       __syncwarp();
@@ -298,8 +302,8 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
         if (cnt > 0 || first) {
           float * Cs = Ci + size_t(s) * n * RS;
           for (int lm = lane; lm < K; lm += 32) {
-            const float * ri = RIf + lofk[lm] * kPad;  // row nn*L1 + l at + nn*L1*kPad
-            const float * yy = Y + lm * kPad;
+            const float * ri = RIf + lofk[lm] * kPadF;  // row nn*L1 + l at + nn*L1*kPadF
+            const float * yy = Y + lm * kPadF;
             float acc[NV];
 #pragma unroll
             for (int nn = 0; nn < NV; ++nn) acc[nn] = 0.f;
@@ -308,7 +312,7 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
               const float y = yy[pl];
 #pragma unroll
               for (int nn = 0; nn < NV; ++nn)
-                if (nn < n) acc[nn] += ri[nn * L1 * kPad + pl] * y;
+                if (nn < n) acc[nn] += ri[nn * L1 * kPadF + pl] * y;
             }
             float * dst = Cs + colk[lm];
 #pragma unroll
@@ -451,7 +455,7 @@ void launch_exp_f32(const ExpansionArgs & a, float * C, uint32_t * present, cuda
   if (a.n_centers == 0) return;
   if (a.fd.n > 16) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
   sph_constants_tu();
-  const size_t smem = size_t(kWarps) * (a.fd.W + a.fd.K) * kPad * sizeof(float);
+  const size_t smem = size_t(kWarps) * (a.fd.W + a.fd.K) * kPadF * sizeof(float);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
