@@ -46,7 +46,9 @@ constexpr int kMaxN = 16;  // largest max_radial of the register-staged path
 // r_ji (x) g_ij (Voigt xx yy zz yz xz xy, the reference's
 // sparse_kernel_predict.hh:355-366) is summed per structure as well.
 template <int L, int NV, bool STRESS>
-__global__ void __launch_bounds__(kThreads, 4)  // 128 registers, no spills at L = 6
+// 5 resident blocks per SM (96 registers, a few bytes of spills at L = 6)
+// measured faster than 4 (128 registers) or 6 (more spills)
+__global__ void __launch_bounds__(kThreads, 5)
 pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, int64_t n_pairs,
                     const float * __restrict__ dC, double * __restrict__ F,
                     const int32_t * __restrict__ center_struct, double * __restrict__ stress) {
