@@ -179,6 +179,7 @@ struct rgpu_structures {
   std::vector<int64_t> pair_off_h;  // host copy of nl.pair_off, made on demand
   bool pair_off_h_valid{false};
   std::vector<int> batch_species;   // sorted atom types present in the batch
+  int64_t centres_of_type[130]{};   // centres per atom type (the mask applied)
   // layout and features
   std::vector<int> species;  // dense layout (sorted)
   DevBuf lut;
@@ -329,6 +330,7 @@ void build_nl(rgpu_structures * s, double cutoff) {
   in.n_centers = s->ncent_d.as<int32_t>();
   in.center_off = s->center_off_d.as<int64_t>();
   in.atom_struct = s->atom_struct_d.as<int32_t>();
+  in.n_centers_total = s->center_off_h[s->n_struct];
   build_neighbour_list(in, cutoff, s->nlw, s->nl, s->status_d, s->status_h, s->st);
   s->pair_off_h_valid = false;
   s->nl_valid = true;
@@ -380,10 +382,9 @@ void sort_rows(rgpu_structures * s) {
   launch_species_sort(nc, s->types_d.as<int32_t>(), s->nl.center_atom, s->lut.as<int8_t>(), s->fd.S,
                       s->species_count_d.as<int64_t>(), s->row_of_center.as<int32_t>(),
                       s->center_of_row.as<int32_t>(), s->sort_tmp, s->st);
+  // the counts per central species are known on the host since the upload
   s->species_count.assign(s->fd.S, 0);
-  RGPU_CUDA(cudaMemcpyAsync(s->species_count.data(), s->species_count_d.p, sizeof(int64_t) * s->fd.S,
-                            cudaMemcpyDeviceToHost, s->st));
-  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  for (int sI = 0; sI < s->fd.S; ++sI) s->species_count[sI] = s->centres_of_type[s->species[sI]];
 }
 
 void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, bool grads,
@@ -1373,6 +1374,9 @@ rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const
     if (center_mask)
       for (int64_t a = 0; a < s->n_atoms; ++a)
         if (!center_mask[a]) s->has_mask = true;
+    std::fill(s->centres_of_type, s->centres_of_type + 130, int64_t(0));
+    for (int64_t a = 0; a < s->n_atoms; ++a)
+      if (!center_mask || center_mask[a]) ++s->centres_of_type[s->types[a]];
     std::vector<int32_t> ncent(n_structures), astruct(s->n_atoms);
     s->center_off_h.assign(n_structures + 1, 0);
     std::vector<int32_t> tag2idx;

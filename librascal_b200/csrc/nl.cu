@@ -486,12 +486,12 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   nl_pack_kernel<<<div_up(n_sites, kThreads), kThreads, 0, st>>>(
       n_sites, w.sorted.as<int64_t>(), w.site_x.as<double>(), w.sorted_x.as<double>());
   RGPU_LAUNCHED();
-  check_status("binning");
+  // The binning status (an atom outside every bin) is read with the pair
+  // count below: the binning kernels clamp their box indices, so everything
+  // up to there stays in bounds even when it is set.
 
   // 4. centres: structure of each centre row
-  int64_t n_centers = 0;
-  RGPU_CUDA(cudaMemcpyAsync(&n_centers, in.center_off + S, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
-  RGPU_CUDA(cudaStreamSynchronize(st));
+  const int64_t n_centers = in.n_centers_total;
   w.center_struct.ensure(sizeof(int32_t) * (n_centers + 1));
   w.center_atom.ensure(sizeof(int32_t) * (n_centers + 1));
   center_struct_kernel<<<S, 128, 0, st>>>(S, in.center_off, w.center_struct.as<int32_t>());
@@ -525,7 +525,7 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   int64_t n_pairs = 0;
   RGPU_CUDA(cudaMemcpyAsync(&n_pairs, w.pair_off.as<int64_t>() + n_centers, sizeof(int64_t),
                             cudaMemcpyDeviceToHost, st));
-  RGPU_CUDA(cudaStreamSynchronize(st));
+  check_status("binning");  // synchronises: n_pairs is on the host after it
   w.pair_j.ensure(sizeof(int32_t) * (n_pairs + 1));
   w.pair_shift.ensure(sizeof(int32_t) * 3 * (n_pairs + 1));
   w.pair_dist.ensure(sizeof(double) * (n_pairs + 1));

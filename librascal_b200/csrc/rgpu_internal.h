@@ -125,6 +125,7 @@ struct NlInputs {
   const int32_t * n_centers;   // [n_struct]
   const int64_t * center_off;  // [n_struct+1]
   const int32_t * atom_struct; // [n_atoms]
+  int64_t n_centers_total;     // center_off[n_struct], known on the host
 };
 struct NlOutputs {
   int64_t n_centers{0}, n_pairs{0};
