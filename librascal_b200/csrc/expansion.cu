@@ -286,11 +286,24 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
       }
       if (lane < np) order_s[wid][before + __popc(my_mask & lanemask_lt())] = uint8_t(lane);
       __syncwarp();
+      // lanes = radial channels c and c + 32 (then c + 64, ... when W is
+      // larger); four pairs per step, so that their table loads are in
+      // flight together
+      const bool c1_ok = lane + 32 < W, c0_ok = lane < W;
+#pragma unroll 4
       for (int q = 0; q < np; ++q) {
         const float fa = pa_s[wid][q], fb = pb_s[wid][q], f = fc_s[wid][q];
         const float ca = fa * fa - 1.f, cb = fb * fb - 1.f;
         const float4 * row = a.sp.q4f + size_t(pk_s[wid][q]) * W;
-        for (int c = lane; c < W; c += 32) {
+        if (c0_ok) {
+          const float4 t = __ldg(row + lane);
+          RIf[lane * kPadF + q] = f * (fa * (t.x + ca * t.y) + fb * (t.z + cb * t.w));
+        }
+        if (c1_ok) {
+          const float4 t = __ldg(row + lane + 32);
+          RIf[(lane + 32) * kPadF + q] = f * (fa * (t.x + ca * t.y) + fb * (t.z + cb * t.w));
+        }
+        for (int c = lane + 64; c < W; c += 32) {
           const float4 t = __ldg(row + c);
           RIf[c * kPadF + q] = f * (fa * (t.x + ca * t.y) + fb * (t.z + cb * t.w));
         }
