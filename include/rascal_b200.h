@@ -226,6 +226,35 @@ rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s,
                                     int precision, double * energies,
                                     double * forces, double * neg_stress);
 
+/* One step of a molecular-dynamics loop on the structures of the last
+ * rgpu_structures_set (same atoms, types and cells; positions wrapped into
+ * the cells): new positions [n_atoms x 3] in; energies, forces and, when
+ * neg_stress is not NULL, the negative stress out, as rgpu_gap_predict_stress
+ * gives them on the FP32 path. The first call runs the ordinary path, then
+ * records the step, neighbour list included, as a CUDA graph with the list
+ * built to capacities 25 % above that step's counts; later calls copy the
+ * positions into pinned memory and replay the graph, with one
+ * synchronisation per step. A step whose neighbour list outgrows the
+ * capacities, or whose input is invalid, is recomputed by the ordinary path
+ * (which reports input errors with the reference's messages) and the graph
+ * is recorded again. Another call that reallocates a device buffer of this
+ * handle, of the model or of its calculator makes the next step record
+ * anew. Replaces, for the FP32 path, the
+ * per-step predict calls of GenericMDCalculator.calculate
+ * (bindings/rascal/models/genericmd.py:84-130). */
+rgpu_status rgpu_md_step(rgpu_gap_model * m, rgpu_structures * s, const double * positions,
+                         double * energies, double * forces, double * neg_stress);
+/* Whether the structures handle holds a recorded MD step (1) or will run
+ * the ordinary path next (0); info (may be NULL) receives the
+ * neighbour-list capacities of the recording (sites, boxes, pairs), the
+ * number of replays since it was recorded, and why the last recording was
+ * not replayed (0 none, 1 one of its device buffers was reallocated by
+ * another call on this handle or model, 3 another model,
+ * layout or stress setting, 100 + status code when the replayed step set
+ * one, e.g. 204 for outgrown capacities). No counterpart in the
+ * reference. */
+rgpu_status rgpu_md_step_info(const rgpu_structures * s, int32_t * recorded, int64_t * info /* [5] */);
+
 /* Sparse kernel matrices for training a GAP model, FP64 (the reference's
  * arithmetic). Columns follow the order of the model's sparse points;
  * weights and self contributions are not used.

@@ -62,6 +62,8 @@ SIGNATURES = {
                                         c_dbl_p]),
     "rgpu_gap_predict_stress": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, c_dbl_p,
                                                c_dbl_p, c_dbl_p]),
+    "rgpu_md_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_dbl_p, c_dbl_p, c_dbl_p, c_dbl_p]),
+    "rgpu_md_step_info": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_i64_p]),
     "rgpu_sparse_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, c_dbl_p]),
     "rgpu_sparse_kernel_derivative": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, c_dbl_p]),
     "rgpu_sparse_kernel_mm": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p]),

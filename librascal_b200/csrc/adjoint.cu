@@ -58,6 +58,12 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
   const bool vec = (n == NV);
   const int lane = threadIdx.x & 31;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+  // the list's own total bounds the loop (below n_pairs when the list was
+  // built to a capacity)
+  {
+    const int64_t listed = a.pair_off[a.n_centers];
+    if (listed < n_pairs) n_pairs = listed;
+  }
   // the loop bound is warp-uniform: the F_i sums below shuffle across lanes
   for (int64_t base = int64_t(blockIdx.x) * blockDim.x + threadIdx.x - lane; base < n_pairs; base += stride) {
     const int64_t p = base + lane;

@@ -196,6 +196,21 @@ struct rgpu_structures {
   bool feat_x32{false};  // FP32 features also kept unsplit (for export)
   DevBuf dCp, dCs, dXp;
   DevBuf knm, W64, plist, Vvir;  // sparse kernel matrices for training
+  // MD step recorded as a CUDA graph (rgpu_md_step)
+  cudaGraph_t md_graph{nullptr};
+  cudaGraphExec_t md_exec{nullptr};
+  const rgpu_gap_model * md_model{nullptr};
+  bool md_stress{false};
+  NlCaps md_caps{};
+  std::vector<const void *> md_buffers;  // device buffer addresses at recording
+  std::vector<int> md_species;
+  int64_t md_replays{0};       // replays since the graph was recorded
+  int64_t md_reason{0};        // why the last step did not replay: 0 none (first step or no
+                               // recording), 1 a buffer moved, 3 model or layout, 100 + status
+  bool md_no_graph{false};     // recording failed once: ordinary path only
+  double * md_pos_h{nullptr};  // pinned: positions in, outputs out
+  double * md_out_h{nullptr};
+  size_t md_pos_cap{0}, md_out_cap{0};
   // status and timing
   DevStatus * status_d{nullptr};
   DevStatus * status_h{nullptr};
@@ -1229,6 +1244,229 @@ static void sparse_kernel_mm_impl(rgpu_gap_model * m, double * out) {
   RGPU_CUDA(cudaStreamSynchronize(st));
 }
 
+// ------------------------------------------------------------------ MD step
+// A step of a molecular-dynamics loop on a fixed set of structures: the FP32
+// path from new positions to energies, forces (and the negative stress),
+// with no host synchronisation inside, so that it is recorded once as a
+// CUDA graph and then replayed. The neighbour list is built to capacities
+// 25 % above the counts of the step that recorded the graph; when a step
+// outgrows them (status 104) it is recomputed by the ordinary path and the
+// graph is recorded again.
+// Addresses of every device buffer a recorded step can use: those of the
+// structures handle (neighbour-list work included), of the model and of its
+// calculator. The recording is replayed only while none of them moved.
+static std::vector<const void *> md_buffers(const rgpu_gap_model * m, const rgpu_structures * s) {
+  std::vector<const void *> v;
+  for (const DevBuf * b : {&s->atom_off_d, &s->pos_d, &s->types_d, &s->cells_d, &s->pbc_d, &s->tag2idx_d,
+                           &s->ncent_d, &s->center_off_d, &s->atom_struct_d, &s->lut, &s->row_of_center,
+                           &s->center_of_row, &s->species_count_d, &s->sort_tmp, &s->present, &s->C64, &s->X64,
+                           &s->invn64, &s->C32, &s->X32, &s->xscale32, &s->E_d, &s->F_d, &s->S_d, &s->K64,
+                           &s->t64, &s->erow64, &s->Wh, &s->Wl, &s->dX32, &s->dC32, &s->epart, &s->Xh, &s->Xl,
+                           &s->dCp, &s->dCs, &s->dXp, &s->knm, &s->W64, &s->plist, &s->Vvir})
+    v.push_back(b->p);
+  const NlWork & w = s->nlw;
+  for (const DevBuf * b : {&w.geom, &w.counts64, &w.scan_tmp, &w.ghost_off, &w.site_x, &w.site_type, &w.site_real,
+                           &w.site_shift, &w.site_box, &w.box_base, &w.box_count, &w.box_ptr, &w.box_fill,
+                           &w.sorted, &w.sorted_x, &w.sorted_info, &w.pair_count, &w.center_atom,
+                           &w.center_struct, &w.pair_off, &w.pair_j, &w.pair_shift, &w.pair_dist, &w.pair_dir,
+                           &w.pair_center})
+    v.push_back(b->p);
+  for (const DevBuf * b : {&m->T64, &m->alpha64, &m->Th, &m->Tl, &m->Tth, &m->Ttl, &m->alpha32, &m->ucol})
+    v.push_back(b->p);
+  const rgpu_calculator * c = m->calc;
+  for (const DevBuf * b : {&c->grid, &c->y, &c->y2h, &c->yf, &c->y2hf, &c->q4f, &c->center}) v.push_back(b->p);
+  return v;
+}
+
+static void md_drop(rgpu_structures * s) {
+  if (s->md_exec) cudaGraphExecDestroy(s->md_exec);
+  if (s->md_graph) cudaGraphDestroy(s->md_graph);
+  s->md_exec = nullptr;
+  s->md_graph = nullptr;
+  s->md_model = nullptr;
+}
+
+// The step's work on the structures' stream, positions from s->md_pos_h.
+static void md_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress) {
+  rgpu_calculator * c = m->calc;
+  cudaStream_t st = s->st;
+  const int64_t na = s->n_atoms;
+  RGPU_CUDA(cudaMemcpyAsync(s->pos_d.p, s->md_pos_h, sizeof(double) * 3 * na, cudaMemcpyHostToDevice, st));
+  NlInputs in;
+  in.n_struct = s->n_struct;
+  in.n_atoms = na;
+  in.atom_off = s->atom_off_d.as<int64_t>();
+  in.pos = s->pos_d.as<double>();
+  in.types = s->types_d.as<int32_t>();
+  in.cells = s->cells_d.as<double>();
+  in.pbc = s->pbc_d.as<int32_t>();
+  in.tag2idx = nullptr;
+  in.n_centers = s->ncent_d.as<int32_t>();
+  in.center_off = s->center_off_d.as<int64_t>();
+  in.atom_struct = s->atom_struct_d.as<int32_t>();
+  in.n_centers_total = s->center_off_h[s->n_struct];
+  build_neighbour_list(in, c->hy.cutoff, s->nlw, s->nl, s->status_d, s->status_h, st, &s->md_caps);
+  // features (the FP32 branch of compute_features, layout unchanged)
+  sort_rows(s);
+  const int64_t nc = s->nl.n_centers;
+  const FeatureDims & fd = s->fd;
+  ExpansionArgs ea = exp_args(c, s);
+  PsArgs pa;
+  pa.fd = fd;
+  pa.n_centers = nc;
+  pa.normalize = c->hy.normalize;
+  pa.row_of_center = s->row_of_center.as<int32_t>();
+  launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), st);
+  launch_ps_fwd_fp32(pa, s->C32.as<float>(), nullptr, s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(),
+                     s->xscale32.as<float>(), st);
+  RGPU_CUDA(cudaMemsetAsync(s->E_d.p, 0, sizeof(double) * s->n_struct, st));
+  RGPU_CUDA(cudaMemsetAsync(s->F_d.p, 0, sizeof(double) * 3 * na, st));
+  if (stress) RGPU_CUDA(cudaMemsetAsync(s->S_d.p, 0, sizeof(double) * 6 * s->n_struct, st));
+  gap_fast(m, s, s->E_d.as<double>(), s->F_d.as<double>(), true, stress ? s->S_d.as<double>() : nullptr);
+  double * out = s->md_out_h;
+  RGPU_CUDA(cudaMemcpyAsync(out, s->E_d.p, sizeof(double) * s->n_struct, cudaMemcpyDeviceToHost, st));
+  RGPU_CUDA(cudaMemcpyAsync(out + s->n_struct, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, st));
+  if (stress)
+    RGPU_CUDA(cudaMemcpyAsync(out + s->n_struct + 3 * na, s->S_d.p, sizeof(double) * 6 * s->n_struct,
+                              cudaMemcpyDeviceToHost, st));
+  RGPU_CUDA(cudaMemcpyAsync(s->status_h, s->status_d, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+}
+
+// Energy baseline and cell volume, as in gap_predict_impl.
+static void md_finish(const rgpu_gap_model * m, const rgpu_structures * s, double * energies, double * forces,
+                      double * neg_stress) {
+  const int64_t na = s->n_atoms;
+  const double * out = s->md_out_h;
+  if (energies) {
+    double sc[130] = {0.};
+    for (size_t i = 0; i < m->species.size(); ++i)
+      if (m->species[i] >= 0 && m->species[i] < 130) sc[m->species[i]] = m->self_contrib[i];
+    for (int st = 0; st < s->n_struct; ++st) {
+      double y0 = 0.;
+      for (int64_t a = s->atom_off[st]; a < s->atom_off[st + 1]; ++a) y0 += sc[s->types[a]];
+      energies[st] = out[st] + y0;
+    }
+  }
+  if (forces) std::memcpy(forces, out + s->n_struct, sizeof(double) * 3 * na);
+  if (neg_stress)
+    for (int st = 0; st < s->n_struct; ++st) {
+      const double v = cell_volume(&s->cells_h[9 * size_t(st)]);
+      for (int k = 0; k < 6; ++k) neg_stress[6 * st + k] = out[s->n_struct + 3 * na + 6 * st + k] / v;
+    }
+}
+
+static void md_step_impl(rgpu_gap_model * m, rgpu_structures * s, const double * positions, double * energies,
+                         double * forces, double * neg_stress) {
+  if (!m || !s || !positions) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+  const bool stress = neg_stress != nullptr;
+  const int64_t na = s->n_atoms;
+  ensure_stream(s);
+  bool replay = false;
+  if (s->md_exec) {
+    if (s->md_model != m || s->md_stress != stress || m->layout_species != s->species ||
+        s->md_species != s->species)
+      s->md_reason = 3;
+    else if (md_buffers(m, s) != s->md_buffers)
+      s->md_reason = 1;
+    else
+      replay = true;
+  }
+  if (replay) {
+    std::memcpy(s->md_pos_h, positions, sizeof(double) * 3 * na);
+    RGPU_CUDA(cudaGraphLaunch(s->md_exec, s->st));
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    ++s->md_replays;
+    const int where = gemm_tc_timeout(true);
+    if (where)
+      throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM: a bounded pipeline wait gave up (stage " +
+                                        std::to_string(where) + ")");
+    if (s->status_h->code == 0) {
+      md_finish(m, s, energies, forces, neg_stress);
+      return;
+    }
+    // outgrown capacities or an input error: the ordinary path below
+    // rebuilds, or reports the error with its message
+    s->md_reason = 100 + s->status_h->code;
+    RGPU_CUDA(cudaMemsetAsync(s->status_d, 0, sizeof(DevStatus), s->st));
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    s->status_h->code = 0;
+  }
+  md_drop(s);
+  // the ordinary path: checks the input, sizes every buffer, gives this step's results
+  upload(s, s->pos_d, positions, sizeof(double) * 3 * na);
+  s->nl_valid = false;
+  s->feat_valid = false;
+  gap_predict_impl(m, s, RGPU_PRECISION_FP32, energies, forces, neg_stress);
+  if (s->md_no_graph) return;
+  // capacities 25 % above this step's counts
+  int64_t sites = 0, boxes = 0;
+  neighbour_list_counts(s->nlw, sites, boxes);
+  s->md_caps.sites = sites + sites / 4 + 64;
+  s->md_caps.boxes = boxes + boxes / 4 + 64;
+  s->md_caps.pairs = s->nl.n_pairs + s->nl.n_pairs / 4 + 256;
+  if (s->md_pos_cap < size_t(3 * na)) {
+    if (s->md_pos_h) cudaFreeHost(s->md_pos_h);
+    RGPU_CUDA(cudaMallocHost(&s->md_pos_h, sizeof(double) * 3 * std::max<int64_t>(na, 1)));
+    s->md_pos_cap = size_t(3 * na);
+  }
+  const size_t nout = size_t(s->n_struct) * 7 + 3 * size_t(na);
+  if (s->md_out_cap < nout) {
+    if (s->md_out_h) cudaFreeHost(s->md_out_h);
+    RGPU_CUDA(cudaMallocHost(&s->md_out_h, sizeof(double) * std::max<size_t>(nout, 1)));
+    s->md_out_cap = nout;
+  }
+  if (stress) s->S_d.ensure(sizeof(double) * 6 * (s->n_struct + 1));
+  std::memcpy(s->md_pos_h, positions, sizeof(double) * 3 * na);
+  // one run without recording sizes the capacity buffers (no allocation may
+  // happen while recording) and checks that the step fits them
+  s->timed = false;
+  md_enqueue(m, s, stress);
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  if (s->status_h->code != 0 || gemm_tc_timeout(true)) {
+    // cannot happen with fresh capacities unless something is off: leave
+    // the step to the ordinary path next time
+    RGPU_CUDA(cudaMemsetAsync(s->status_d, 0, sizeof(DevStatus), s->st));
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    s->status_h->code = 0;
+    return;
+  }
+  // record; a step that cannot be recorded keeps the ordinary path
+  bool ok = cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+  if (ok) {
+    try {
+      md_enqueue(m, s, stress);
+    } catch (...) {
+      ok = false;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->st, &g);
+    ok = ok && e == cudaSuccess && g != nullptr;
+    if (ok) {
+      s->md_graph = g;
+      ok = cudaGraphInstantiate(&s->md_exec, s->md_graph, 0) == cudaSuccess;
+    } else if (g) {
+      cudaGraphDestroy(g);
+    }
+  }
+  if (!ok) {
+    (void)cudaGetLastError();
+    md_drop(s);
+    s->md_no_graph = true;
+    s->nl_valid = false;
+    s->feat_valid = false;
+    return;
+  }
+  s->md_model = m;
+  s->md_stress = stress;
+  s->md_buffers = md_buffers(m, s);
+  s->md_species = s->species;
+  s->md_replays = 0;
+  // the ordinary step above already produced this call's results; the
+  // positions of the next step arrive in md_pos_h
+  s->nl_valid = false;
+  s->feat_valid = false;
+}
+
 // ===================================================================== C ABI
 extern "C" {
 
@@ -1336,6 +1574,10 @@ rgpu_status rgpu_structures_destroy(rgpu_structures * s) {
   return guard([&] {
     if (!s) return;
     if (s->st) cudaStreamSynchronize(s->st);
+    if (s->md_exec) cudaGraphExecDestroy(s->md_exec);
+    if (s->md_graph) cudaGraphDestroy(s->md_graph);
+    if (s->md_pos_h) cudaFreeHost(s->md_pos_h);
+    if (s->md_out_h) cudaFreeHost(s->md_out_h);
     if (s->pinned) cudaFreeHost(s->pinned);
     if (s->status_h) cudaFreeHost(s->status_h);
     if (s->status_d) cudaFree(s->status_d);
@@ -1351,6 +1593,8 @@ rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const
                                 const int32_t * pbc, const uint8_t * center_mask) {
   return guard([&] {
     if (!s || n_structures < 0 || !atom_offsets) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    md_drop(s);
+    s->md_no_graph = false;
     ensure_stream(s);
     s->n_struct = n_structures;
     s->atom_off.assign(atom_offsets, atom_offsets + n_structures + 1);
@@ -1670,6 +1914,25 @@ rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s, int
   return guard([&] {
     if (!neg_stress) throw Error(RGPU_ERR_INVALID_ARGUMENT, "neg_stress output is required");
     gap_predict_impl(m, s, precision, energies, forces, neg_stress);
+  });
+}
+
+rgpu_status rgpu_md_step(rgpu_gap_model * m, rgpu_structures * s, const double * positions, double * energies,
+                         double * forces, double * neg_stress) {
+  return guard([&] { md_step_impl(m, s, positions, energies, forces, neg_stress); });
+}
+
+rgpu_status rgpu_md_step_info(const rgpu_structures * s, int32_t * recorded, int64_t * info) {
+  return guard([&] {
+    if (!s || !recorded) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    *recorded = s->md_exec ? 1 : 0;
+    if (info) {
+      info[0] = s->md_caps.sites;
+      info[1] = s->md_caps.boxes;
+      info[2] = s->md_caps.pairs;
+      info[3] = s->md_replays;
+      info[4] = s->md_reason;
+    }
   });
 }
 

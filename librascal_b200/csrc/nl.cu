@@ -190,7 +190,7 @@ __global__ void nl_sites_kernel(int64_t n_atoms, const int64_t * __restrict__ at
                                 double * __restrict__ site_x, int32_t * __restrict__ site_type,
                                 int32_t * __restrict__ site_real, int32_t * __restrict__ site_shift,
                                 int64_t * __restrict__ site_box, int32_t * __restrict__ box_count,
-                                DevStatus * st) {
+                                DevStatus * st, int64_t site_cap, int64_t box_cap) {
   int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= n_atoms) return;
   int s = atom_struct[t];
@@ -202,6 +202,10 @@ __global__ void nl_sites_kernel(int64_t n_atoms, const int64_t * __restrict__ at
   double x0[3] = {pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]};
   int typ = types[a];
   auto put = [&](int64_t site, const double * x, const int * p) {
+    if (site >= site_cap) {
+      set_status(st, 104, s, int(a));  // more sites than the capacity
+      return;
+    }
     site_x[3 * site + 0] = x[0];
     site_x[3 * site + 1] = x[1];
     site_x[3 * site + 2] = x[2];
@@ -216,6 +220,11 @@ __global__ void nl_sites_kernel(int64_t n_atoms, const int64_t * __restrict__ at
     b[1] = min(b[1], g.nboxes[1] - 2);
     b[2] = min(b[2], g.nboxes[2] - 2);
     int64_t box = box_base[s] + (int64_t(b[0]) * g.nboxes[1] + b[1]) * g.nboxes[2] + b[2];
+    if (box >= box_cap) {
+      set_status(st, 104, s, int(a));  // more boxes than the capacity
+      site_box[site] = -1;
+      return;
+    }
     site_box[site] = box;
     atomicAdd(&box_count[box], 1);
   };
@@ -234,12 +243,22 @@ __global__ void nl_sites_kernel(int64_t n_atoms, const int64_t * __restrict__ at
   }
 }
 
+// n_sites bounds the grid; with ghosts_dev (the device total of ghost
+// sites) the count is n_atoms + *ghosts_dev when that is smaller.
+__device__ __forceinline__ int64_t site_count(int64_t n_sites, const int64_t * ghosts_dev, int64_t n_atoms) {
+  if (!ghosts_dev) return n_sites;
+  const int64_t n = n_atoms + *ghosts_dev;
+  return n < n_sites ? n : n_sites;
+}
+
 __global__ void nl_scatter_kernel(int64_t n_sites, const int64_t * __restrict__ site_box,
                                   const int64_t * __restrict__ box_ptr,
-                                  int32_t * __restrict__ box_fill, int64_t * __restrict__ sorted) {
+                                  int32_t * __restrict__ box_fill, int64_t * __restrict__ sorted,
+                                  const int64_t * __restrict__ ghosts_dev, int64_t n_atoms) {
   int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n_sites) return;
+  if (i >= site_count(n_sites, ghosts_dev, n_atoms)) return;
   int64_t b = site_box[i];
+  if (b < 0) return;  // a site past the box capacity
   int64_t slot = box_ptr[b] + atomicAdd(&box_fill[b], 1);
   sorted[slot] = i;
 }
@@ -248,7 +267,7 @@ __global__ void nl_scatter_kernel(int64_t n_sites, const int64_t * __restrict__ 
 __global__ void nl_boxsort_kernel(int64_t n_boxes, const int64_t * __restrict__ box_ptr,
                                   int64_t * __restrict__ sorted) {
   int64_t b = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (b >= n_boxes) return;
+  if (b >= n_boxes) return;  // boxes past the used ones (capacity mode) are empty
   int64_t lo = box_ptr[b], hi = box_ptr[b + 1];
   for (int64_t i = lo + 1; i < hi; ++i) {
     int64_t v = sorted[i];
@@ -262,9 +281,11 @@ __global__ void nl_boxsort_kernel(int64_t n_boxes, const int64_t * __restrict__ 
 }
 
 __global__ void nl_pack_kernel(int64_t n_sites, const int64_t * __restrict__ sorted,
-                               const double * __restrict__ site_x, double * __restrict__ sorted_x) {
+                               const double * __restrict__ site_x, double * __restrict__ sorted_x,
+                               const int64_t * __restrict__ box_total) {
   int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i >= n_sites) return;
+  // the binned sites (box_ptr's total): all sites unless some overflowed
+  if (i >= n_sites || (box_total && i >= *box_total)) return;
   int64_t s = sorted[i];
   sorted_x[3 * i + 0] = site_x[3 * s + 0];
   sorted_x[3 * i + 1] = site_x[3 * s + 1];
@@ -283,6 +304,8 @@ struct GatherCtx {
   const double * sorted_x;
   const double * site_x;
   double cutoff, rc2;
+  int64_t box_cap, pair_cap;  // capacities (the exact counts when synchronised)
+  DevStatus * status;
 };
 
 // One warp per centre. MODE 0 counts, MODE 1 writes the pairs.
@@ -309,10 +332,21 @@ __global__ void nl_gather_kernel(int64_t n_centers, GatherCtx c, int64_t * __res
   b[0] = min(b[0], g.nboxes[0] - 2);
   b[1] = min(b[1], g.nboxes[1] - 2);
   b[2] = min(b[2], g.nboxes[2] - 2);
+  // a structure whose mesh reaches past the box capacity is skipped (capacity mode)
+  if (c.box_base[s] + int64_t(g.nboxes[0]) * g.nboxes[1] * g.nboxes[2] > c.box_cap) {
+    if (lane == 0) set_status(c.status, 104, s, 0);
+    if (MODE == 0 && lane == 0) count[ci] = 1;
+    return;
+  }
   int64_t out = 0;
   int64_t base = 0;
   if (MODE == 1) {
     base = pair_off[ci];
+    if (base + 1 + 0 > c.pair_cap) {  // not even the self pair fits
+      if (lane == 0) set_status(c.status, 104, s, int(ci));
+      return;
+    }
+    if (pair_off[ci + 1] > c.pair_cap && lane == 0) set_status(c.status, 104, s, int(ci));
     if (lane == 0) {
       center_atom[ci] = site_real[site];
       pair_j[base] = site_real[site];
@@ -342,7 +376,7 @@ __global__ void nl_gather_kernel(int64_t n_centers, GatherCtx c, int64_t * __res
           ok = (sj != site) && (d2 <= c.rc2);
         }
         unsigned m = __ballot_sync(0xffffffffu, ok);
-        if (MODE == 1 && ok) {
+        if (MODE == 1 && ok && base + out + __popc(m & lanemask_lt()) < c.pair_cap) {
           int64_t p = base + out + __popc(m & lanemask_lt());
           pair_j[p] = site_real[sj];
           pair_shift[3 * p + 0] = site_shift[3 * sj + 0];
@@ -366,7 +400,7 @@ __global__ void nl_gather_kernel(int64_t n_centers, GatherCtx c, int64_t * __res
   }
   if (MODE == 0 && lane == 0) count[ci] = out + 1;
   if (MODE == 1)
-    for (int64_t p = base - 1 + lane; p < base + out; p += 32) pair_center[p] = int32_t(ci);
+    for (int64_t p = base - 1 + lane; p < base + out && p < c.pair_cap; p += 32) pair_center[p] = int32_t(ci);
   (void)site_type;
 }
 
@@ -379,10 +413,24 @@ __global__ void center_struct_kernel(int n_struct, const int64_t * __restrict__ 
     center_struct[i] = s;
 }
 
+// Capacity mode: offsets past the pair capacity are clamped to it, so that
+// every later per-centre loop stays inside the pair buffers even when the
+// list overflowed (status 104 then tells the caller to rebuild).
+__global__ void nl_clamp_offsets_kernel(int64_t n, int64_t * __restrict__ pair_off, int64_t cap) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n && pair_off[i] > cap) pair_off[i] = cap;
+}
+
 }  // namespace
 
+void neighbour_list_counts(const NlWork & w, int64_t & sites, int64_t & boxes) {
+  sites = w.last_sites;
+  boxes = w.last_boxes;
+}
+
 void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutputs & out,
-                          DevStatus * status_dev, DevStatus * status_host, cudaStream_t st) {
+                          DevStatus * status_dev, DevStatus * status_host, cudaStream_t st,
+                          const NlCaps * caps) {
   const int S = in.n_struct;
   const int64_t N = in.n_atoms;
   auto check_status = [&](const char * stage) {
@@ -434,7 +482,7 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   nl_setup_kernel<<<div_up(S, 128), 128, 0, st>>>(S, in.atom_off, in.cells, in.pbc, in.n_centers,
                                                   cutoff, geom, w.counts64.as<int64_t>(), status_dev);
   RGPU_LAUNCHED();
-  check_status("setup");
+  if (!caps) check_status("setup");
   nl_check_kernel<<<div_up(N, kThreads), kThreads, 0, st>>>(N, in.atom_struct, in.pos, in.types,
                                                             geom, status_dev);
   RGPU_LAUNCHED();
@@ -447,14 +495,25 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
       N, in.atom_struct, in.tag2idx, in.pos, geom, w.pair_count.as<int32_t>());
   RGPU_LAUNCHED();
   scan_exclusive_i32to64(w.pair_count.as<int32_t>(), w.ghost_off.as<int64_t>(), N, w.scan_tmp, st);
-  int64_t totals[2];
-  RGPU_CUDA(cudaMemcpyAsync(&totals[0], w.ghost_off.as<int64_t>() + N, sizeof(int64_t),
-                            cudaMemcpyDeviceToHost, st));
-  RGPU_CUDA(cudaMemcpyAsync(&totals[1], w.box_base.as<int64_t>() + S, sizeof(int64_t),
-                            cudaMemcpyDeviceToHost, st));
-  check_status("check");
-  const int64_t n_sites = N + totals[0];
-  const int64_t n_boxes = totals[1];
+  int64_t n_sites = 0, n_boxes = 0;
+  if (caps) {
+    // capacity mode: no host synchronisation; the kernels stop at the
+    // capacities and the device counts bound the work
+    n_sites = caps->sites;
+    n_boxes = caps->boxes;
+  } else {
+    int64_t totals[2];
+    RGPU_CUDA(cudaMemcpyAsync(&totals[0], w.ghost_off.as<int64_t>() + N, sizeof(int64_t),
+                              cudaMemcpyDeviceToHost, st));
+    RGPU_CUDA(cudaMemcpyAsync(&totals[1], w.box_base.as<int64_t>() + S, sizeof(int64_t),
+                              cudaMemcpyDeviceToHost, st));
+    check_status("check");
+    n_sites = N + totals[0];
+    n_boxes = totals[1];
+    w.last_sites = n_sites;
+    w.last_boxes = n_boxes;
+  }
+  const int64_t * ghosts_dev = caps ? w.ghost_off.as<int64_t>() + N : nullptr;
 
   // 3. sites and binning
   w.site_x.ensure(sizeof(double) * 3 * n_sites);
@@ -471,20 +530,21 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
       N, in.atom_off, in.atom_struct, in.tag2idx, in.pos, in.types, geom, w.ghost_off.as<int64_t>(),
       w.box_base.as<int64_t>(), cutoff, w.site_x.as<double>(), w.site_type.as<int32_t>(),
       w.site_real.as<int32_t>(), w.site_shift.as<int32_t>(), w.site_box.as<int64_t>(),
-      w.box_count.as<int32_t>(), status_dev);
+      w.box_count.as<int32_t>(), status_dev, n_sites, n_boxes);
   RGPU_LAUNCHED();
   scan_exclusive_i32to64(w.box_count.as<int32_t>(), w.box_ptr.as<int64_t>(), n_boxes, w.scan_tmp, st);
   w.sorted.ensure(sizeof(int64_t) * n_sites);
   w.sorted_x.ensure(sizeof(double) * 3 * n_sites);
   nl_scatter_kernel<<<div_up(n_sites, kThreads), kThreads, 0, st>>>(
       n_sites, w.site_box.as<int64_t>(), w.box_ptr.as<int64_t>(), w.box_fill.as<int32_t>(),
-      w.sorted.as<int64_t>());
+      w.sorted.as<int64_t>(), ghosts_dev, N);
   RGPU_LAUNCHED();
   nl_boxsort_kernel<<<div_up(n_boxes, kThreads), kThreads, 0, st>>>(n_boxes, w.box_ptr.as<int64_t>(),
                                                                    w.sorted.as<int64_t>());
   RGPU_LAUNCHED();
   nl_pack_kernel<<<div_up(n_sites, kThreads), kThreads, 0, st>>>(
-      n_sites, w.sorted.as<int64_t>(), w.site_x.as<double>(), w.sorted_x.as<double>());
+      n_sites, w.sorted.as<int64_t>(), w.site_x.as<double>(), w.sorted_x.as<double>(),
+      caps ? w.box_ptr.as<int64_t>() + n_boxes : nullptr);
   RGPU_LAUNCHED();
   // The binning status (an atom outside every bin) is read with the pair
   // count below: the binning kernels clamp their box indices, so everything
@@ -511,6 +571,9 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   c.site_x = w.site_x.as<double>();
   c.cutoff = cutoff;
   c.rc2 = cutoff * cutoff;
+  c.box_cap = n_boxes;
+  c.pair_cap = INT64_MAX;  // set below, once the pair count or capacity is known
+  c.status = status_dev;
   w.counts64.ensure(sizeof(int64_t) * (n_centers + 1));
   w.pair_off.ensure(sizeof(int64_t) * (n_centers + 1));
   const int warps_per_block = kThreads / 32;
@@ -523,9 +586,14 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
   }
   scan_exclusive_i64(w.counts64.as<int64_t>(), w.pair_off.as<int64_t>(), n_centers, w.scan_tmp, st);
   int64_t n_pairs = 0;
-  RGPU_CUDA(cudaMemcpyAsync(&n_pairs, w.pair_off.as<int64_t>() + n_centers, sizeof(int64_t),
-                            cudaMemcpyDeviceToHost, st));
-  check_status("binning");  // synchronises: n_pairs is on the host after it
+  if (caps) {
+    n_pairs = caps->pairs;
+  } else {
+    RGPU_CUDA(cudaMemcpyAsync(&n_pairs, w.pair_off.as<int64_t>() + n_centers, sizeof(int64_t),
+                              cudaMemcpyDeviceToHost, st));
+    check_status("binning");  // synchronises: n_pairs is on the host after it
+  }
+  c.pair_cap = n_pairs;
   w.pair_j.ensure(sizeof(int32_t) * (n_pairs + 1));
   w.pair_shift.ensure(sizeof(int32_t) * 3 * (n_pairs + 1));
   w.pair_dist.ensure(sizeof(double) * (n_pairs + 1));
@@ -537,6 +605,11 @@ void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutp
         w.site_real.as<int32_t>(), w.site_shift.as<int32_t>(), w.center_atom.as<int32_t>(),
         w.pair_j.as<int32_t>(), w.pair_shift.as<int32_t>(), w.pair_dist.as<double>(),
         w.pair_dir.as<double>(), w.pair_center.as<int32_t>());
+    RGPU_LAUNCHED();
+  }
+  if (caps) {
+    nl_clamp_offsets_kernel<<<div_up(n_centers + 1, kThreads), kThreads, 0, st>>>(
+        n_centers + 1, w.pair_off.as<int64_t>(), n_pairs);
     RGPU_LAUNCHED();
   }
   out.n_centers = n_centers;

@@ -142,12 +142,24 @@ struct NlWork {
   DevBuf geom, counts64, scan_tmp, ghost_off, site_x, site_type, site_real, site_shift,
       site_box, box_base, box_count, box_ptr, box_fill, sorted, sorted_x, sorted_info,
       pair_count;
+  int64_t last_sites{0}, last_boxes{0};
   DevBuf center_atom, center_struct, pair_off, pair_j, pair_shift, pair_dist, pair_dir, pair_center;
 };
-// Builds the full list with self pairs and the strict cutoff. Synchronises
-// the stream a few times to size buffers. Throws Error on invalid input.
+// Capacities for a neighbour list built without host synchronisation: the
+// buffers are sized to them, the kernels stop at them and set status 104
+// when a count exceeds its capacity (the results are then unusable).
+struct NlCaps {
+  int64_t sites, boxes, pairs;
+};
+// Builds the full list with self pairs and the strict cutoff. Without caps
+// it synchronises the stream a few times to size buffers and throws Error on
+// invalid input; with caps it enqueues everything and leaves the status word
+// for the caller to read.
 void build_neighbour_list(const NlInputs & in, double cutoff, NlWork & w, NlOutputs & out,
-                          DevStatus * status_dev, DevStatus * status_host, cudaStream_t st);
+                          DevStatus * status_dev, DevStatus * status_host, cudaStream_t st,
+                          const NlCaps * caps = nullptr);
+// Site and box counts of the last list built with synchronisation.
+void neighbour_list_counts(const NlWork & w, int64_t & sites, int64_t & boxes);
 
 // ------------------------------------------------------------------ features
 struct FeatureDims {

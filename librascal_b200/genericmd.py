@@ -7,10 +7,12 @@ a list of atomic numbers, and returns energy, forces and the 3 x 3 stress
 for each position and cell update, assuming the order and identity of the
 atoms do not change.
 
-Each step keeps one structures handle: the positions are updated in place
-(`rgpu_structures_update_positions`), the neighbour list is rebuilt on the
-device and one `rgpu_gap_predict_stress` call returns energy, forces and
-stress together. No device buffer is reallocated after the first step.
+Each step keeps one structures handle. With the FP32 path on a periodic
+system whose cell does not change, a step is one `rgpu_md_step` call: the
+whole step, neighbour list included, is recorded once as a CUDA graph and
+replayed with the new positions. Otherwise the positions are updated in
+place and one `rgpu_gap_predict_stress` call returns energy, forces and
+stress together; no device buffer is reallocated after the first step.
 """
 import numpy as np
 
@@ -79,17 +81,21 @@ class GenericMDCalculator:
         pos = self._wrap(positions, cell_matrix)
         frame = dict(positions=pos, numbers=self.numbers, cell=cell_matrix, pbc=self.pbc)
         batch = frames_to_batch([frame])
-        if self.structures is None or self._cell is None or not np.array_equal(self._cell, cell_matrix) \
-                or not np.any(self.pbc):
+        new_cell = self.structures is None or self._cell is None or not np.array_equal(self._cell, cell_matrix) \
+            or not np.any(self.pbc)
+        if new_cell:
             # first step, a new cell, or a cluster whose bounding-box cell follows the atoms
             if self.structures is None:
                 self.structures = StructureSet(batch)
             else:
                 self.structures.set(batch)
             self._cell = cell_matrix.copy()
+        if self.model.precision == "fp32" and np.any(self.pbc):
+            E, F, NS = self.model._gap().md_step(self.structures, batch["positions"], stress=True)
         else:
-            self.structures.update_positions(batch["positions"])
-        E, F, NS = self.model._gap().predict_stress(self.structures, self.model.precision)
+            if not new_cell:
+                self.structures.update_positions(batch["positions"])
+            E, F, NS = self.model._gap().predict_stress(self.structures, self.model.precision)
         energy = E
         stress_voigt = -NS[0]
         stress_matrix = np.zeros((3, 3))

@@ -292,6 +292,20 @@ class GAPModel:
                                                 N.ptr(F, N.c_dbl_p), N.ptr(NS, N.c_dbl_p)))
         return E, F, NS
 
+    def md_step(self, structures, positions, stress=False):
+        """One MD step on `structures` with new `positions` (n_atoms x 3,
+        inside the cells), FP32 path: (energies, forces, negative stress or
+        None). After the first call the step replays a recorded CUDA graph
+        (rgpu_md_step)."""
+        pos = N.f64(positions)
+        E = np.zeros(structures.n_structures)
+        F = np.zeros((structures.n_atoms, 3))
+        NS = np.zeros((structures.n_structures, 6)) if stress else None
+        N.check(N.lib().rgpu_md_step(self._h, structures.handle, N.ptr(pos, N.c_dbl_p), N.ptr(E, N.c_dbl_p),
+                                     N.ptr(F, N.c_dbl_p), N.ptr(NS, N.c_dbl_p)))
+        structures.batch = dict(structures.batch, positions=pos)
+        return E, F, NS
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and N._lib is not None:

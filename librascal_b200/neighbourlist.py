@@ -146,6 +146,15 @@ class StructureSet:
     def synchronize(self):
         N.check(N.lib().rgpu_synchronize(self._h))
 
+    def md_step_info(self):
+        """(recorded, (site, box, pair capacities), replays since the
+        recording, reason code of the last step that did not replay) of the
+        MD step graph (rgpu_md_step_info)."""
+        rec = ctypes.c_int32()
+        info = np.zeros(5, np.int64)
+        N.check(N.lib().rgpu_md_step_info(self._h, ctypes.byref(rec), N.ptr(info, N.c_i64_p)))
+        return bool(rec.value), tuple(int(c) for c in info[:3]), int(info[3]), int(info[4])
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and N._lib is not None:
