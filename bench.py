@@ -52,9 +52,10 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=40, help="clusters in the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="gap", choices=["gap", "training"],
+    p.add_argument("--workload", default="gap", choices=["gap", "training", "md"],
                    help="gap: E+F prediction (the headline); training: sparse-kernel K_NM energy and "
-                        "gradient rows for GAP fitting")
+                        "gradient rows for GAP fitting; md: MD steps of the reference's fitted methane "
+                        "model (rgpu_md_step)")
     return p.parse_args()
 
 
@@ -339,6 +340,84 @@ def run_training(args):
     return 0
 
 
+MD_METRIC = "GAP MD steps/s on 1 B200 (energy, forces, stress per step; FP32 path, recorded step)"
+
+
+def run_md(args):
+    """One step = rgpu_md_step on the 10-atom methane dimer with the
+    reference's fitted GAP model (tests/golden/simple_gap_model.json):
+    positions in from host memory, energy, forces and stress out to host
+    memory, each step replaying the recorded CUDA graph."""
+    import torch
+    import librascal_b200 as rb
+    from librascal_b200 import io
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    golden = os.path.join(ROOT, "tests", "golden")
+    krr = io.load_obj(os.path.join(golden, "simple_gap_model.json"))
+    frame = io.read_extxyz(os.path.join(golden, "methane_dimer_sample.xyz"), 0)
+    cell = frame["cell"]
+    pos0 = frame["positions"] + np.diag(cell) / 2.0
+    st = rb.StructureSet(rb.frames_to_batch([dict(frame, positions=pos0)]))
+    model = krr._gap()
+    ext = torch.cuda.ExternalStream(st.stream())
+    rng = np.random.default_rng(args.seed)
+    steps = [pos0 + 0.01 * rng.normal(size=pos0.shape) for _ in range(args.warmup + args.steps)]
+    for p in steps[:args.warmup]:
+        model.md_step(st, p, stress=True)
+    lib = rb.lib()
+    l0 = lib.rgpu_kernel_launches(0)
+    with Clocks(torch.cuda.current_device()) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for p in steps[args.warmup:]:
+            model.md_step(st, p, stress=True)
+        e1.record(ext)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    recorded, caps, replays, _ = st.md_step_info()
+    # kernels replayed from the graph do not pass the library's launch
+    # counter: count the graph's kernel nodes per replayed step
+    launches = int(lib.rgpu_kernel_launches(0) - l0) + st.md_graph_kernels * min(replays, args.steps)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        h = krr.get_representation_calculator()._get_init_params()
+        oc = O.Calculator(h["interaction_cutoff"], h["cutoff_smooth_width"], h["max_radial"], h["max_angular"],
+                          h["gaussian_sigma_constant"], spline=False, normalize=h["normalize"],
+                          radial_scaling=h["cutoff_function_parameters"])
+        species = krr.X_train.get_species()
+        T = krr.X_train.dense(species)
+        sps = np.asarray(krr.X_train.species)
+        n_cpu = 20
+        t = time.perf_counter()
+        for p in steps[:n_cpu]:
+            b = rb.frames_to_batch([dict(frame, positions=p)])
+            O.Run(oc, b, species, gradients=True).gap_stress(sps, T, krr.weights, krr.kernel.zeta)
+        secs = time.perf_counter() - t
+        cpu = dict(value=n_cpu / secs, unit="steps/s", cores=1, kind="port",
+                   sample="%d steps of the same structure, CPU FP64 restatement (direct GTO as the model "
+                          "asks), 1 thread, %.2f s" % (n_cpu, secs))
+    n_atoms = len(frame["numbers"])
+    line = dict(metric=MD_METRIC, value=1e3 / ms, unit="steps/s", n_gpus=1, steps=args.steps,
+                warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="the reference's methane-dimer structure with 0.01 A random displacements",
+                config=dict(workload="methane dimer (10 atoms, periodic 30 A cell), simple_gap_model.json "
+                                     "(rc 7.5, n 4, l 2, RadialScaling, 30 sparse points, zeta 2)",
+                            recorded_graph=bool(recorded), replays=replays, capacities=caps,
+                            l2="inputs far below L2; a latency measurement"),
+                roofline=dict(bound="hbm", kernel="latency-bound step (about 40 small launches)",
+                              achieved=None, peak=None, unit="GB/s", frac=None, traffic=None,
+                              note="a 10-atom step moves a few hundred KB; the measure is latency"),
+                cpu_baseline=cpu,
+                e2e=dict(value=1e3 / ms, unit="steps/s", h2d_bytes_per_step=int(8 * 3 * n_atoms),
+                         d2h_bytes_per_step=int(8 * (1 + 3 * n_atoms + 6))),
+                gpu_launches=launches, clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -346,6 +425,8 @@ def main():
         return run_reference_arm(args)
     if args.workload == "training":
         return run_training(args)
+    if args.workload == "md":
+        return run_md(args)
     import torch
     import librascal_b200 as rb
     from librascal_b200 import sharding, synthetic

@@ -251,9 +251,9 @@ rgpu_status rgpu_md_step(rgpu_gap_model * m, rgpu_structures * s, const double *
  * not replayed (0 none, 1 one of its device buffers was reallocated by
  * another call on this handle or model, 3 another model,
  * layout or stress setting, 100 + status code when the replayed step set
- * one, e.g. 204 for outgrown capacities). No counterpart in the
- * reference. */
-rgpu_status rgpu_md_step_info(const rgpu_structures * s, int32_t * recorded, int64_t * info /* [5] */);
+ * one, e.g. 204 for outgrown capacities) and the number of kernels one
+ * replay launches. No counterpart in the reference. */
+rgpu_status rgpu_md_step_info(const rgpu_structures * s, int32_t * recorded, int64_t * info /* [6] */);
 
 /* Sparse kernel matrices for training a GAP model, FP64 (the reference's
  * arithmetic). Columns follow the order of the model's sparse points;

@@ -205,6 +205,7 @@ struct rgpu_structures {
   std::vector<const void *> md_buffers;  // device buffer addresses at recording
   std::vector<int> md_species;
   int64_t md_replays{0};       // replays since the graph was recorded
+  int64_t md_kernels{0};       // kernel nodes of the recorded graph
   int64_t md_reason{0};        // why the last step did not replay: 0 none (first step or no
                                // recording), 1 a buffer moved, 3 model or layout, 100 + status
   bool md_no_graph{false};     // recording failed once: ordinary path only
@@ -1460,6 +1461,18 @@ static void md_step_impl(rgpu_gap_model * m, rgpu_structures * s, const double *
   s->md_stress = stress;
   s->md_buffers = md_buffers(m, s);
   s->md_species = s->species;
+  {
+    size_t n = 0;
+    s->md_kernels = 0;
+    if (cudaGraphGetNodes(s->md_graph, nullptr, &n) == cudaSuccess && n > 0) {
+      std::vector<cudaGraphNode_t> nodes(n);
+      if (cudaGraphGetNodes(s->md_graph, nodes.data(), &n) == cudaSuccess)
+        for (cudaGraphNode_t nd : nodes) {
+          cudaGraphNodeType t;
+          if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++s->md_kernels;
+        }
+    }
+  }
   s->md_replays = 0;
   // the ordinary step above already produced this call's results; the
   // positions of the next step arrive in md_pos_h
@@ -1932,6 +1945,7 @@ rgpu_status rgpu_md_step_info(const rgpu_structures * s, int32_t * recorded, int
       info[2] = s->md_caps.pairs;
       info[3] = s->md_replays;
       info[4] = s->md_reason;
+      info[5] = s->md_kernels;
     }
   });
 }

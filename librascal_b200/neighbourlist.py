@@ -151,8 +151,9 @@ class StructureSet:
         recording, reason code of the last step that did not replay) of the
         MD step graph (rgpu_md_step_info)."""
         rec = ctypes.c_int32()
-        info = np.zeros(5, np.int64)
+        info = np.zeros(6, np.int64)
         N.check(N.lib().rgpu_md_step_info(self._h, ctypes.byref(rec), N.ptr(info, N.c_i64_p)))
+        self.md_graph_kernels = int(info[5])
         return bool(rec.value), tuple(int(c) for c in info[:3]), int(info[3]), int(info[4])
 
     def __del__(self):
