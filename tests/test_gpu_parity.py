@@ -1,6 +1,6 @@
 """GPU parity against the CPU oracle, through the C ABI.
 
-Bars (BASELINE / north_star):
+Bars:
   * neighbour list: identical pairs, order, shifts, distances and directions
     (bit-exact; the oracle fixes the FP association, no FMA);
   * plain FP64 features and gradients: <= 1e-10 in the reference's
