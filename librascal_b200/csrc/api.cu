@@ -935,17 +935,20 @@ static void gap_predict_impl(rgpu_gap_model * m, rgpu_structures * s, int precis
     else
       gap_fast(m, s, s->E_d.as<double>(), s->F_d.as<double>(), want_forces, stress_d);
     mark(s, 8);
-    if (energies) {
-      RGPU_CUDA(cudaMemcpyAsync(energies, s->E_d.p, sizeof(double) * s->n_struct, cudaMemcpyDeviceToHost, s->st));
-    }
-    if (forces) {
-      RGPU_CUDA(cudaMemcpyAsync(forces, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, s->st));
-    }
-    if (neg_stress) {
-      RGPU_CUDA(cudaMemcpyAsync(neg_stress, s->S_d.p, sizeof(double) * 6 * s->n_struct, cudaMemcpyDeviceToHost,
-                                s->st));
-    }
+    // outputs through the pinned staging buffer: a device-to-host copy into
+    // the caller's pageable memory is staged by the driver at a fraction of
+    // the bandwidth
+    const size_t eb = energies ? sizeof(double) * s->n_struct : 0, fb = forces ? sizeof(double) * 3 * na : 0,
+                 sb = neg_stress ? sizeof(double) * 6 * s->n_struct : 0;
+    if (eb + fb + sb > s->pinned_cap) RGPU_CUDA(cudaStreamSynchronize(s->st));  // no copy may use the old buffer
+    unsigned char * pin = static_cast<unsigned char *>(staging(s, eb + fb + sb + 64));
+    if (eb) RGPU_CUDA(cudaMemcpyAsync(pin, s->E_d.p, eb, cudaMemcpyDeviceToHost, s->st));
+    if (fb) RGPU_CUDA(cudaMemcpyAsync(pin + eb, s->F_d.p, fb, cudaMemcpyDeviceToHost, s->st));
+    if (sb) RGPU_CUDA(cudaMemcpyAsync(pin + eb + fb, s->S_d.p, sb, cudaMemcpyDeviceToHost, s->st));
     RGPU_CUDA(cudaStreamSynchronize(s->st));
+    if (eb) std::memcpy(energies, pin, eb);
+    if (fb) std::memcpy(forces, pin + eb, fb);
+    if (sb) std::memcpy(neg_stress, pin + eb + fb, sb);
     if (precision == RGPU_PRECISION_FP32) {
       const int where = gemm_tc_timeout(true);
       if (where)
