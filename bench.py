@@ -1,18 +1,41 @@
 #!/usr/bin/env python
-"""GAP energy + forces throughput (atoms/s) on many uneven small molecules.
+"""GAP energy + forces throughput (atoms/s) on one B200, FP32 adjoint path
+against the plain FP64 GPU path, with the force error of the fast path.
 
-Workload (one step = one pass of the hot path over one batch): 10 000
-non-periodic random-walk clusters of 3..29 atoms (Z in {1,6,7,8,9}, half H),
-SOAP power spectrum with r_c = 5 A, smooth width 0.5 A, n_max = 8,
-l_max = 6, sigma = 0.4 A, GTO spline, normalised; sparse GAP with 4000
-sparse environments (proportional to the species counts), zeta = 2,
-weights ~ N(0, 1). Each step builds the neighbour list, the expansion, the
-power spectrum, the GAP energies and the forces of every atom.
+Workloads (one step = one pass of the hot path over one batch: neighbour
+list, spherical expansion, power spectrum, GAP energies, forces of every
+atom):
 
-  value  device-resident inputs (uploaded once), outputs left on the device;
-  e2e    through the C ABI with host buffers: the step's structures are
-         copied host->device and the energies and forces device->host
-         inside the timed region.
+  gap        (default) 10 000 non-periodic random-walk clusters of 3..29
+             atoms (Z in {1,6,7,8,9}, half H); r_c 5 A, smooth width 0.5 A,
+             n_max 8, l_max 6, sigma 0.4 A, GTO spline, normalised; 4 000
+             sparse environments in proportion to the species counts,
+             zeta 2, weights ~ N(0, 1)
+  bulk       one periodic cubic box of 100 000 atoms at 0.05 atoms/A^3,
+             Z in {14, 8} 1:2; r_c 6, n_max 12, l_max 9, sigma 0.5; 4 000
+             sparse points in proportion to the species counts
+  triclinic  256 sheared periodic cells of 32..512 atoms at 0.1 atoms/A^3,
+             Z in {1,6,7,8}; r_c 5, n_max 8, l_max 6, sigma 0.4; 2 000
+             sparse points per species
+  training   K_NM energy and gradient rows for GAP fitting (FP64)
+  md         MD steps of the reference's fitted methane model
+
+Reported for the gap-like workloads:
+  value     FP32 path, device-resident inputs (uploaded once), outputs left
+            on the device;
+  e2e       the same through the C ABI with host buffers: the step's
+            structures are copied host->device and the energies and forces
+            device->host inside the timed region;
+  plain_fp64_ms_per_step, speedup_vs_plain_fp64
+            the plain FP64 GPU path (the reference's algorithm with the
+            materialised dX/dr) on the same batch, timed the same way;
+  force_err, energy_err
+            max|F32 - F64| / max|F64| and max|E32 - E64| / max|E64| over the
+            whole batch, and both GPU paths against the CPU oracle on the
+            CPU-baseline sample (oracle_errors);
+  roofline  the tensor-core GEMMs against the measured sustained BF16 rate;
+            stage_roofline gives every per-centre kernel against HBM and the
+            measured FP32 FMA rate.
 
 `--impl reference` times the CPU restatement of the reference algorithm (the
 oracle; the reference itself cannot be built here) on a bounded sample of
@@ -31,12 +54,63 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-HYPERS = dict(interaction_cutoff=5.0, cutoff_smooth_width=0.5, max_radial=8, max_angular=6,
-              gaussian_sigma_type="Constant", gaussian_sigma_constant=0.4,
-              optimization=dict(Spline=dict(accuracy=1e-8)))
 METRIC = "GAP E+F atoms/s on 1 B200: adjoint+FP32 vs plain FP64 GPU, force err <=1e-4"
-WORKLOAD = ("molecule_clusters: 10000 non-periodic clusters of 3-29 atoms, Z in {1,6,7,8,9} (H 0.5), "
-            "rc 5.0, n 8, l 6, sigma 0.4, GTO spline, 4000 sparse points, zeta 2")
+FORCE_ERR_BAR = 1e-4
+TARGET_SPEEDUP = 5.0
+
+
+def _hypers(rc, n, l, sigma):
+    return dict(interaction_cutoff=rc, cutoff_smooth_width=0.5, max_radial=n, max_angular=l,
+                gaussian_sigma_type="Constant", gaussian_sigma_constant=sigma,
+                optimization=dict(Spline=dict(accuracy=1e-8)))
+
+
+def workload_spec(name, seed):
+    """Hypers, batch maker, sparse-point rule, the batch the sparse points
+    are picked from and the CPU sample of one gap-like workload."""
+    from librascal_b200 import synthetic
+    if name == "gap":
+        return dict(
+            name=name, hypers=_hypers(5.0, 8, 6, 0.4), n_sparse=4000, per_species=None,
+            desc=("molecule_clusters: 10000 non-periodic clusters of 3-29 atoms, Z in {1,6,7,8,9} (H 0.5), "
+                  "rc 5.0, n 8, l 6, sigma 0.4, GTO spline, 4000 sparse points, zeta 2"),
+            make=lambda n_struct, s: synthetic.molecule_clusters(n_struct=n_struct, seed=s),
+            default_struct=10000, shardable=True,
+            # sparse points: picked from the features of the first 1 000 clusters
+            selection=lambda batch: _first(batch, 1000),
+            # CPU sample: the first clusters of the batch
+            sample=lambda batch, k: _first(batch, k), sample_default=40,
+            sample_desc="first %d clusters")
+    if name == "bulk":
+        return dict(
+            name=name, hypers=_hypers(6.0, 12, 9, 0.5), n_sparse=4000, per_species=None,
+            desc=("bulk_box: one periodic cubic box of 100000 atoms at 0.05 atoms/A^3, Z in {14,8} 1:2, "
+                  "min distance 1.2 A, rc 6.0, n 12, l 9, sigma 0.5, GTO spline, 4000 sparse points, zeta 2"),
+            make=lambda n_struct, s: synthetic.bulk_box(seed=s),
+            default_struct=1, shardable=False,
+            # a box of 8 000 atoms with the same density and composition
+            selection=lambda batch: synthetic.bulk_box(n_atoms=8000, seed=seed + 17),
+            # a 300-atom box of the same density and composition (side 18.2 A)
+            sample=lambda batch, k: synthetic.bulk_box(n_atoms=300, seed=seed + 23), sample_default=1,
+            sample_desc="one 300-atom box of the same density and composition (%d)")
+    if name == "triclinic":
+        return dict(
+            name=name, hypers=_hypers(5.0, 8, 6, 0.4), n_sparse=None, per_species=2000,
+            desc=("triclinic_cells: 256 periodic cells with +-10% shear, 32-512 atoms at 0.1 atoms/A^3, "
+                  "Z in {1,6,7,8}, rc 5.0, n 8, l 6, sigma 0.4, GTO spline, 2000 sparse points per species, "
+                  "zeta 2"),
+            make=lambda n_struct, s: synthetic.triclinic_cells(n_struct=n_struct, seed=s),
+            default_struct=256, shardable=True,
+            selection=lambda batch: _first(batch, 64),
+            sample=lambda batch, k: _first(batch, k), sample_default=2,
+            sample_desc="first %d cells")
+    raise ValueError(name)
+
+
+def _first(batch, k):
+    from librascal_b200 import sharding
+    k = min(k, len(batch["atom_offsets"]) - 1)
+    return sharding.shard_batch(batch, 0, k)
 
 
 def parse():
@@ -46,16 +120,19 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    p.add_argument("--n-struct", type=int, default=10000)
-    p.add_argument("--n-sparse", type=int, default=4000)
+    p.add_argument("--n-struct", type=int, default=None, help="structures per GPU (default: the workload's)")
+    p.add_argument("--n-sparse", type=int, default=None)
     p.add_argument("--seed", type=int, default=0)
-    p.add_argument("--cpu-sample", type=int, default=40, help="clusters in the CPU baseline sample")
+    p.add_argument("--cpu-sample", type=int, default=None, help="structures in the CPU baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="gap", choices=["gap", "training", "md"],
-                   help="gap: E+F prediction (the headline); training: sparse-kernel K_NM energy and "
-                        "gradient rows for GAP fitting; md: MD steps of the reference's fitted methane "
-                        "model (rgpu_md_step)")
+    p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison")
+    p.add_argument("--plain-steps", type=int, default=2)
+    p.add_argument("--workload", default="gap", choices=["gap", "bulk", "triclinic", "training", "md"],
+                   help="gap: E+F prediction on 10 000 molecule clusters (the headline); bulk: one periodic "
+                        "100 000-atom box (n 12, l 9); triclinic: 256 sheared periodic cells, 2 000 sparse "
+                        "points per species; training: sparse-kernel K_NM energy and gradient rows for GAP "
+                        "fitting; md: MD steps of the reference's fitted methane model (rgpu_md_step)")
     return p.parse_args()
 
 
@@ -66,25 +143,28 @@ def dist_env():
     return rank, world, local
 
 
-def sparse_selection(rb, calc, batch, n_sparse, seed):
-    """4000 sparse environments, per species in proportion to its atom count,
-    picked at random (seeded) from features of the first 1000 clusters."""
-    from librascal_b200 import synthetic
-    off = batch["atom_offsets"]
-    n_pick = min(1000, len(off) - 1)
-    sub = {k: v for k, v in batch.items() if k != "atom_offsets"}
-    a1 = off[n_pick]
-    sub = dict(atom_offsets=off[:n_pick + 1], positions=batch["positions"][:a1], numbers=batch["numbers"][:a1],
-               cells=batch["cells"][:n_pick], pbc=batch["pbc"][:n_pick])
-    species = sorted(set(int(z) for z in batch["numbers"]))
-    al = calc.transform(rb.AtomsList(rb.StructureSet(sub)))
-    keys = calc.get_keys(species)
-    X = al.get_features(calc, keys=keys)
-    info = al.get_representation_info()
-    counts = {s: int(np.sum(batch["numbers"] == s)) for s in species}
+def sparse_counts(numbers, species, n_sparse, per_species):
+    """Sparse points per species: a fixed number each, or n_sparse split in
+    proportion to the species' atom counts."""
+    if per_species is not None:
+        return {s: int(per_species) for s in species}
+    counts = {s: int(np.sum(numbers == s)) for s in species}
     tot = sum(counts.values())
     per = {s: int(round(n_sparse * c / tot)) for s, c in counts.items()}
     per[species[0]] += n_sparse - sum(per.values())
+    return per
+
+
+def sparse_selection(rb, calc, sel_batch, numbers, n_sparse, per_species, seed):
+    """Sparse environments picked at random (seeded) from the features of
+    sel_batch, per species as sparse_counts gives them; weights ~ N(0, 1)."""
+    from librascal_b200 import synthetic
+    species = sorted(set(int(z) for z in numbers) | set(int(z) for z in sel_batch["numbers"]))
+    al = calc.transform(rb.AtomsList(rb.StructureSet(sel_batch)))
+    keys = calc.get_keys(species)
+    X = al.get_features(calc, keys=keys)
+    info = al.get_representation_info()
+    per = sparse_counts(numbers, species, n_sparse, per_species)
     idx = synthetic.select_sparse_points(X, info[:, 2], per, seed=seed)
     rng = np.random.default_rng(seed + 1)
     alpha = rng.normal(size=len(idx))
@@ -93,30 +173,38 @@ def sparse_selection(rb, calc, batch, n_sparse, seed):
     return sp, alpha, species, X[idx], info[idx, 2]
 
 
-def oracle_sample(batch, n_clusters, species, T, sps, alpha, threads=1):
-    """Time the CPU restatement (reference algorithm, FP64) on the first
-    n_clusters structures; returns (seconds, atoms)."""
+def oracle_calc(hypers):
+    from oracle import oracle as O
+    return O.Calculator(hypers["interaction_cutoff"], hypers["cutoff_smooth_width"], hypers["max_radial"],
+                        hypers["max_angular"], hypers["gaussian_sigma_constant"], spline=True, accuracy=1e-8)
+
+
+def oracle_run(hypers, batch, species, T, sps, alpha, threads=1):
+    """The CPU restatement (reference algorithm, FP64) on every structure of
+    `batch`, one structure per task; returns (seconds, atoms, E, F)."""
     from concurrent.futures import ThreadPoolExecutor
     from oracle import oracle as O
-    calc = O.Calculator(HYPERS["interaction_cutoff"], HYPERS["cutoff_smooth_width"], HYPERS["max_radial"],
-                        HYPERS["max_angular"], HYPERS["gaussian_sigma_constant"], spline=True, accuracy=1e-8)
+    calc = oracle_calc(hypers)
     off = batch["atom_offsets"]
+    n = len(off) - 1
 
     def one(i):
         a0, a1 = off[i], off[i + 1]
         b = dict(atom_offsets=np.array([0, a1 - a0]), positions=batch["positions"][a0:a1],
                  numbers=batch["numbers"][a0:a1], cells=batch["cells"][i:i + 1], pbc=batch["pbc"][i:i + 1])
         r = O.Run(calc, b, species, gradients=True)
-        r.gap(sps, T, alpha, 2)
-        return int(a1 - a0)
+        return r.gap(sps, T, alpha, 2)
 
     t = time.perf_counter()
     if threads <= 1:
-        atoms = sum(one(i) for i in range(n_clusters))
+        res = [one(i) for i in range(n)]
     else:
         with ThreadPoolExecutor(threads) as ex:
-            atoms = sum(ex.map(one, range(n_clusters)))
-    return time.perf_counter() - t, atoms
+            res = list(ex.map(one, range(n)))
+    secs = time.perf_counter() - t
+    E = np.concatenate([r[0] for r in res])
+    F = np.concatenate([r[1] for r in res])
+    return secs, int(off[-1]), E, F
 
 
 class Clocks:
@@ -186,71 +274,58 @@ def peaks():
     return 1400.0, 6650.0, "fallback sustained"
 
 
-# DRAM bytes (read + write) per grouped GEMM launch at the benchmark workload:
-# the average of the forward and backward launches of one capture of the
-# 2 000-cluster case (32 505 atoms), scaled by atoms to 160 449 atoms
-# (profiles/gemm_tc_bf16x3_clusters2000.md).
+def fma_peaks(lib):
+    """FP32 and FP64 FMA TFLOP/s of this GPU, measured by the library's
+    microbenchmark (rgpu_measure_fma_peak)."""
+    import ctypes
+    out = {}
+    for name, prec in (("fp32", 1), ("fp64", 0)):
+        v = ctypes.c_double()
+        rc = lib.rgpu_measure_fma_peak(prec, ctypes.byref(v))
+        out[name] = v.value if rc == 0 else None
+    return out
+
+
+# DRAM bytes (read + write) per grouped GEMM launch at the molecule-cluster
+# workload: the average of the forward and backward launches of one ncu
+# capture of the 2 000-cluster case (32 505 atoms), scaled by atoms to
+# 160 449 atoms.
 GEMM_TRAFFIC_PER_LAUNCH = 0.5 * (1.498e9 + 1.766e9) * 160449 / 32505
 
 
-def run_reference_arm(args):
-    rank, world, _ = dist_env()
-    if rank != 0:
-        return 0
-    from librascal_b200 import synthetic
-    # the first clusters of the same seeded batch as the GPU arm; the sparse
-    # points come from the oracle features of the first 1 000 of them (enough
-    # centres of every species for the 4 000-point model)
-    n_pool = 1000
-    batch = synthetic.molecule_clusters(n_struct=max(args.cpu_sample * (args.steps + args.warmup), n_pool),
-                                        seed=args.seed)
-    species = sorted(set(int(z) for z in batch["numbers"]))
-    from oracle import oracle as O
-    calc = O.Calculator(HYPERS["interaction_cutoff"], HYPERS["cutoff_smooth_width"], HYPERS["max_radial"],
-                        HYPERS["max_angular"], HYPERS["gaussian_sigma_constant"], spline=True, accuracy=1e-8)
-    off = batch["atom_offsets"]
-    k = min(n_pool, len(off) - 1)
-    sub = dict(atom_offsets=off[:k + 1], positions=batch["positions"][:off[k]], numbers=batch["numbers"][:off[k]],
-               cells=batch["cells"][:k], pbc=batch["pbc"][:k])
-    r = O.Run(calc, sub, species)
-    X = r.power_spectrum()
-    ca, _, _ = r.centers()
-    rowsp = sub["numbers"][ca]
-    counts = {s: int(np.sum(batch["numbers"] == s)) for s in species}
-    tot = sum(counts.values())
-    per = {s: int(round(args.n_sparse * c / tot)) for s, c in counts.items()}
-    idx = synthetic.select_sparse_points(X, rowsp, per, seed=args.seed)
-    T, sps = X[idx], rowsp[idx]
-    alpha = np.random.default_rng(args.seed + 1).normal(size=len(idx))
-    threads = os.cpu_count() or 1
-    rates, secs_timed = [], []
-    for step in range(args.warmup + args.steps):
-        lo = step * args.cpu_sample
-        b = dict(atom_offsets=off[lo:lo + args.cpu_sample + 1] - off[lo],
-                 positions=batch["positions"][off[lo]:off[lo + args.cpu_sample]],
-                 numbers=batch["numbers"][off[lo]:off[lo + args.cpu_sample]],
-                 cells=batch["cells"][lo:lo + args.cpu_sample], pbc=batch["pbc"][lo:lo + args.cpu_sample])
-        secs, atoms = oracle_sample(b, args.cpu_sample, species, T, sps, alpha, threads)
-        if step >= args.warmup:
-            rates.append(atoms / secs)
-            secs_timed.append(secs)
-    v = float(np.mean(rates))
-    line = dict(metric=METRIC, value=v, unit="atoms/s", n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
-                ms_per_step=1e3 * float(np.mean(secs_timed)), higher_is_better=True, scaling="weak",
-                vs_baseline=None, dtype="f64",
-                data="synthetic", impl="reference",
-                config=dict(workload=WORKLOAD, sample="%d clusters per step, %d sparse points" %
-                            (args.cpu_sample, len(idx))),
-                cpu_baseline=dict(value=v, unit="atoms/s", cores=threads, kind="port",
-                                  sample="%d clusters (%d sparse points) per step, CPU FP64 restatement, "
-                                         "%d threads" % (args.cpu_sample, len(idx), threads)),
-                e2e=dict(value=v, unit="atoms/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
-    print(json.dumps(line), flush=True)
-    return 0
+def row_stride(L):
+    """Floats between consecutive (species, radial) rows of the FP32
+    expansion coefficients: l-blocks padded to 4 floats, the stride an odd
+    multiple of 4."""
+    s = sum((2 * l + 1 + 3) // 4 * 4 for l in range(L + 1))
+    return s if (s // 4) % 2 == 1 else s + 4
 
 
+def stage_roofline(stages, nc, n_pairs, n_atoms, S, n, L, Dpad, hbm, fp32):
+    """Per-centre kernels of the FP32 path against HBM: algorithmic bytes each
+    kernel must move in its layout (pair data read once, per-centre arrays
+    read or written once) over its CUDA-event time."""
+    K = (L + 1) ** 2
+    C = 4.0 * nc * S * n * row_stride(L)   # FP32 expansion coefficients
+    dC = 4.0 * nc * S * n * K              # dE/dC
+    X2 = 4.0 * nc * Dpad                   # BF16 hi + lo rows
+    pair = 36.0 * n_pairs                  # distance, direction, neighbour index
+    rows = {
+        "expansion": (2, pair + C),
+        "power_spectrum": (3, C + X2 + 4.0 * nc),
+        "ps_backward": (6, C + X2 + 4.0 * nc * Dpad + dC + 4.0 * nc),
+        "pair_adjoint": (7, pair + 4.0 * n_pairs + dC + 24.0 * n_atoms),
+    }
+    out = {}
+    for k, (i, b) in rows.items():
+        ms = float(stages[i])
+        gbs = b / (ms * 1e-3) / 1e9 if ms > 0 else None
+        out[k] = dict(ms=round(ms, 4), algorithmic_gb=round(b / 1e9, 4), achieved_gbs=gbs,
+                      frac_hbm=(gbs / hbm) if gbs else None)
+    out["peaks"] = dict(hbm_gbs=hbm, fp32_tflops_measured=fp32)
+    return out
 TRAINING_METRIC = "GAP training K_NM rows (energy + position gradients) atoms/s on 1 B200, FP64"
-FP64_NOMINAL_TFLOPS = 37.0  # no measured FP64 peak on this pool; B200 nominal FP64 (CUDA cores)
+FP64_NOMINAL_TFLOPS = 37.0  # B200 nominal FP64 (CUDA cores), used only if the measurement fails
 
 
 def run_training(args):
@@ -261,11 +336,14 @@ def run_training(args):
     from librascal_b200 import _native as N, synthetic
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    n_struct = min(args.n_struct, 1000)
+    spec = workload_spec("gap", args.seed)
+    hypers = spec["hypers"]
+    n_struct = min(args.n_struct or 1000, 1000)
     batch = synthetic.molecule_clusters(n_struct=n_struct, seed=args.seed + rank)
     n_atoms = int(batch["atom_offsets"][-1])
-    calc = rb.SphericalInvariants(**HYPERS)
-    sp, alpha, species, T_sel, sps_sel = sparse_selection(rb, calc, batch, args.n_sparse, args.seed)
+    calc = rb.SphericalInvariants(**hypers)
+    sp, alpha, species, T_sel, sps_sel = sparse_selection(rb, calc, batch, batch["numbers"],
+                                                          args.n_sparse or spec["n_sparse"], None, args.seed)
     kern = rb.Kernel(calc, name="GAP", zeta=2, target_type="Structure", kernel_type="Sparse")
     model = kern._model(sp)
     st = rb.StructureSet(batch)
@@ -308,8 +386,7 @@ def run_training(args):
         off = batch["atom_offsets"]
         sub = dict(atom_offsets=off[:ns + 1], positions=batch["positions"][:off[ns]],
                    numbers=batch["numbers"][:off[ns]], cells=batch["cells"][:ns], pbc=batch["pbc"][:ns])
-        oc = O.Calculator(HYPERS["interaction_cutoff"], HYPERS["cutoff_smooth_width"], HYPERS["max_radial"],
-                          HYPERS["max_angular"], HYPERS["gaussian_sigma_constant"], spline=True, accuracy=1e-8)
+        oc = oracle_calc(hypers)
         t = time.perf_counter()
         r = O.Run(oc, sub, species, gradients=True)
         r.kernel_nm(sps_sel, T_sel, 2)
@@ -318,6 +395,10 @@ def run_training(args):
         cpu = dict(value=float(off[ns]) / secs, unit="atoms/s", cores=1, kind="port",
                    sample="first %d clusters (%d atoms), K_NM energy + gradient rows, CPU FP64 restatement, "
                           "1 thread, %.1f s" % (ns, int(off[ns]), secs))
+    fp64_peak = fma_peaks(lib)["fp64"]
+    fp64_kind = "measured FP64 FMA rate of this GPU (rgpu_measure_fma_peak)"
+    if not fp64_peak:
+        fp64_peak, fp64_kind = FP64_NOMINAL_TFLOPS, "nominal FP64 (the measurement failed)"
     line = dict(metric=TRAINING_METRIC, value=value, unit="atoms/s", n_gpus=1, steps=args.steps,
                 warmup=args.warmup, ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f64", data="synthetic",
@@ -328,9 +409,8 @@ def run_training(args):
                             l2="inputs larger than L2: dX/dr chunks of up to 24 GB"),
                 roofline=dict(bound="fp64", kernel="gathered FP64 tile GEMM of the gradient block (dgemm.cuh), "
                               "with the materialised dX/dr chunks in the same timed stage",
-                              achieved=achieved, peak=FP64_NOMINAL_TFLOPS, unit="TFLOP/s",
-                              frac=achieved / FP64_NOMINAL_TFLOPS, traffic=None,
-                              peak_kind="nominal FP64 (no measured FP64 peak on this pool)",
+                              achieved=achieved, peak=fp64_peak, unit="TFLOP/s",
+                              frac=achieved / fp64_peak, traffic=None, peak_kind=fp64_kind,
                               flops_per_step=flops),
                 cpu_baseline=cpu,
                 e2e=dict(value=n_atoms / float(np.mean(wall)), unit="atoms/s", h2d_bytes_per_step=0,
@@ -418,31 +498,109 @@ def run_md(args):
     return 0
 
 
-def main():
-    args = parse()
-    rank, world, local = dist_env()
-    if args.impl == "reference":
-        return run_reference_arm(args)
-    if args.workload == "training":
-        return run_training(args)
-    if args.workload == "md":
-        return run_md(args)
+def run_reference_arm(args):
+    """The reference algorithm (CPU restatement, FP64) on a bounded sample of
+    the workload per step, with all host threads; rank 0 only."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    spec = workload_spec(args.workload if args.workload in ("gap", "bulk", "triclinic") else "gap", args.seed)
+    hypers = spec["hypers"]
+    k = args.cpu_sample or spec["sample_default"]
+    n_struct = args.n_struct or spec["default_struct"]
+    if spec["shardable"]:
+        # the first structures of the same seeded batch as the GPU arm, a
+        # new sample for every step
+        batch = spec["make"](max(k * (args.steps + args.warmup), min(n_struct, 1000)), args.seed)
+        samples = [_slice(batch, step * k, (step + 1) * k) for step in range(args.warmup + args.steps)]
+    else:
+        samples = [spec["sample"](None, k)] * (args.warmup + args.steps)
+        batch = spec["make"](1, args.seed)
+    sel = spec["selection"](batch)
+    species = sorted(set(int(z) for z in batch["numbers"]) | set(int(z) for z in sel["numbers"]))
+    # sparse points from the oracle's features of the selection batch
+    r = O.Run(oracle_calc(hypers), sel, species)
+    X = r.power_spectrum()
+    ca, _, _ = r.centers()
+    rowsp = sel["numbers"][ca]
+    from librascal_b200 import synthetic
+    per = sparse_counts(batch["numbers"], species, args.n_sparse or spec["n_sparse"], spec["per_species"])
+    idx = synthetic.select_sparse_points(X, rowsp, per, seed=args.seed)
+    T, sps = X[idx], rowsp[idx]
+    alpha = np.random.default_rng(args.seed + 1).normal(size=len(idx))
+    threads = os.cpu_count() or 1
+    rates, secs_timed = [], []
+    for step, b in enumerate(samples):
+        secs, atoms, _, _ = oracle_run(hypers, b, species, T, sps, alpha, threads)
+        if step >= args.warmup:
+            rates.append(atoms / secs)
+            secs_timed.append(secs)
+    v = float(np.mean(rates))
+    desc = spec["sample_desc"] % k
+    line = dict(metric=METRIC, value=v, unit="atoms/s", n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
+                ms_per_step=1e3 * float(np.mean(secs_timed)), higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic", impl="reference",
+                config=dict(workload=spec["desc"], sample="%s per step, %d sparse points" % (desc, len(idx))),
+                cpu_baseline=dict(value=v, unit="atoms/s", cores=threads, kind="port",
+                                  sample="%s (%d sparse points) per step, CPU FP64 restatement, %d threads"
+                                         % (desc, len(idx), threads)),
+                e2e=dict(value=v, unit="atoms/s", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _slice(batch, a, b):
+    from librascal_b200 import sharding
+    n = len(batch["atom_offsets"]) - 1
+    return sharding.shard_batch(batch, min(a, n), min(b, n))
+
+
+def rel_err(a, b):
+    """max|a - b| / max|b| (0 for an all-zero reference)."""
+    d = float(np.abs(np.asarray(a) - np.asarray(b)).max()) if np.size(b) else 0.0
+    s = float(np.abs(np.asarray(b)).max()) if np.size(b) else 0.0
+    return d / s if s > 0 else d
+
+
+def run_gap(args):
+    """The gap-like workloads: FP32 adjoint path timed with device-resident
+    inputs (value) and through the C ABI with host buffers (e2e), the plain
+    FP64 GPU path on the same batch, the accuracy of both, and the CPU
+    baseline."""
     import torch
     import librascal_b200 as rb
-    from librascal_b200 import sharding, synthetic
+    from librascal_b200 import _native as N, sharding
+    rank, world, local = dist_env()
+    spec = workload_spec(args.workload, args.seed)
+    hypers = spec["hypers"]
     pg = None
     if world > 1:
-        import torch.distributed as dist
         import datetime
+        import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
     torch.cuda.set_device(local)
     dev = torch.cuda.current_device()
 
-    batch = synthetic.molecule_clusters(n_struct=args.n_struct, seed=args.seed + rank)
+    n_struct = args.n_struct or spec["default_struct"]
+    if spec["shardable"]:
+        # one seeded batch of world x n_struct structures, cut into per-rank
+        # shards of nearly equal cost: every GPU has about n_struct
+        # structures' work (weak scaling) and no two ranks share a structure
+        full = spec["make"](n_struct * world, args.seed)
+        parts = sharding.partition(sharding.structure_costs(full), world)
+        batch = sharding.shard_batch(full, *parts[rank])
+        parallelism = "dp%d: structures sharded across ranks by cost (sharding.partition)" % world
+    else:
+        full = spec["make"](1, args.seed + rank)  # one box per rank: replicas
+        batch = full
+        parallelism = "dp%d: one box per rank (replicas)" % world
     n_atoms = int(batch["atom_offsets"][-1])
-    calc = rb.SphericalInvariants(**HYPERS)
-    sp, alpha, species, T_sel, sps_sel = sparse_selection(rb, calc, batch, args.n_sparse, args.seed)
+    calc = rb.SphericalInvariants(**hypers)
+    sp, alpha, species, T_sel, sps_sel = sparse_selection(rb, calc, spec["selection"](full), full["numbers"],
+                                                          args.n_sparse or spec["n_sparse"], spec["per_species"],
+                                                          args.seed)
     model = rb.GAPModel(calc, sp, alpha, zeta=2)
     st = rb.StructureSet(batch)
     ext = torch.cuda.ExternalStream(st.stream())
@@ -456,10 +614,24 @@ def main():
     def max_over_ranks(x):
         return sharding.max_over_ranks(x, device="cuda") if pg is not None else x
 
+    def timed(step, steps, warmup):
+        for _ in range(warmup):
+            step()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        for _ in range(steps):
+            step()
+        e1.record(ext)
+        e1.synchronize()
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1)) / steps
+
     # ---- value: inputs resident, outputs on the device
-    def step_resident():
+    def step_resident(precision=args.precision):
         st.invalidate()
-        model.predict(st, args.precision, energies=False, forces=False)
+        model.predict(st, precision, energies=False, forces=False)
 
     for _ in range(args.warmup):
         step_resident()
@@ -484,10 +656,15 @@ def main():
         step_resident()
         stages += st.stage_times()
     stages /= 3
-    off = batch["atom_offsets"]
+    import ctypes
+    nc_, np_ = ctypes.c_int64(), ctypes.c_int64()
+    N.check(lib.rgpu_neighbour_list_size(st.handle, ctypes.byref(nc_), ctypes.byref(np_)))
+    n_centers, n_pairs = nc_.value, np_.value
     counts = np.array([np.sum(batch["numbers"] == s) for s in species])
     msp = np.array([int(np.sum(np.asarray(sp.species) == s)) for s in species])
-    D = len(species) * (len(species) + 1) // 2 * HYPERS["max_radial"] ** 2 * (HYPERS["max_angular"] + 1)
+    S, n, L = len(species), hypers["max_radial"], hypers["max_angular"]
+    D = S * (S + 1) // 2 * n ** 2 * (L + 1)
+    Dpad = (D + 31) // 32 * 32
     gemm_flops = 4.0 * float(np.sum(counts * msp)) * D  # forward + backward
     gemm_ms = stages[4] + stages[5]
     bf16_peak, hbm_peak, peak_kind = peaks()
@@ -495,6 +672,7 @@ def main():
 
     # ---- e2e: host buffers through the C ABI
     e2e = None
+    off = batch["atom_offsets"]
     if not args.no_e2e:
         E = np.zeros(len(off) - 1)
         F = np.zeros((n_atoms, 3))
@@ -503,68 +681,109 @@ def main():
         num = np.ascontiguousarray(batch["numbers"], np.int32)
         cel = np.ascontiguousarray(batch["cells"], np.float64)
         pbc = np.ascontiguousarray(batch["pbc"], np.int32)
-        from librascal_b200 import _native as N
+        prec = N.PRECISION_FP32 if args.precision == "fp32" else N.PRECISION_FP64
 
         def step_e2e():
             N.check(lib.rgpu_structures_set(st.handle, len(off64) - 1, N.ptr(off64, N.c_i64_p),
                                             N.ptr(pos, N.c_dbl_p), N.ptr(num, N.c_int_p), N.ptr(cel, N.c_dbl_p),
                                             N.ptr(pbc, N.c_int_p), None))
-            N.check(lib.rgpu_gap_predict(model.handle, st.handle, N.PRECISION_FP32 if args.precision == "fp32"
-                                         else N.PRECISION_FP64, N.ptr(E, N.c_dbl_p), N.ptr(F, N.c_dbl_p)))
+            N.check(lib.rgpu_gap_predict(model.handle, st.handle, prec, N.ptr(E, N.c_dbl_p), N.ptr(F, N.c_dbl_p)))
 
-        for _ in range(args.warmup):
-            step_e2e()
-        barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(ext)
-        for _ in range(args.steps):
-            step_e2e()
-        e1.record(ext)
-        e1.synchronize()
-        barrier()
-        ms_e2e = max_over_ranks(e0.elapsed_time(e1)) / args.steps
+        ms_e2e = timed(step_e2e, args.steps, args.warmup)
         h2d = off64.nbytes + pos.nbytes + num.nbytes + cel.nbytes + pbc.nbytes
         h2d += 4 * (len(off64) - 1) + 8 * len(off64) + 4 * n_atoms  # centre counts, offsets, atom->structure
         d2h = E.nbytes + F.nbytes
         e2e = dict(value=n_atoms * world / (ms_e2e * 1e-3), unit="atoms/s", h2d_bytes_per_step=int(h2d),
                    d2h_bytes_per_step=int(d2h), ms_per_step=ms_e2e)
 
-    # ---- CPU baseline (rank 0, N = 1)
+    # ---- the metric's comparison: the plain FP64 GPU path, same batch
+    plain = None
+    acc = None
+    if not args.no_plain and args.precision == "fp32":
+        plain_ms = timed(lambda: step_resident("fp64"), max(args.plain_steps, 1), 1)
+        plain_stages = st.stage_times()
+        st.invalidate()
+        E32, F32 = model.predict(st, "fp32")
+        st.invalidate()
+        E64, F64 = model.predict(st, "fp64")
+        st.invalidate()
+        acc = dict(force_err=max_over_ranks(rel_err(F32, F64)), energy_err=max_over_ranks(rel_err(E32, E64)))
+        plain = dict(ms=plain_ms, stage_ms=[round(float(x), 3) for x in plain_stages])
+
+    # ---- CPU baseline and the accuracy of both GPU paths against the oracle
+    # on the same sample (rank 0, N = 1)
     cpu = None
+    oracle_errors = None
+    fma = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        k = args.cpu_sample or spec["sample_default"]
+        sample = spec["sample"](batch, k)
         T = sp.dense(species)
-        secs, atoms = oracle_sample(batch, args.cpu_sample, species, T, np.asarray(sp.species), alpha, 1)
+        secs, atoms, E_o, F_o = oracle_run(hypers, sample, species, T, np.asarray(sp.species), alpha, 1)
         cpu = dict(value=atoms / secs, unit="atoms/s", cores=1, kind="port",
-                   sample="first %d clusters (%d atoms), E+F, CPU FP64 restatement of the reference algorithm, "
-                          "1 thread, %.1f s" % (args.cpu_sample, atoms, secs))
+                   sample="%s (%d atoms), E+F, CPU FP64 restatement of the reference algorithm, 1 thread, "
+                          "%.1f s" % (spec["sample_desc"] % k, atoms, secs))
+        ss = rb.StructureSet(sample)
+        oracle_errors = dict(sample=spec["sample_desc"] % k, atoms=atoms)
+        for prec in ("fp64", "fp32"):
+            Eg, Fg = model.predict(ss, prec)
+            ss.invalidate()
+            oracle_errors[prec] = dict(force_err=rel_err(Fg, F_o), energy_err=rel_err(Eg, E_o))
+        del ss
+    if rank == 0:
+        fma = fma_peaks(lib)
 
     if rank == 0:
+        speedup = (plain["ms"] / ms) if plain else None
         line = dict(
             metric=METRIC, value=value, unit="atoms/s", n_gpus=world, steps=args.steps, warmup=args.warmup,
             ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None,
             dtype="f32" if args.precision == "fp32" else "f64", data="synthetic",
-            config=dict(workload=WORKLOAD, n_structures=int(len(off) - 1), n_atoms=n_atoms,
-                        sparse_points=int(sp.size()), precision=args.precision,
-                        parallelism="dp%d (independent structures per rank)" % world,
-                        l2="inputs larger than L2: X and dE/dX are %.1f GB each" %
-                           (n_atoms * D * 4 / 1e9),
+            config=dict(workload=spec["desc"], n_structures=int(len(off) - 1), n_atoms=n_atoms,
+                        n_pairs=int(n_pairs), sparse_points=int(sp.size()), precision=args.precision,
+                        parallelism=parallelism,
+                        l2="inputs larger than L2: X and dE/dX are %.1f GB each" % (n_atoms * Dpad * 4 / 1e9),
                         stage_ms=dict(zip(["total", "neighbour_list", "expansion", "power_spectrum",
                                            "gemm_fwd", "gemm_bwd", "ps_backward", "pair_adjoint"],
                                           [round(float(x), 4) for x in stages]))),
+            plain_fp64_ms_per_step=plain["ms"] if plain else None,
+            plain_fp64_atoms_per_s=(n_atoms * world / (plain["ms"] * 1e-3)) if plain else None,
+            plain_fp64_stage_ms=plain["stage_ms"] if plain else None,
+            speedup_vs_plain_fp64=speedup,
+            force_err=acc["force_err"] if acc else None,
+            energy_err=acc["energy_err"] if acc else None,
+            force_err_bar=FORCE_ERR_BAR,
+            meets_target=(bool(speedup >= TARGET_SPEEDUP and acc["force_err"] <= FORCE_ERR_BAR)
+                          if plain else None),
+            oracle_errors=oracle_errors,
             roofline=dict(bound="tensor", kernel="tcgen05 BF16x3 GEMMs (forward + backward)",
                           achieved=achieved, peak=bf16_peak, unit="TFLOP/s",
                           frac=(achieved / bf16_peak) if achieved else None,
-                          traffic=GEMM_TRAFFIC_PER_LAUNCH if args.n_struct == 10000 else None,
+                          traffic=(GEMM_TRAFFIC_PER_LAUNCH if (args.workload == "gap" and n_struct == 10000)
+                                   else None),
                           peak_kind="%s dense bf16; achieved counts algorithmic 2MNK flops, the "
                                     "3-term split issues 3x that on the tensor pipe" % peak_kind,
                           issued_frac=(3 * achieved / bf16_peak) if achieved else None,
                           flops_per_step=gemm_flops),
+            stage_roofline=stage_roofline(stages, n_centers, n_pairs, n_atoms, S, n, L, Dpad, hbm_peak,
+                                          fma["fp32"] if fma else None),
+            measured_fma_tflops=fma,
             cpu_baseline=cpu, e2e=e2e, gpu_launches=launches, clocks=clk.summary())
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()
     return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    if args.workload == "training":
+        return run_training(args)
+    if args.workload == "md":
+        return run_md(args)
+    return run_gap(args)
 
 
 if __name__ == "__main__":

@@ -226,6 +226,29 @@ rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s,
                                     int precision, double * energies,
                                     double * forces, double * neg_stress);
 
+/* The adjoint path split for automatic differentiation (a
+ * torch.autograd.Function): the reference computes energies and forces in
+ * separate calls, KRR.predict and KRR.predict_forces
+ * (bindings/rascal/models/krr.py:92-166); here the forward keeps on the
+ * device what the force pass needs, and the backward applies an upstream
+ * gradient per structure. Both run the FP32 path; DEVICE pointers, ordered on
+ * the structure set's stream (rgpu_structures_stream), which is synchronised
+ * before the calls return.
+ * Forward: positions_dev [n_atoms x 3] FP64 (NULL: keep the current
+ * positions; otherwise they replace them, inside the cells as for
+ * rgpu_structures_set) -> energies_dev [n_structures] FP64, baseline
+ * included. */
+rgpu_status rgpu_gap_forward_dev(rgpu_gap_model * m, rgpu_structures * s,
+                                 const double * positions_dev,
+                                 double * energies_dev);
+/* Backward of the last rgpu_gap_forward_dev of the same model on the same
+ * structures (RGPU_ERR_NOT_COMPUTED if another call on the structures came
+ * in between): grad_dev [n_atoms x 3] FP64 = sum_A energies_grad_dev[A]
+ * dE_A/dr. */
+rgpu_status rgpu_gap_backward_dev(rgpu_gap_model * m, rgpu_structures * s,
+                                  const double * energies_grad_dev,
+                                  double * grad_dev);
+
 /* One step of a molecular-dynamics loop on the structures of the last
  * rgpu_structures_set (same atoms, types and cells; positions wrapped into
  * the cells): new positions [n_atoms x 3] in; energies, forces and, when
@@ -298,6 +321,12 @@ int64_t rgpu_kernel_launches(int reset);
  * gradient chunks (materialised dX/dr and the gathered GEMMs). */
 rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out,
                              int32_t n_stages);
+/* Measured FMA throughput of the current device's CUDA cores in TFLOP/s,
+ * FP32 (RGPU_PRECISION_FP32) or FP64 (RGPU_PRECISION_FP64) pipe: every SM
+ * filled with independent FMA chains, best of five launches timed with CUDA
+ * events (2 flops per FMA). The denominator of the FP32- and FP64-pipe
+ * roofline fractions. No counterpart in the reference. */
+rgpu_status rgpu_measure_fma_peak(int precision, double * tflops);
 
 /* ---------------------------------------------------------------------- */
 /* Unit-test hook for the tensor-core GEMM (no reference counterpart; the
@@ -313,6 +342,15 @@ rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K,
                                    float * C_dev, float * e_dev,
                                    void * stream);
 
+/* Test hook for the bounded waits of the tensor-core GEMMs (no reference
+ * counterpart): the number of polls after which the MMA warp's wait for
+ * staged operands gives up (0: at once; negative: the default, about 4 M
+ * polls). A wait that gives up makes the GEMM wind down (copies and MMAs
+ * already started are waited for, TMEM is freed) and the call return
+ * RGPU_ERR_TIMEOUT; the status is cleared for the next call. Process-wide;
+ * restore the default after use. */
+rgpu_status rgpu_debug_set_gemm_wait_limit(int64_t polls);
+
 /* ---------------------------------------------------------------------- */
 /* GAP energies without device allocation. No counterpart in the reference:
  * it is the per-row energy of the mode-1 GEMM above,
@@ -321,14 +359,16 @@ rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K,
  * synchronise the whole device, stalling every other stream of a process
  * that shares the GPU, such as an MD integrator's own kernels).
  * DEVICE pointers, row-major FP32: A [M x K], B [N x K], alpha [N], e [M].
- * All scratch lives in one static 16 MiB device array; sizes needing more
- * (about 4 M Kp + 4 N Kp + 4 M Np + 4 M ceil(N/256) bytes, Kp = K rounded up
- * to 64, Np = N rounded up to 32) return RGPU_ERR_CAPACITY.
- * The first call on each device does the setup (symbol lookup, kernel
- * attributes) and should precede any stream capture. The call is ordered on
- * `stream` (a cudaStream_t or NULL) and returns after it completes; calls
- * that overlap in time share the scratch and race, so callers serialise
- * them. */
+ * All scratch lives in one static 16 MiB device array, which every GPU that
+ * loads the library holds until the process exits; sizes needing more
+ * (about 4 M Kp + 4 N Kp + 4 M ceil(N/256) bytes, Kp = K rounded up to 64)
+ * return RGPU_ERR_CAPACITY before any pointer is touched.
+ * The first call on each device does the setup (the address lookup of the
+ * static arrays, kept for the life of the process; a cudaDeviceReset after
+ * it is not supported) and should precede any stream capture. The work is
+ * ordered on `stream` (a cudaStream_t or NULL), and the call synchronises
+ * that stream before it returns, to read the GEMM's status word. Calls that
+ * overlap in time share the scratch and race, so callers serialise them. */
 rgpu_status rgpu_gap_energies_noalloc(int64_t M, int64_t N, int64_t K,
                                       const float * A_dev, const float * B_dev,
                                       const float * alpha_dev, int32_t zeta,

@@ -16,7 +16,10 @@ LIB_PATH = os.path.join(_HERE, "_lib", "librascal_b200.so")
 RGPU_OK = 0
 PRECISION_FP64 = 0
 PRECISION_FP32 = 1
+ERR_INVALID_ARGUMENT = 1  # RGPU_ERR_INVALID_ARGUMENT
 ERR_CAPACITY = 3  # RGPU_ERR_CAPACITY
+ERR_TIMEOUT = 4  # RGPU_ERR_TIMEOUT
+ERR_NOT_COMPUTED = 7  # RGPU_ERR_NOT_COMPUTED
 
 _EXC_OVERFLOW = 3
 
@@ -62,6 +65,8 @@ SIGNATURES = {
                                         c_dbl_p]),
     "rgpu_gap_predict_stress": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, c_dbl_p,
                                                c_dbl_p, c_dbl_p]),
+    "rgpu_gap_forward_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rgpu_gap_backward_dev": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rgpu_md_step": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, c_dbl_p, c_dbl_p, c_dbl_p, c_dbl_p]),
     "rgpu_md_step_info": (ctypes.c_int, [ctypes.c_void_p, c_int_p, c_i64_p]),
     "rgpu_sparse_kernel": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, c_dbl_p]),
@@ -70,9 +75,11 @@ SIGNATURES = {
     "rgpu_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
     "rgpu_kernel_launches": (ctypes.c_int64, [ctypes.c_int]),
     "rgpu_stage_times": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p, ctypes.c_int32]),
+    "rgpu_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, c_dbl_p]),
     "rgpu_debug_gemm_bf16x3": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rgpu_debug_set_gemm_wait_limit": (ctypes.c_int, [ctypes.c_int64]),
     "rgpu_gap_energies_noalloc": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                                  ctypes.c_void_p, ctypes.c_void_p]),

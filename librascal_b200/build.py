@@ -32,6 +32,7 @@ SOURCES = [
     ("gemm.cu", [], "gemm"),
     ("gemm_tc.cu", [], "gemm_tc"),
     ("noalloc.cu", [], "noalloc"),
+    ("peaks.cu", [], "peaks"),
     ("adjoint.cu", [], "adjoint"),
     ("training.cu", [], "training"),
     ("api.cu", [], "api"),

@@ -149,6 +149,7 @@ void parse_hypers(const std::string & kind, const std::string & text, Hypers & h
 
 // ------------------------------------------------------------------ handles
 struct rgpu_calculator {
+  int device{-1};  // device of the uploaded tables (-1: not uploaded yet)
   Hypers hy;
   RadialSpline spline;
   DevBuf grid, y, y2h, yf, y2hf, q4f, center;
@@ -158,6 +159,7 @@ struct rgpu_calculator {
 struct GapLayout;
 
 struct rgpu_structures {
+  int device{-1};  // device current at creation: owns the stream and every buffer
   cudaStream_t st{nullptr};
   int n_struct{0};
   int64_t n_atoms{0};
@@ -212,6 +214,10 @@ struct rgpu_structures {
   double * md_pos_h{nullptr};  // pinned: positions in, outputs out
   double * md_out_h{nullptr};
   size_t md_pos_cap{0}, md_out_cap{0};
+  // autograd: the model whose forward (rgpu_gap_forward_dev) left W, the
+  // features and the list in place for rgpu_gap_backward_dev (null: none)
+  const rgpu_gap_model * fwd_model{nullptr};
+  DevBuf y0_d;  // per-structure energy baseline of fwd_model
   // status and timing
   DevStatus * status_d{nullptr};
   DevStatus * status_h{nullptr};
@@ -221,6 +227,7 @@ struct rgpu_structures {
 };
 
 struct rgpu_gap_model {
+  int device{-1};  // device of the model's buffers (-1: none allocated yet)
   rgpu_calculator * calc{nullptr};
   std::vector<int> species;  // model layout species (sorted)
   int M{0};
@@ -243,8 +250,46 @@ struct rgpu_gap_model {
 
 namespace {
 
+// Runs the rest of a call on a structure set's device and gives the caller
+// back the device that was current before. A structure set belongs to the
+// device that was current when it was created (its stream and buffers live
+// there), so a call made while another device is current still works on its
+// own device's memory.
+struct OnDevice {
+  int prev{-1};
+  explicit OnDevice(const rgpu_structures * s) {
+    if (!s || s->device < 0) return;
+    int cur = 0;
+    RGPU_CUDA(cudaGetDevice(&cur));
+    if (cur != s->device) {
+      RGPU_CUDA(cudaSetDevice(s->device));
+      prev = cur;
+    }
+  }
+  ~OnDevice() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  OnDevice(const OnDevice &) = delete;
+  OnDevice & operator=(const OnDevice &) = delete;
+};
+
+// Ties a calculator or model to the current device on its first device
+// allocation, and rejects later use with a structure set of another device
+// (its buffers would be another GPU's memory).
+void bind_device(int & owner, const char * what) {
+  const int dev = current_device();
+  if (owner < 0) {
+    owner = dev;
+  } else if (owner != dev) {
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, std::string(what) + " lives on device " + std::to_string(owner) +
+                                               " and cannot be used with a structure set of device " +
+                                               std::to_string(dev));
+  }
+}
+
 void ensure_stream(rgpu_structures * s) {
   if (!s->st) {
+    s->device = current_device();
     RGPU_CUDA(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
     RGPU_CUDA(cudaMalloc(&s->status_d, sizeof(DevStatus)));
     RGPU_CUDA(cudaMemset(s->status_d, 0, sizeof(DevStatus)));
@@ -255,7 +300,10 @@ void ensure_stream(rgpu_structures * s) {
 
 void * staging(rgpu_structures * s, size_t bytes) {
   if (bytes > s->pinned_cap) {
-    if (s->pinned) cudaFreeHost(s->pinned);
+    if (s->pinned) {
+      RGPU_CUDA(cudaStreamSynchronize(s->st));  // no copy in flight may still use it
+      cudaFreeHost(s->pinned);
+    }
     s->pinned = nullptr;
     RGPU_CUDA(cudaMallocHost(&s->pinned, bytes));
     s->pinned_cap = bytes;
@@ -334,6 +382,7 @@ void set_layout(rgpu_structures * s, const Hypers & hy, const std::vector<int> &
 
 void build_nl(rgpu_structures * s, double cutoff) {
   if (s->nl_valid && s->nl_cutoff == cutoff) return;
+  s->fwd_model = nullptr;
   NlInputs in;
   in.n_struct = s->n_struct;
   in.n_atoms = s->n_atoms;
@@ -412,6 +461,7 @@ void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, b
     s->feat_gradients = s->feat_gradients || grads;
     return;
   }
+  s->fwd_model = nullptr;
   mark(s, 2);
   sort_rows(s);
   const int64_t nc = s->nl.n_centers;
@@ -570,6 +620,7 @@ void model_layout_bf16(rgpu_gap_model * m, rgpu_structures * s);
 // Device copies of a model's sparse points in the batch's layout: FP64
 // always, the BF16 splits of the tensor-core path only when `bf16` asks.
 void model_layout(rgpu_gap_model * m, rgpu_structures * s, bool bf16) {
+  bind_device(m->device, "the GAP model");
   const FeatureDims & fd = s->fd;
   if (m->layout_species == s->species && m->layout_D == fd.D) {
     if (bf16 && !m->layout_bf16) model_layout_bf16(m, s);
@@ -769,12 +820,25 @@ int64_t eofs_of(const rgpu_structures * s, const rgpu_gap_model * m, int sI) {
   return o;
 }
 
-void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_d, bool forces,
-              double * stress_d) {
-  rgpu_calculator * c = m->calc;
+// W offsets of the species segments (rows x Mpad BF16 each) in s->Wh/Wl.
+std::vector<int64_t> w_offsets(const rgpu_gap_model * m, const rgpu_structures * s) {
+  std::vector<int64_t> wofs(s->fd.S);
+  int64_t woff = 0;
+  for (int sI = 0; sI < s->fd.S; ++sI) {
+    wofs[sI] = woff;
+    woff += s->species_count[sI] * m->segs[sI].Mpad;
+  }
+  return wofs;
+}
+
+// Fast path, forward half: the grouped tcgen05 GEMM with the GAP epilogue
+// (energy partials and W = alpha zeta k^(zeta-1) as a BF16 pair), then the
+// per-structure energies (baseline not included).
+void gap_fast_forward(rgpu_gap_model * m, rgpu_structures * s, double * E_d) {
   const FeatureDims & fd = s->fd;
   const int64_t nc = s->nl.n_centers;
   cudaStream_t st = s->st;
+  s->fwd_model = nullptr;
   mark(s, 4);
   // per-species W (BF16 hi/lo) and energy partial buffers
   int64_t wtot = 0, eparts = 0;
@@ -790,13 +854,12 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
   const __nv_bfloat16 * Xl = s->Xl.as<__nv_bfloat16>();
   __nv_bfloat16 * Wh = s->Wh.as<__nv_bfloat16>();
   __nv_bfloat16 * Wl = s->Wl.as<__nv_bfloat16>();
-  int64_t row0 = 0, woff = 0;
-  std::vector<int64_t> wofs(fd.S);
+  const std::vector<int64_t> wofs = w_offsets(m, s);
+  int64_t row0 = 0;
   std::vector<Bf16x3Gemm> fwd;
   for (int sI = 0; sI < fd.S; ++sI) {
     const int64_t rows = s->species_count[sI];
     const GapSpecies & g = m->segs[sI];
-    wofs[sI] = woff;
     if (rows > 0 && g.M > 0) {
       Bf16x3Gemm a{};
       a.M = rows;
@@ -809,8 +872,8 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
       a.B_lo = m->Tl.as<__nv_bfloat16>() + size_t(g.m0) * fd.Dpad;
       a.ldb = fd.Dpad;
       a.epilogue = 1;
-      a.W_hi = Wh + woff;
-      a.W_lo = Wl + woff;
+      a.W_hi = Wh + wofs[sI];
+      a.W_lo = Wl + wofs[sI];
       a.ldw = g.Mpad;
       a.alpha = m->alpha32.as<float>() + g.m0;
       a.zeta = m->zeta;
@@ -819,7 +882,6 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
       fwd.push_back(a);
     }
     row0 += rows;
-    woff += rows * g.Mpad;
   }
   gemm_bf16x3_grouped(fwd.data(), int(fwd.size()), st);
   row0 = 0;
@@ -834,8 +896,25 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
     row0 += rows;
   }
   mark(s, 5);
-  if (!forces) return;
-  row0 = 0;
+}
+
+// Fast path, backward half: dE/dx = W T (grouped GEMM), the power-spectrum
+// backward to dE/dc, then the pair adjoint into F_d (= -dE/dr) and the
+// optional stress sums. With struct_scale, the contributions of every
+// structure are multiplied by struct_scale[structure] (an upstream gradient
+// per structure energy).
+void gap_fast_backward(rgpu_gap_model * m, rgpu_structures * s, double * F_d, double * stress_d,
+                       const double * struct_scale = nullptr) {
+  rgpu_calculator * c = m->calc;
+  const FeatureDims & fd = s->fd;
+  const int64_t nc = s->nl.n_centers;
+  cudaStream_t st = s->st;
+  const __nv_bfloat16 * Xh = s->Xh.as<__nv_bfloat16>();
+  const __nv_bfloat16 * Xl = s->Xl.as<__nv_bfloat16>();
+  __nv_bfloat16 * Wh = s->Wh.as<__nv_bfloat16>();
+  __nv_bfloat16 * Wl = s->Wl.as<__nv_bfloat16>();
+  const std::vector<int64_t> wofs = w_offsets(m, s);
+  int64_t row0 = 0;
   std::vector<Bf16x3Gemm> bwd;
   for (int sI = 0; sI < fd.S; ++sI) {
     const int64_t rows = s->species_count[sI];
@@ -870,10 +949,19 @@ void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_
   s->dC32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.nK + 64);
   launch_ps_bwd_fp32(pa, s->C32.as<float>(), Xh, Xl, s->xscale32.as<float>(), s->dX32.as<float>(),
                      s->dC32.as<float>(), st);
+  if (struct_scale)
+    launch_scale_rows_by_group(s->dC32.as<float>(), nc, int64_t(fd.S) * fd.nK, s->nl.center_struct, struct_scale,
+                               st);
   mark(s, 7);
   ExpansionArgs ea = exp_args(c, s);
   launch_pair_adjoint_fp32(ea, s->nl.pair_center, s->nl.n_pairs, s->dC32.as<float>(), F_d, st,
                            s->nl.center_struct, stress_d);
+}
+
+void gap_fast(rgpu_gap_model * m, rgpu_structures * s, double * E_d, double * F_d, bool forces,
+              double * stress_d) {
+  gap_fast_forward(m, s, E_d);
+  if (forces) gap_fast_backward(m, s, F_d, stress_d);
 }
 
 }  // namespace
@@ -898,6 +986,18 @@ static double cell_volume(const double * cell) {
 
 extern "C" {
 static void calculator_to_device(rgpu_calculator * c);
+}
+
+// Energy baseline of each structure (models/krr.py:68-90), FP64 on the host:
+// a table over the atom types (validated to [0, 130) by rgpu_structures_set).
+static std::vector<double> structure_baselines(const rgpu_gap_model * m, const rgpu_structures * s) {
+  double sc[130] = {0.};
+  for (size_t i = 0; i < m->species.size(); ++i)
+    if (m->species[i] >= 0 && m->species[i] < 130) sc[m->species[i]] = m->self_contrib[i];
+  std::vector<double> y0(s->n_struct, 0.);
+  for (int k = 0; k < s->n_struct; ++k)
+    for (int64_t a = s->atom_off[k]; a < s->atom_off[k + 1]; ++a) y0[k] += sc[s->types[a]];
+  return y0;
 }
 
 // Energies, forces and (optionally) the negative stress of a GAP model: the
@@ -940,8 +1040,9 @@ static void gap_predict_impl(rgpu_gap_model * m, rgpu_structures * s, int precis
     // the bandwidth
     const size_t eb = energies ? sizeof(double) * s->n_struct : 0, fb = forces ? sizeof(double) * 3 * na : 0,
                  sb = neg_stress ? sizeof(double) * 6 * s->n_struct : 0;
-    if (eb + fb + sb > s->pinned_cap) RGPU_CUDA(cudaStreamSynchronize(s->st));  // no copy may use the old buffer
-    unsigned char * pin = static_cast<unsigned char *>(staging(s, eb + fb + sb + 64));
+    const size_t need = eb + fb + sb + 64;
+    if (need > s->pinned_cap) RGPU_CUDA(cudaStreamSynchronize(s->st));  // no copy may use the old buffer
+    unsigned char * pin = static_cast<unsigned char *>(staging(s, need));
     if (eb) RGPU_CUDA(cudaMemcpyAsync(pin, s->E_d.p, eb, cudaMemcpyDeviceToHost, s->st));
     if (fb) RGPU_CUDA(cudaMemcpyAsync(pin + eb, s->F_d.p, fb, cudaMemcpyDeviceToHost, s->st));
     if (sb) RGPU_CUDA(cudaMemcpyAsync(pin + eb + fb, s->S_d.p, sb, cudaMemcpyDeviceToHost, s->st));
@@ -956,17 +1057,8 @@ static void gap_predict_impl(rgpu_gap_model * m, rgpu_structures * s, int precis
                                           std::to_string(where) + ")");
     }
     if (energies) {
-      // baseline (models/krr.py:68-90) on the host, FP64: a table over the
-      // atom types (validated to [0, 130) by rgpu_structures_set)
-      double sc[130] = {0.};
-      for (size_t i = 0; i < m->species.size(); ++i)
-        if (m->species[i] >= 0 && m->species[i] < 130) sc[m->species[i]] = m->self_contrib[i];
-      const int32_t * types = s->types.data();
-      for (int st = 0; st < s->n_struct; ++st) {
-        double y0 = 0.;
-        for (int64_t a = s->atom_off[st]; a < s->atom_off[st + 1]; ++a) y0 += sc[types[a]];
-        energies[st] += y0;
-      }
+      const std::vector<double> y0 = structure_baselines(m, s);
+      for (int st = 0; st < s->n_struct; ++st) energies[st] += y0[st];
     }
     if (forces && precision == RGPU_PRECISION_FP64)
       for (int64_t i = 0; i < 3 * na; ++i) forces[i] = -forces[i];
@@ -976,6 +1068,65 @@ static void gap_predict_impl(rgpu_gap_model * m, rgpu_structures * s, int precis
         for (int k = 0; k < 6; ++k) neg_stress[6 * st + k] /= v;
       }
   }
+}
+
+// Forward half of the adjoint path for automatic differentiation: energies
+// of the FP32 path into device memory, with everything the backward needs
+// (neighbour list, features, W) left on the device. The reference computes
+// energies and forces in separate calls, KRR.predict and
+// KRR.predict_forces (bindings/rascal/models/krr.py:92-166).
+static void gap_forward_dev_impl(rgpu_gap_model * m, rgpu_structures * s, const double * positions_dev,
+                                 double * energies_dev) {
+  if (!m || !s || !energies_dev) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (s->has_mask)
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, "Can't compute spherical expansion gradients with masked center atoms",
+                RGPU_EXC_LOGIC_ERROR);
+  calculator_to_device(m->calc);
+  s->timed = false;
+  if (positions_dev) {
+    RGPU_CUDA(cudaMemcpyAsync(s->pos_d.p, positions_dev, sizeof(double) * 3 * s->n_atoms,
+                              cudaMemcpyDeviceToDevice, s->st));
+    s->nl_valid = false;
+    s->feat_valid = false;
+  }
+  build_nl(s, m->calc->hy.cutoff);
+  compute_features(m->calc, s, RGPU_PRECISION_FP32, true, m->species, /*need_x32=*/false);
+  model_layout(m, s, true);
+  s->E_d.ensure(sizeof(double) * (s->n_struct + 1));
+  RGPU_CUDA(cudaMemsetAsync(s->E_d.p, 0, sizeof(double) * s->n_struct, s->st));
+  gap_fast_forward(m, s, s->E_d.as<double>());
+  const std::vector<double> y0 = structure_baselines(m, s);
+  upload(s, s->y0_d, y0.data(), sizeof(double) * y0.size());
+  launch_add_f64(s->E_d.as<double>(), s->y0_d.as<double>(), energies_dev, s->n_struct, s->st);
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  const int where = gemm_tc_timeout(true);
+  if (where)
+    throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM: a bounded pipeline wait gave up (stage " +
+                                      std::to_string(where) + ")");
+  s->fwd_model = m;
+}
+
+// Backward half: grad_dev[a][c] = sum_A energies_grad_dev[A] dE_A/dr_a[c]
+// from the state the forward left: dE/dx = W T, the power-spectrum
+// backward, the per-structure scaling, the pair adjoint.
+static void gap_backward_dev_impl(rgpu_gap_model * m, rgpu_structures * s, const double * energies_grad_dev,
+                                  double * grad_dev) {
+  if (!m || !s || !energies_grad_dev || !grad_dev) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (s->fwd_model != m || !s->feat_valid || !s->nl_valid)
+    throw Error(RGPU_ERR_NOT_COMPUTED, "the backward needs the forward of the same model and structures, with "
+                                       "no other call on the structures in between");
+  s->timed = false;
+  const int64_t na = s->n_atoms;
+  s->F_d.ensure(sizeof(double) * 3 * (na + 1));
+  RGPU_CUDA(cudaMemsetAsync(s->F_d.p, 0, sizeof(double) * 3 * na, s->st));
+  gap_fast_backward(m, s, s->F_d.as<double>(), nullptr, energies_grad_dev);
+  // the adjoint accumulates forces, -dE/dr
+  launch_scale_f64(s->F_d.as<double>(), -1.0, grad_dev, 3 * na, s->st);
+  RGPU_CUDA(cudaStreamSynchronize(s->st));
+  const int where = gemm_tc_timeout(true);
+  if (where)
+    throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM: a bounded pipeline wait gave up (stage " +
+                                      std::to_string(where) + ")");
 }
 
 // ---------------------------------------------------------------- training
@@ -1507,6 +1658,7 @@ rgpu_status rgpu_calculator_destroy(rgpu_calculator * calc) {
 // Device copies of the radial table, made on first use so that a calculator
 // can be built (and its FP64 table inspected) on a host without a GPU.
 static void calculator_to_device(rgpu_calculator * c) {
+  bind_device(c->device, "the calculator");
   if (c->dev.y) return;
   {
     const RadialSpline & sp = c->spline;
@@ -1588,6 +1740,7 @@ rgpu_status rgpu_structures_create(rgpu_structures ** out) {
 
 rgpu_status rgpu_structures_destroy(rgpu_structures * s) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!s) return;
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->md_exec) cudaGraphExecDestroy(s->md_exec);
@@ -1608,6 +1761,7 @@ rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const
                                 const double * positions, const int32_t * numbers, const double * cells,
                                 const int32_t * pbc, const uint8_t * center_mask) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!s || n_structures < 0 || !atom_offsets) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
     md_drop(s);
     s->md_no_graph = false;
@@ -1671,30 +1825,39 @@ rgpu_status rgpu_structures_set(rgpu_structures * s, int32_t n_structures, const
     upload_many(s, ups);
     s->nl_valid = false;
     s->feat_valid = false;
+    s->fwd_model = nullptr;
   });
 }
 
 rgpu_status rgpu_structures_update_positions(rgpu_structures * s, const double * positions) {
   return guard([&] {
+    OnDevice on_dev(s);
     upload(s, s->pos_d, positions, sizeof(double) * 3 * s->n_atoms);
     s->nl_valid = false;
     s->feat_valid = false;
+    s->fwd_model = nullptr;
   });
 }
 
 rgpu_status rgpu_structures_invalidate(rgpu_structures * s) {
   return guard([&] {
+    OnDevice on_dev(s);
     s->nl_valid = false;
     s->feat_valid = false;
+    s->fwd_model = nullptr;
   });
 }
 
 rgpu_status rgpu_structures_stream(const rgpu_structures * s, void ** stream) {
-  return guard([&] { *stream = static_cast<void *>(s->st); });
+  return guard([&] {
+    OnDevice on_dev(s);
+    *stream = static_cast<void *>(s->st);
+  });
 }
 
 rgpu_status rgpu_neighbour_list_build(rgpu_structures * s, double cutoff) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!(cutoff > 0)) throw Error(RGPU_ERR_INVALID_ARGUMENT, "cutoff must be > 0");
     build_nl(s, cutoff);
   });
@@ -1702,6 +1865,7 @@ rgpu_status rgpu_neighbour_list_build(rgpu_structures * s, double cutoff) {
 
 rgpu_status rgpu_neighbour_list_size(const rgpu_structures * s, int64_t * n_centers, int64_t * n_pairs) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!s->nl_valid) throw Error(RGPU_ERR_NOT_COMPUTED, "the neighbour list has not been built");
     *n_centers = s->nl.n_centers;
     *n_pairs = s->nl.n_pairs;
@@ -1711,6 +1875,7 @@ rgpu_status rgpu_neighbour_list_size(const rgpu_structures * s, int64_t * n_cent
 rgpu_status rgpu_neighbour_list_get(const rgpu_structures * s, int32_t * center_atom, int64_t * pair_offsets,
                                     int32_t * j_atom, int32_t * shift, double * distance, double * direction) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!s->nl_valid) throw Error(RGPU_ERR_NOT_COMPUTED, "the neighbour list has not been built");
     const int64_t nc = s->nl.n_centers, np = s->nl.n_pairs;
     auto get = [&](void * dst, const void * src, size_t bytes) {
@@ -1728,6 +1893,7 @@ rgpu_status rgpu_neighbour_list_get(const rgpu_structures * s, int32_t * center_
 
 rgpu_status rgpu_compute(rgpu_calculator * calc, rgpu_structures * s, int precision, int gradients) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!calc || !s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
     if (precision != RGPU_PRECISION_FP64 && precision != RGPU_PRECISION_FP32)
       throw Error(RGPU_ERR_INVALID_ARGUMENT, "unknown precision");
@@ -1744,6 +1910,7 @@ rgpu_status rgpu_compute(rgpu_calculator * calc, rgpu_structures * s, int precis
 
 rgpu_status rgpu_get_species(const rgpu_structures * s, int32_t * n_species, int32_t * species) {
   return guard([&] {
+    OnDevice on_dev(s);
     *n_species = int32_t(s->species.size());
     for (size_t i = 0; i < s->species.size(); ++i) species[i] = s->species[i];
   });
@@ -1752,6 +1919,7 @@ rgpu_status rgpu_get_species(const rgpu_structures * s, int32_t * n_species, int
 rgpu_status rgpu_get_feature_keys(const rgpu_calculator * calc, const rgpu_structures * s, int32_t * n_keys,
                                   int32_t * keys) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!s->feat_valid || s->feat_calc != calc) throw Error(RGPU_ERR_NOT_COMPUTED, "features have not been computed");
     auto k = present_keys(calc, s);
     *n_keys = int32_t(k.size());
@@ -1766,6 +1934,7 @@ rgpu_status rgpu_get_feature_keys(const rgpu_calculator * calc, const rgpu_struc
 rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structures * s, int32_t n_keys,
                               const int32_t * keys, double * out) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!s->feat_valid || s->feat_calc != calc) throw Error(RGPU_ERR_NOT_COMPUTED, "features have not been computed");
     const FeatureDims & fd = s->fd;
     const int64_t nc = s->nl.n_centers;
@@ -1822,6 +1991,7 @@ rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structure
 rgpu_status rgpu_get_features_gradient(const rgpu_calculator * calc, const rgpu_structures * s_in, int32_t n_keys,
                                        const int32_t * keys, double * out) {
   return guard([&] {
+    OnDevice on_dev(s_in);
     rgpu_structures * s = const_cast<rgpu_structures *>(s_in);
     if (!s->feat_valid || s->feat_calc != calc) throw Error(RGPU_ERR_NOT_COMPUTED, "features have not been computed");
     if (!s->feat_gradients) throw Error(RGPU_ERR_NOT_COMPUTED, "gradients were not requested (compute_gradients)");
@@ -1922,24 +2092,48 @@ rgpu_status rgpu_gap_model_destroy(rgpu_gap_model * m) {
 
 rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precision, double * energies,
                              double * forces) {
-  return guard([&] { gap_predict_impl(m, s, precision, energies, forces, nullptr); });
+  return guard([&] {
+    OnDevice on_dev(s);
+    gap_predict_impl(m, s, precision, energies, forces, nullptr);
+  });
 }
 
 rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s, int precision, double * energies,
                                     double * forces, double * neg_stress) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!neg_stress) throw Error(RGPU_ERR_INVALID_ARGUMENT, "neg_stress output is required");
     gap_predict_impl(m, s, precision, energies, forces, neg_stress);
   });
 }
 
+rgpu_status rgpu_gap_forward_dev(rgpu_gap_model * m, rgpu_structures * s, const double * positions_dev,
+                                 double * energies_dev) {
+  return guard([&] {
+    OnDevice on_dev(s);
+    gap_forward_dev_impl(m, s, positions_dev, energies_dev);
+  });
+}
+
+rgpu_status rgpu_gap_backward_dev(rgpu_gap_model * m, rgpu_structures * s, const double * energies_grad_dev,
+                                  double * grad_dev) {
+  return guard([&] {
+    OnDevice on_dev(s);
+    gap_backward_dev_impl(m, s, energies_grad_dev, grad_dev);
+  });
+}
+
 rgpu_status rgpu_md_step(rgpu_gap_model * m, rgpu_structures * s, const double * positions, double * energies,
                          double * forces, double * neg_stress) {
-  return guard([&] { md_step_impl(m, s, positions, energies, forces, neg_stress); });
+  return guard([&] {
+    OnDevice on_dev(s);
+    md_step_impl(m, s, positions, energies, forces, neg_stress);
+  });
 }
 
 rgpu_status rgpu_md_step_info(const rgpu_structures * s, int32_t * recorded, int64_t * info) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!s || !recorded) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
     *recorded = s->md_exec ? 1 : 0;
     if (info) {
@@ -1955,6 +2149,7 @@ rgpu_status rgpu_md_step_info(const rgpu_structures * s, int32_t * recorded, int
 
 rgpu_status rgpu_sparse_kernel(rgpu_gap_model * m, rgpu_structures * s, int32_t target_atom, double * out) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!out) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
     sparse_kernel_impl(m, s, target_atom != 0, out);
   });
@@ -1963,6 +2158,7 @@ rgpu_status rgpu_sparse_kernel(rgpu_gap_model * m, rgpu_structures * s, int32_t 
 rgpu_status rgpu_sparse_kernel_derivative(rgpu_gap_model * m, rgpu_structures * s, int32_t neg_stress,
                                           double * out) {
   return guard([&] {
+    OnDevice on_dev(s);
     if (!out) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
     sparse_kernel_derivative_impl(m, s, neg_stress != 0, out);
   });
@@ -1992,13 +2188,25 @@ __global__ void sum_parts_kernel(const float * parts, int n_parts, int64_t M, fl
 }
 }  // namespace
 
+// Scratch of the GEMM test hook, one set per device (the hook is called
+// from one host thread at a time).
+struct DebugGemmBuffers {
+  DevBuf ah, al, bh, bl, wh, wl, parts;
+};
+static PerDevice<DebugGemmBuffers> g_debug_gemm_buffers;
+
+rgpu_status rgpu_debug_set_gemm_wait_limit(int64_t polls) {
+  return guard([&] { set_gemm_wait_limit(polls); });
+}
+
 rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K, const float * A, const float * B,
                                    const float * alpha, int32_t zeta, float * C, float * e, void * stream) {
   return guard([&] {
     if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !C) throw Error(RGPU_ERR_INVALID_ARGUMENT, "bad GEMM arguments");
     if (mode == 0 && N % 4 != 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "N must be a multiple of 4");
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    static DevBuf ah, al, bh, bl, wh, wl, parts;
+    DebugGemmBuffers & B_ = g_debug_gemm_buffers.at(current_device());
+    DevBuf &ah = B_.ah, &al = B_.al, &bh = B_.bh, &bl = B_.bl, &wh = B_.wh, &wl = B_.wl, &parts = B_.parts;
     const int64_t Kp = (K + 63) / 64 * 64, Np = (N + 31) / 32 * 32;
     ah.ensure(2 * size_t(M) * Kp);
     al.ensure(2 * size_t(M) * Kp);
@@ -2047,14 +2255,27 @@ rgpu_status rgpu_gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const flo
   return guard([&] { gap_energies_noalloc(M, N, K, A, B, alpha, zeta, e, static_cast<cudaStream_t>(stream)); });
 }
 
+rgpu_status rgpu_measure_fma_peak(int precision, double * tflops) {
+  return guard([&] {
+    if (!tflops) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    if (precision != RGPU_PRECISION_FP64 && precision != RGPU_PRECISION_FP32)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+    *tflops = measure_fma_peak(precision);
+  });
+}
+
 rgpu_status rgpu_synchronize(rgpu_structures * s) {
-  return guard([&] { RGPU_CUDA(cudaStreamSynchronize(s->st)); });
+  return guard([&] {
+    OnDevice on_dev(s);
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+  });
 }
 
 int64_t rgpu_kernel_launches(int reset) { return rgpu::launches(reset != 0); }
 
 rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out, int32_t n_stages) {
   return guard([&] {
+    OnDevice on_dev(s);
     RGPU_CUDA(cudaStreamSynchronize(s->st));
     // 0 whole call, 1 neighbour list, 2 expansion, 3 power spectrum,
     // 4 forward GEMMs, 5 backward GEMMs, 6 power-spectrum backward (plain:

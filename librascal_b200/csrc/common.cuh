@@ -91,15 +91,17 @@ struct SphConst {
   float c2f[kMaxL + 1];
 };
 // Each translation unit that evaluates spherical harmonics holds its own copy
-// (no relocatable device code); sph_constants_tu() fills it once.
+// (no relocatable device code), and every device has its own instance of
+// it: sph_constants_tu() fills the current device's copy the first time a
+// kernel of this translation unit is launched there.
 static __constant__ SphConst c_sph;
 SphConst make_sph_constants();
+static PerDevice<char> g_sph_filled;
 static inline void sph_constants_tu() {
-  static bool done = false;
-  if (done) return;
-  SphConst h = make_sph_constants();
-  cuda_check(cudaMemcpyToSymbol(c_sph, &h, sizeof(h)), "cudaMemcpyToSymbol(c_sph)");
-  done = true;
+  g_sph_filled.once(current_device(), [](char &) {
+    SphConst h = make_sph_constants();
+    cuda_check(cudaMemcpyToSymbol(c_sph, &h, sizeof(h)), "cudaMemcpyToSymbol(c_sph)");
+  });
 }
 
 template <typename T>

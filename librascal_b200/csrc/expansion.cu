@@ -138,8 +138,8 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
     lofk[lm] = uint8_t(l);
   }
   __syncthreads();
-  for (int64_t ci = int64_t(blockIdx.x) * kWarps + wid; ci < a.n_centers;
-       ci += int64_t(gridDim.x) * kWarps) {
+  const int nw = blockDim.x >> 5;  // warps per block (fewer than kWarps for large W + K)
+  for (int64_t ci = int64_t(blockIdx.x) * nw + wid; ci < a.n_centers; ci += int64_t(gridDim.x) * nw) {
     T * Ci = C + size_t(ci) * S * nK;
     for (int e = lane; e < S * nK; e += 32) Ci[e] = T(0);
     __syncwarp();
@@ -366,8 +366,8 @@ expansion_grad_kernel(ExpansionArgs a, int64_t c0, int64_t c1, int64_t p_base,
   const int W = a.fd.W, n = a.fd.n, nK = a.fd.nK;
   double * RI = reinterpret_cast<double *>(smem_raw) + size_t(wid) * 2 * W * 32;
   double * P1 = RI + W * 32;
-  for (int64_t ci = c0 + int64_t(blockIdx.x) * kWarps + wid; ci < c1;
-       ci += int64_t(gridDim.x) * kWarps) {
+  const int nw = blockDim.x >> 5;  // warps per block (fewer than kWarps for large W)
+  for (int64_t ci = c0 + int64_t(blockIdx.x) * nw + wid; ci < c1; ci += int64_t(gridDim.x) * nw) {
     const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
     for (int64_t p = p_lo + lane; p < p_hi; p += 32) {
       const double r = a.pair_dist[p];
@@ -421,25 +421,40 @@ __global__ void expansion_selfgrad_kernel(ExpansionArgs a, int64_t c0, int64_t p
   }
 }
 
+// Warps per block of a kernel whose warps each need `per_warp` bytes of
+// shared memory: kWarps, or as many as the device's per-block limit allows
+// (the FP64 tiles of large n (l+1) + (l+1)^2 do not fit four times).
+int warps_for(size_t per_warp, const char * what) {
+  int dev = 0, optin = 0;
+  RGPU_CUDA(cudaGetDevice(&dev));
+  RGPU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const int w = int(std::min<size_t>(kWarps, size_t(optin) / per_warp));
+  if (w < 1)
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, std::string(what) + ": max_radial x (max_angular + 1) too large for "
+                                                               "shared memory");
+  return w;
+}
+
 template <typename T>
-size_t exp_smem(const FeatureDims & fd) {
-  return size_t(kWarps) * (fd.W + fd.K + 1) * kPad * sizeof(T);
+size_t exp_smem_per_warp(const FeatureDims & fd) {
+  return size_t(fd.W + fd.K + 1) * kPad * sizeof(T);
 }
 
 template <typename T>
 void launch_exp(const ExpansionArgs & a, T * C, uint32_t * present, cudaStream_t st) {
   if (a.n_centers == 0) return;
   sph_constants_tu();
-  const size_t smem = exp_smem<T>(a.fd);
+  const int warps = warps_for(exp_smem_per_warp<T>(a.fd), "spherical expansion");
+  const size_t smem = size_t(warps) * exp_smem_per_warp<T>(a.fd);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int grid = int(std::min<int64_t>((a.n_centers + kWarps - 1) / kWarps, int64_t(sms) * 16));
+  int grid = int(std::min<int64_t>((a.n_centers + warps - 1) / warps, int64_t(sms) * 16));
 #define RGPU_EXP_CASE(LL)                                                                   \
   case LL:                                                                                  \
     RGPU_CUDA(cudaFuncSetAttribute(expansion_kernel<T, LL>,                                 \
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    expansion_kernel<T, LL><<<grid, kWarps * 32, smem, st>>>(a, C, present);                \
+    expansion_kernel<T, LL><<<grid, warps * 32, smem, st>>>(a, C, present);                 \
     break;
   switch (a.fd.L) {
     RGPU_EXP_CASE(0)
@@ -530,13 +545,15 @@ void launch_expansion_grad_fp64(const ExpansionArgs & a, int64_t c0, int64_t c1,
                                 double * dCp, cudaStream_t st) {
   if (c1 <= c0) return;
   sph_constants_tu();
-  const size_t smem = size_t(kWarps) * 2 * a.fd.W * 32 * sizeof(double);
-  int grid = int(std::min<int64_t>((c1 - c0 + kWarps - 1) / kWarps, 148 * 16));
+  const size_t per_warp = size_t(2) * a.fd.W * 32 * sizeof(double);
+  const int warps = warps_for(per_warp, "spherical expansion gradients");
+  const size_t smem = size_t(warps) * per_warp;
+  int grid = int(std::min<int64_t>((c1 - c0 + warps - 1) / warps, 148 * 16));
 #define RGPU_GRAD_CASE(LL)                                                                  \
   case LL:                                                                                  \
     RGPU_CUDA(cudaFuncSetAttribute(expansion_grad_kernel<LL>,                               \
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-    expansion_grad_kernel<LL><<<grid, kWarps * 32, smem, st>>>(a, c0, c1, p_base, dCp);     \
+    expansion_grad_kernel<LL><<<grid, warps * 32, smem, st>>>(a, c0, c1, p_base, dCp);      \
     break;
   switch (a.fd.L) {
     RGPU_GRAD_CASE(0)

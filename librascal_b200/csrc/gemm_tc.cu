@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 
@@ -71,14 +72,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t * bar, uint32_t parity) {
 __device__ __forceinline__ void mbar_arrive(uint64_t * bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// Bounded wait: false when the limit was hit (the status word records it).
-__device__ __forceinline__ bool mbar_wait(uint64_t * bar, uint32_t parity, TcStatus * st, int where) {
-  for (long long i = 0; i < kSpinLimit; ++i) {
+// Bounded wait: false when `limit` polls were not enough (the status word
+// records it) or another wait of the launch already gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t * bar, uint32_t parity, TcStatus * st, int where,
+                                          long long limit = kSpinLimit) {
+  for (long long i = 0; i < limit; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((i & 63) == 63 && *reinterpret_cast<volatile int *>(&st->timeout)) return false;
   }
   if (atomicCAS(&st->timeout, 0, 1) == 0) st->where = where;
   return false;
+}
+// Wait for work this CTA itself started (TMA copies into its shared memory,
+// its own MMAs) before the CTA releases the memory they write. Unlike
+// mbar_wait it does not give up when another wait of the launch has: that
+// work completes on its own, and the shared memory and TMEM must not be
+// released under it. Still bounded, by kSpinLimit polls.
+__device__ __forceinline__ void mbar_drain(uint64_t * bar, uint32_t parity, TcStatus * st, int where) {
+  for (long long i = 0; i < kSpinLimit; ++i)
+    if (mbar_try_wait(bar, parity)) return;
+  if (atomicCAS(&st->timeout, 0, 1) == 0) st->where = where;
 }
 __device__ __forceinline__ void tma_load_2d(void * dst, const CUtensorMap * map, uint64_t * bar, int x, int y) {
   asm volatile(
@@ -159,14 +172,15 @@ struct TcArgs {
   int epilogue;        // 0 store FP32 C; 1 GAP forward
   float * C;           // FP32 output (epilogue 0), row stride ldc
   int64_t ldc;
-  __nv_bfloat16 * W_hi;  // epilogue 1 outputs, row stride ldw (zero beyond N)
-  __nv_bfloat16 * W_lo;
+  __nv_bfloat16 * W_hi;  // epilogue 1 outputs, row stride ldw (zero beyond N);
+  __nv_bfloat16 * W_lo;  // W_hi == nullptr: energy partials only
   int64_t ldw;
   const float * alpha;  // [N]
   int zeta;
   float * e_part;       // [gridDim.x][M]
   const float * row_scale;  // epilogue 1: k = row_scale[row] * (A B^T) (null: 1)
   TcStatus * status;
+  long long mma_wait_limit;  // polls of the MMA warp's operand waits
 };
 
 template <int BN, int STAGES, int BK = kBK>
@@ -241,7 +255,7 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant_
       // drain: the last copies must have landed before the CTA releases its
       // shared memory (they normally have; this matters after a timeout)
       for (int kb = issued > STAGES ? issued - STAGES : 0; kb < issued; ++kb)
-        mbar_wait(&full[kb % STAGES], uint32_t(kb / STAGES) & 1u, g.status, 4);
+        mbar_drain(&full[kb % STAGES], uint32_t(kb / STAGES) & 1u, g.status, 4);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -250,7 +264,7 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant_
       for (int kb = 0; kb < nk && ok; ++kb) {
         const int s = kb % STAGES;
         const uint32_t ph = uint32_t(kb / STAGES) & 1u;
-        if (!mbar_wait(&full[s], ph, g.status, 2)) {
+        if (!mbar_wait(&full[s], ph, g.status, 2, g.mma_wait_limit)) {
           ok = false;
           break;
         }
@@ -294,7 +308,8 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant_
               if (col + i < g.N) out[i] = v[i];
           }
         } else {
-          if (col >= g.ldw) continue;
+          // W_hi == nullptr: energies only, no W output
+          if (g.W_hi && col >= g.ldw) continue;
           if (g.row_scale) {
             const float rs = __ldg(g.row_scale + row);
 #pragma unroll
@@ -309,6 +324,7 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant_
             hi[i] = __float2bfloat16_rn(w);
             lo[i] = __float2bfloat16_rn(w - __bfloat162float(hi[i]));
           }
+          if (!g.W_hi) continue;
           uint4 * dh = reinterpret_cast<uint4 *>(g.W_hi + row * g.ldw + col);
           uint4 * dl = reinterpret_cast<uint4 *>(g.W_lo + row * g.ldw + col);
           dh[0] = reinterpret_cast<uint4 *>(hi)[0];
@@ -323,6 +339,10 @@ gemm_tc_kernel(const __grid_constant__ CUtensorMap mA_hi, const __grid_constant_
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
+    // every MMA issued has finished before TMEM is released (the epilogue
+    // waited for this already unless a wait of the launch gave up)
+    if (lane == 0) mbar_drain(accum, 0u, g.status, 6);
+    __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(BN)));
   }
@@ -359,6 +379,7 @@ struct TcGroupedArgs {
   int zeta;
   int64_t n_tiles;
   TcStatus * status;
+  long long mma_wait_limit;  // polls of the MMA warp's operand waits
 };
 
 __device__ __forceinline__ int find_group(const TcGroupedArgs & p, int64_t t) {
@@ -434,7 +455,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
       // the last copies must have landed before the CTA releases its shared
       // memory (they normally have; this matters after a timeout)
       for (uint32_t k = it > uint32_t(STAGES) ? it - STAGES : 0u; k < it; ++k)
-        mbar_wait(&full[k % STAGES], (k / STAGES) & 1u, status, 4);
+        mbar_drain(&full[k % STAGES], (k / STAGES) & 1u, status, 4);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -456,7 +477,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         for (int kb = 0; kb < nk; ++kb) {
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1u;
-          if (!mbar_wait(&full[s], ph, status, 2)) {
+          if (!mbar_wait(&full[s], ph, status, 2, p.mma_wait_limit)) {
             ok = false;
             break;
           }
@@ -478,7 +499,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         mma_commit(&tfull[b]);  // also after a failed wait, so the epilogue moves on
       }
       mma_commit(done);  // completes when every MMA issued above has finished
-      mbar_wait(done, 0u, status, 6);
+      mbar_drain(done, 0u, status, 6);
     }
   } else {
     const int q = warp & 3;  // TMEM lane quadrant of this warp
@@ -605,14 +626,22 @@ void split_bf16(const float * x, int64_t rows, int64_t cols, int64_t ldx, __nv_b
   RGPU_LAUNCHED();
 }
 
-// Status word of the tcgen05 GEMM (device global, one per process).
+// Polls of the MMA warp's waits for staged operands: kSpinLimit, unless a
+// test lowers it to make those waits run out (rgpu_debug_set_gemm_wait_limit).
+static std::atomic<long long> g_mma_wait_limit{kSpinLimit};
+
+void set_gemm_wait_limit(long long polls) { g_mma_wait_limit.store(polls < 0 ? kSpinLimit : polls); }
+
+// Status word of the tcgen05 GEMM: one per device, allocated on the current
+// device the first time a GEMM runs there.
+static PerDevice<TcStatus *> g_tc_status;
 static TcStatus * tc_status() {
-  static TcStatus * p = nullptr;
-  if (!p) {
-    cuda_check(cudaMalloc(&p, sizeof(TcStatus)), "cudaMalloc(tc status)");
-    cuda_check(cudaMemset(p, 0, sizeof(TcStatus)), "cudaMemset(tc status)");
-  }
-  return p;
+  return g_tc_status.once(current_device(), [](TcStatus *& p) {
+    TcStatus * q = nullptr;
+    cuda_check(cudaMalloc(&q, sizeof(TcStatus)), "cudaMalloc(tc status)");
+    cuda_check(cudaMemset(q, 0, sizeof(TcStatus)), "cudaMemset(tc status)");
+    p = q;
+  });
 }
 
 void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st) {
@@ -638,6 +667,7 @@ void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st) {
   t.e_part = g.e_part;
   t.row_scale = g.row_scale;
   t.status = tc_status();
+  t.mma_wait_limit = g_mma_wait_limit.load();
   cuda_check(cudaFuncSetAttribute(gemm_tc_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)),
              "cudaFuncSetAttribute(gemm_tc)");
@@ -670,6 +700,7 @@ void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st)
   t.e_part = g.e_part;
   t.row_scale = g.row_scale;
   t.status = reinterpret_cast<TcStatus *>(status_dev);
+  t.mma_wait_limit = g_mma_wait_limit.load();
   cuda_check(cudaFuncSetAttribute(gemm_tc_kernel<BN, STAGES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   int(smem)),
              "cudaFuncSetAttribute(gemm_tc)");
@@ -721,6 +752,7 @@ void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
   p.n_groups = ng;
   p.n_tiles = tiles;
   p.status = tc_status();
+  p.mma_wait_limit = g_mma_wait_limit.load();
   int dev = 0, sms = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");

@@ -2,20 +2,21 @@
 //
 // e[r] = sum_n alpha_n (A_r . B_n)^zeta for FP32 device matrices A [M x K]
 // and B [N x K], computed with the tcgen05 BF16x3 GEMM and its fused GAP
-// epilogue (gemm_tc.cu). Every scratch buffer (the BF16 hi/lo splits of A
-// and B, the epilogue's W output and the per-tile energy partials) is carved
+// epilogue (gemm_tc.cu) in its energies-only form. Every scratch buffer (the
+// BF16 hi/lo splits of A and B and the per-tile energy partials) is carved
 // out of one file-scope device array, and the bounded-wait status word is a
 // second one, so a call never allocates device memory.
 //
 // Setup: the first call on a device (with that device current) looks the
-// two arrays up with cudaGetSymbolAddress; it should come before any stream
-// capture. Concurrency: all calls share the one array, so calls that
-// overlap in time (from several host threads or streams) race; callers
-// serialise them.
+// two arrays up with cudaGetSymbolAddress and keeps their addresses for the
+// life of the process; it should come before any stream capture. A
+// cudaDeviceReset after that first call is not supported: the kept
+// addresses would belong to the destroyed context. Concurrency: all calls
+// share the one array, so calls that overlap in time (from several host
+// threads or streams) race; callers serialise them.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "common.cuh"
@@ -25,7 +26,6 @@ namespace rgpu {
 namespace {
 
 constexpr size_t kScratchBytes = size_t(16) << 20;  // 16 MiB
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 static __device__ __align__(16) int g_status[4];
@@ -34,25 +34,18 @@ struct DevicePointers {
   unsigned char * scratch = nullptr;
   int * status = nullptr;
 };
-DevicePointers g_ptrs[kMaxDevices];
-std::mutex g_setup_mutex;
+PerDevice<DevicePointers> g_ptrs;
 
 // Addresses of the two arrays on the current device, looked up once.
 DevicePointers setup_current_device() {
-  int dev = 0;
-  RGPU_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) throw Error(RGPU_ERR_INVALID_ARGUMENT, "device index out of range");
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  DevicePointers & p = g_ptrs[dev];
-  if (!p.scratch) {
+  return g_ptrs.once(current_device(), [](DevicePointers & p) {
     void * s = nullptr;
     void * w = nullptr;
     RGPU_CUDA(cudaGetSymbolAddress(&s, g_scratch));
     RGPU_CUDA(cudaGetSymbolAddress(&w, g_status));
     p.status = static_cast<int *>(w);
     p.scratch = static_cast<unsigned char *>(s);
-  }
-  return p;
+  });
 }
 
 __global__ void sum_parts_kernel(const float * __restrict__ parts, int n_parts, int64_t M, float * __restrict__ e) {
@@ -72,28 +65,34 @@ void gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const float * A, cons
   if (M <= 0 || N <= 0 || K <= 0 || !A || !B || !alpha || !e)
     throw Error(RGPU_ERR_INVALID_ARGUMENT, "bad arguments: sizes must be positive and pointers non-null");
   if (zeta < 1) throw Error(RGPU_ERR_INVALID_ARGUMENT, "zeta must be >= 1");
-  const int64_t Kp = (K + 63) / 64 * 64, Np = (N + 31) / 32 * 32;
+  auto too_big = [&](const std::string & why) {
+    return Error(RGPU_ERR_CAPACITY, "GAP energies without allocation: M=" + std::to_string(M) + ", N=" +
+                                        std::to_string(N) + ", K=" + std::to_string(K) + " " + why +
+                                        ", above the static " + std::to_string(kScratchBytes) +
+                                        " bytes of scratch");
+  };
+  // Each of M, N and K alone bounds a scratch term from below (4 M Kp, 4 N Kp
+  // and 4 M bytes), so one beyond the array's size is rejected before any
+  // product is formed; the products below then stay far inside 64 bits.
+  if (M > int64_t(kScratchBytes) || N > int64_t(kScratchBytes) || K > int64_t(kScratchBytes))
+    throw too_big("exceed the scratch on their own");
+  const int64_t Kp = (K + 63) / 64 * 64;
   const int n_parts = int((N + kTcTileN - 1) / kTcTileN);
-  // scratch layout: A hi, A lo, B hi, B lo, W hi, W lo, energy partials
+  // scratch layout: A hi, A lo, B hi, B lo, energy partials (the epilogue
+  // runs in its energies-only form, so W needs no space)
   const size_t a_bytes = align256(size_t(M) * Kp * 2), b_bytes = align256(size_t(N) * Kp * 2);
-  const size_t w_bytes = align256(size_t(M) * Np * 2), p_bytes = align256(size_t(n_parts) * M * 4);
-  const size_t need = 2 * a_bytes + 2 * b_bytes + 2 * w_bytes + p_bytes;
-  if (need > kScratchBytes)
-    throw Error(RGPU_ERR_CAPACITY, "GAP energies without allocation: M=" + std::to_string(M) +
-                                       ", N=" + std::to_string(N) + ", K=" + std::to_string(K) + " need " +
-                                       std::to_string(need) + " bytes of scratch, above the static " +
-                                       std::to_string(kScratchBytes) + " bytes");
+  const size_t p_bytes = align256(size_t(n_parts) * M * 4);
+  const size_t need = 2 * a_bytes + 2 * b_bytes + p_bytes;
+  if (need > kScratchBytes) throw too_big("need " + std::to_string(need) + " bytes");
   const DevicePointers p = setup_current_device();
   unsigned char * s = p.scratch;
   __nv_bfloat16 * ah = reinterpret_cast<__nv_bfloat16 *>(s);
   __nv_bfloat16 * al = reinterpret_cast<__nv_bfloat16 *>(s + a_bytes);
   __nv_bfloat16 * bh = reinterpret_cast<__nv_bfloat16 *>(s + 2 * a_bytes);
   __nv_bfloat16 * bl = reinterpret_cast<__nv_bfloat16 *>(s + 2 * a_bytes + b_bytes);
-  __nv_bfloat16 * wh = reinterpret_cast<__nv_bfloat16 *>(s + 2 * a_bytes + 2 * b_bytes);
-  __nv_bfloat16 * wl = reinterpret_cast<__nv_bfloat16 *>(s + 2 * a_bytes + 2 * b_bytes + w_bytes);
-  float * parts = reinterpret_cast<float *>(s + 2 * a_bytes + 2 * b_bytes + 2 * w_bytes);
+  float * parts = reinterpret_cast<float *>(s + 2 * a_bytes + 2 * b_bytes);
   // Only the status word must start at zero: the splits write every padded
-  // column, the epilogue every partial and W column that is read.
+  // column and the epilogue every partial that is read.
   RGPU_CUDA(cudaMemsetAsync(p.status, 0, 2 * sizeof(int), st));
   split_bf16(A, M, K, K, ah, al, Kp, st);
   split_bf16(B, N, K, K, bh, bl, Kp, st);
@@ -108,9 +107,9 @@ void gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const float * A, cons
   g.B_lo = bl;
   g.ldb = Kp;
   g.epilogue = 1;
-  g.W_hi = wh;
-  g.W_lo = wl;
-  g.ldw = Np;
+  g.W_hi = nullptr;  // energies only
+  g.W_lo = nullptr;
+  g.ldw = 0;
   g.alpha = alpha;
   g.zeta = zeta;
   g.e_part = parts;

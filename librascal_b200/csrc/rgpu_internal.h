@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/rascal_b200.h"
+#include "per_device.h"
 
 namespace rgpu {
 
@@ -29,6 +30,9 @@ struct Error : std::runtime_error {
 
 void cuda_check(cudaError_t e, const char * what);
 #define RGPU_CUDA(x) ::rgpu::cuda_check((x), #x)
+// Ordinal of the current CUDA device, checked against kMaxDevices (Error
+// RGPU_ERR_CUDA outside it).
+int current_device();
 // Counts launches of this library's kernels (reported by the bench).
 void count_launch(int n = 1);
 #define RGPU_LAUNCHED() ::rgpu::count_launch(1)
@@ -312,13 +316,20 @@ void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st);
 void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st);
 // 0 when no bounded wait of the tcgen05 GEMM gave up, else where it did.
 int gemm_tc_timeout(bool reset);
+// Polls of the tcgen05 GEMMs' MMA-warp operand waits (negative: the
+// default); a test hook that makes those waits run out.
+void set_gemm_wait_limit(long long polls);
 // gemm_bf16x3 reporting a bounded wait that gave up into the caller's device
 // word pair status_dev[0..1] (timeout flag, stage; zero on entry) instead of
-// the process-wide status word. Allocates nothing.
+// the per-device status word. Allocates nothing. With epilogue 1 and
+// W_hi == nullptr only the energy partials are written.
 void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st);
 // Allocation-free GAP energies e[r] = sum_n alpha_n (A_r . B_n)^zeta (noalloc.cu).
 void gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const float * A, const float * B,
                           const float * alpha, int zeta, float * e, cudaStream_t st);
+// Measured FMA throughput (TFLOP/s) of the current device's FP32 or FP64
+// pipe (peaks.cu).
+double measure_fma_peak(int precision);
 // hi/lo BF16 split of a row-major FP32 matrix (columns >= cols become 0).
 void split_bf16(const float * x, int64_t rows, int64_t cols, int64_t ldx, __nv_bfloat16 * hi,
                 __nv_bfloat16 * lo, int64_t ldo, cudaStream_t st);
@@ -404,5 +415,11 @@ void launch_species_sort(int64_t n, const int32_t * types, const int32_t * cente
 void launch_round_tf32(float * x, int64_t n, cudaStream_t st);
 void launch_fill_f64(double * p, int64_t n, double v, cudaStream_t st);
 void launch_fill_f32(float * p, int64_t n, float v, cudaStream_t st);
+// out = a + b; out = a x (n doubles, device)
+void launch_add_f64(const double * a, const double * b, double * out, int64_t n, cudaStream_t st);
+void launch_scale_f64(const double * x, double a, double * out, int64_t n, cudaStream_t st);
+// x[r][c] *= scale[group[r]] for a row-major rows x cols FP32 matrix
+void launch_scale_rows_by_group(float * x, int64_t rows, int64_t cols, const int32_t * group,
+                                const double * scale, cudaStream_t st);
 
 }  // namespace rgpu

@@ -24,6 +24,15 @@ void cuda_check(cudaError_t e, const char * what) {
   }
 }
 
+int current_device() {
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices)
+    throw Error(RGPU_ERR_CUDA, "device ordinal " + std::to_string(dev) + " beyond the library's table of " +
+                                   std::to_string(kMaxDevices) + " devices");
+  return dev;
+}
+
 void DevBuf::ensure(size_t bytes) {
   if (bytes <= cap && p) return;
   release();
@@ -259,6 +268,41 @@ void launch_fill_f64(double * p, int64_t n, double v, cudaStream_t st) {
 void launch_fill_f32(float * p, int64_t n, float v, cudaStream_t st) {
   if (n <= 0) return;
   fill_f32_kernel<<<div_up(n, 256), 256, 0, st>>>(p, n, v);
+  RGPU_LAUNCHED();
+}
+
+namespace {
+__global__ void add_f64_kernel(const double * __restrict__ a, const double * __restrict__ b,
+                               double * __restrict__ out, int64_t n) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a[i] + b[i];
+}
+__global__ void scale_f64_kernel(const double * __restrict__ x, double a, double * __restrict__ out, int64_t n) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a * x[i];
+}
+__global__ void scale_rows_by_group_kernel(float * __restrict__ x, int64_t rows, int64_t cols,
+                                           const int32_t * __restrict__ group, const double * __restrict__ scale) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= rows * cols) return;
+  x[i] *= float(scale[group[i / cols]]);
+}
+}  // namespace
+
+void launch_add_f64(const double * a, const double * b, double * out, int64_t n, cudaStream_t st) {
+  if (n <= 0) return;
+  add_f64_kernel<<<div_up(n, 256), 256, 0, st>>>(a, b, out, n);
+  RGPU_LAUNCHED();
+}
+void launch_scale_f64(const double * x, double a, double * out, int64_t n, cudaStream_t st) {
+  if (n <= 0) return;
+  scale_f64_kernel<<<div_up(n, 256), 256, 0, st>>>(x, a, out, n);
+  RGPU_LAUNCHED();
+}
+void launch_scale_rows_by_group(float * x, int64_t rows, int64_t cols, const int32_t * group,
+                                const double * scale, cudaStream_t st) {
+  if (rows * cols <= 0) return;
+  scale_rows_by_group_kernel<<<div_up(rows * cols, 256), 256, 0, st>>>(x, rows, cols, group, scale);
   RGPU_LAUNCHED();
 }
 

@@ -480,8 +480,17 @@ def train_gap_model(kernel, frames, KNM_, X_sparse, y_train, self_contributions,
 
 
 def gap_energy(positions, model, structures):
-    """Energies of `structures` at `positions` (torch tensor, N x 3) through
-    the adjoint path; differentiable w.r.t. positions."""
+    """Energies of `structures` at `positions` (torch tensor, n_atoms x 3,
+    FP64, on a CUDA device or the host) through the FP32 adjoint path,
+    differentiable with respect to the positions.
+
+    The forward computes the energies only and leaves the neighbour list,
+    the features and W = alpha zeta k^(zeta-1) on the device; the backward
+    runs the second GEMM, the power-spectrum backward and the pair adjoint
+    (rgpu_gap_forward_dev / rgpu_gap_backward_dev), so
+    torch.autograd.grad(E.sum(), positions) gives -forces, the reference's
+    KRR.predict_forces (bindings/rascal/models/krr.py:123-166). CUDA
+    positions and gradients stay on the device."""
     return _gap_function().apply(positions, model, structures)
 
 
@@ -493,25 +502,50 @@ def _gap_function():
     if _GAPFn is None:
         import torch
 
+        def _order(structures):
+            """The library's stream for these structures, and a helper that
+            makes one stream wait for work enqueued on another."""
+            ext = torch.cuda.ExternalStream(structures.stream())
+
+            def after(waiter, producer):
+                ev = torch.cuda.Event()
+                ev.record(producer)
+                waiter.wait_event(ev)
+            return ext, after
+
         class GAPEnergy(torch.autograd.Function):
             """E(r) forward; dE/dr from the adjoint kernels (no stored dX/dr)."""
 
             @staticmethod
             def forward(ctx, positions, model, structures):
-                pos = positions.detach().to("cpu", torch.float64).numpy()
-                structures.update_positions(pos)
-                E, F = model.predict(structures, "fp32")
-                b = structures.batch
-                sidx = np.repeat(np.arange(structures.n_structures), np.diff(b["atom_offsets"]))
-                ctx.save_for_backward(torch.from_numpy(F).to(positions.device),
-                                      torch.from_numpy(sidx).to(positions.device))
-                return torch.from_numpy(E).to(positions.device, positions.dtype)
+                dev = positions.device if positions.is_cuda else torch.device("cuda", torch.cuda.current_device())
+                pos = positions.detach().to(dev, torch.float64).contiguous()
+                if pos.shape != (structures.n_atoms, 3):
+                    raise ValueError("positions must be n_atoms x 3")
+                E = torch.empty(structures.n_structures, dtype=torch.float64, device=dev)
+                ext, after = _order(structures)
+                after(ext, torch.cuda.current_stream(dev))  # positions are ready
+                N.check(N.lib().rgpu_gap_forward_dev(model.handle, structures.handle, pos.data_ptr(),
+                                                     E.data_ptr()))
+                after(torch.cuda.current_stream(dev), ext)
+                ctx.model = model
+                ctx.structures = structures
+                ctx.in_device = positions.device
+                ctx.in_dtype = positions.dtype
+                return E.to(positions.device, positions.dtype)
 
             @staticmethod
             def backward(ctx, gE):
-                F, sidx = ctx.saved_tensors
-                g = -(F * gE.to(F.dtype)[sidx][:, None])
-                return g, None, None
+                structures = ctx.structures
+                dev = torch.device("cuda", torch.cuda.current_device()) if not gE.is_cuda else gE.device
+                g = gE.detach().to(dev, torch.float64).contiguous()
+                out = torch.empty((structures.n_atoms, 3), dtype=torch.float64, device=dev)
+                ext, after = _order(structures)
+                after(ext, torch.cuda.current_stream(dev))
+                N.check(N.lib().rgpu_gap_backward_dev(ctx.model.handle, structures.handle, g.data_ptr(),
+                                                      out.data_ptr()))
+                after(torch.cuda.current_stream(dev), ext)
+                return out.to(ctx.in_device, ctx.in_dtype), None, None
 
         _GAPFn = GAPEnergy
     return _GAPFn

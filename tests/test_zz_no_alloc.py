@@ -71,6 +71,27 @@ def test_noalloc_reuses_scratch_across_shapes():
     assert np.abs(small - ref).max() <= 1e-6 * np.abs(ref).max()
 
 
+def test_noalloc_fits_problems_whose_w_output_would_not():
+    """The energies-only epilogue writes no W, so a problem whose BF16 W
+    (4 M Np bytes, 12 MB here) would overflow the 16 MiB array still runs."""
+    M, N, K = 2000, 1500, 448
+    A, B, alpha = _inputs(M, N, K, 5)
+    ref = _energies(A, B, alpha, 2, noalloc=False)
+    for _ in range(2):
+        e = _energies(A, B, alpha, 2, noalloc=True)
+        assert np.abs(e - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("M,N,K", [(1 << 62, 4, 8), (4, 1 << 62, 8), (4, 4, 1 << 62), (1 << 40, 1 << 30, 64)])
+def test_noalloc_rejects_sizes_whose_products_overflow(M, N, K):
+    """Sizes whose scratch products would wrap around 64 bits are rejected
+    with the capacity error before any pointer is touched."""
+    from librascal_b200 import _native as N_
+    rc = N_.lib().rgpu_gap_energies_noalloc(M, N, K, 16, 16, 16, 2, 16, None)
+    assert rc == N_.ERR_CAPACITY
+    assert "scratch" in N_.lib().rgpu_last_error().decode()
+
+
 def test_noalloc_rejects_sizes_beyond_scratch():
     from librascal_b200 import _native as N
     # 4 * M * Kp alone is 64 MiB here, above the 16 MiB of static scratch;
