@@ -355,7 +355,9 @@ void launch_force_contract_fp64(const FeatureDims & fd, int64_t c0, int64_t c1, 
   RGPU_CUDA(cudaStreamSynchronize(st));
   const int64_t np = p_last - p_first;
   if (np <= 0) return;
-  static thread_local DevBuf pc;
+  // per host thread and per device: another device's buffer is not memory this launch may use
+  static thread_local PerDevice<DevBuf> pc_tab;
+  DevBuf & pc = pc_tab.at(current_device());
   pc.ensure(sizeof(int64_t) * np);
   pair_center2_kernel<<<div_up(c1 - c0, 8), 256, 0, st>>>(c0, c1, pair_off, p_first, pc.as<int64_t>());
   RGPU_LAUNCHED();

@@ -263,7 +263,9 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
   const int64_t np = p_last - p_first;
   if (np <= 0) return;
   // map each pair of the chunk back to its centre (stored just after dX)
-  static thread_local DevBuf pc;
+  // per host thread and per device: another device's buffer is not memory this launch may use
+  static thread_local PerDevice<DevBuf> pc_tab;
+  DevBuf & pc = pc_tab.at(current_device());
   pc.ensure(sizeof(int64_t) * np);
   pair_center_kernel<<<div_up(c1 - c0, 8), 256, 0, st>>>(c0, c1, e.pair_off, p_first, pc.as<int64_t>());
   RGPU_LAUNCHED();

@@ -87,6 +87,9 @@ def test_device_state_uses_per_device_tables():
         text = open(os.path.join(CSRC, name)).read()
         for m in re.finditer(r"static\s+(bool|int|\w+\s*\*)\s+\w+\s*=\s*(false|nullptr|0)\s*;", text):
             offenders.append("%s: %s" % (name, m.group(0)))
+        # device buffers kept across calls belong to a device
+        for m in re.finditer(r"static\s+(thread_local\s+)?DevBuf\b[^;]*;", text):
+            offenders.append("%s: %s" % (name, m.group(0)))
     assert not offenders, offenders
     common = open(os.path.join(CSRC, "common.cuh")).read()
     assert "PerDevice<char> g_sph_filled" in common
