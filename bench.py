@@ -637,6 +637,7 @@ def run_gap(args):
         step_resident()
     barrier()
     l0 = lib.rgpu_kernel_launches(0)
+    g0 = st.graph_info()
     with Clocks(dev) as clk:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -646,16 +647,51 @@ def run_gap(args):
         e1.record(ext)
         e1.synchronize()
     barrier()
-    launches = int(lib.rgpu_kernel_launches(0) - l0)
+    g1 = st.graph_info()
+    # kernels replayed from a recorded graph do not pass the library's launch
+    # counter: count the graph's kernel nodes per replay
+    launches = int(lib.rgpu_kernel_launches(0) - l0) + (g1[1] - g0[1]) * g1[3]
     ms = max_over_ranks(e0.elapsed_time(e1)) / args.steps
     value = n_atoms * world / (ms * 1e-3)
 
-    # ---- stage breakdown (untimed extra passes)
+    # ---- the same steps without the recorded graphs (the ordinary path,
+    # which sizes its buffers through host synchronisations), and the stage
+    # breakdown, which only the ordinary path records
+    st.use_graphs(False)
+    ms_ordinary = timed(step_resident, max(args.steps // 2, 3), 1)
     stages = np.zeros(8)
     for _ in range(3):
         step_resident()
         stages += st.stage_times()
     stages /= 3
+    st.use_graphs(True)
+    # a small batch of the same workload (launch- and synchronisation-bound),
+    # recorded against ordinary
+    small = None
+    if spec["shardable"]:
+        sb = _first(batch, 100)
+        ss = rb.StructureSet(sb)
+        ext_s = torch.cuda.ExternalStream(ss.stream())
+
+        def step_small():
+            ss.invalidate()
+            model.predict(ss, args.precision, energies=False, forces=False)
+
+        small = dict(n_structures=int(len(sb["atom_offsets"]) - 1), n_atoms=int(sb["atom_offsets"][-1]))
+        for g in (True, False):
+            ss.use_graphs(g)
+            for _ in range(3):
+                step_small()
+            torch.cuda.synchronize()
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(ext_s)
+            for _ in range(20):
+                step_small()
+            a1.record(ext_s)
+            a1.synchronize()
+            small["ms_per_step_graph" if g else "ms_per_step_ordinary"] = a0.elapsed_time(a1) / 20
+        del ss
     import ctypes
     nc_, np_ = ctypes.c_int64(), ctypes.c_int64()
     N.check(lib.rgpu_neighbour_list_size(st.handle, ctypes.byref(nc_), ctypes.byref(np_)))
@@ -746,6 +782,10 @@ def run_gap(args):
                         stage_ms=dict(zip(["total", "neighbour_list", "expansion", "power_spectrum",
                                            "gemm_fwd", "gemm_bwd", "ps_backward", "pair_adjoint"],
                                           [round(float(x), 4) for x in stages]))),
+            graphs=dict(ms_per_step_ordinary_path=ms_ordinary, buckets=g1[0], replays_timed=g1[1] - g0[1],
+                        kernels_per_replay=g1[3], small_batch=small,
+                        note="value is timed with the recorded CUDA graph of this size bucket; the ordinary "
+                             "path runs the same kernels with host synchronisations that size its buffers"),
             plain_fp64_ms_per_step=plain["ms"] if plain else None,
             plain_fp64_atoms_per_s=(n_atoms * world / (plain["ms"] * 1e-3)) if plain else None,
             plain_fp64_stage_ms=plain["stage_ms"] if plain else None,

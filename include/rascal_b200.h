@@ -321,6 +321,27 @@ int64_t rgpu_kernel_launches(int reset);
  * gradient chunks (materialised dX/dr and the gathered GEMMs). */
 rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out,
                              int32_t n_stages);
+/* FP32 predictions as recorded CUDA graphs. With graphs on (the default),
+ * rgpu_gap_predict and rgpu_gap_predict_stress at RGPU_PRECISION_FP32 record
+ * the whole call (neighbour list, features, GEMMs, backward, adjoint, output
+ * copies) as a CUDA graph per size bucket: the model, whether outputs and
+ * the stress are asked for, the numbers of structures and atoms, the species
+ * layout and the centres per species, and the addresses of the device
+ * buffers involved. The first call of a bucket runs the ordinary path
+ * (which sizes buffers through a few host synchronisations) and records the
+ * bucket with the neighbour list built to capacities 12.5 % above its
+ * counts; later calls of the bucket replay the graph with one
+ * synchronisation. A replay whose list outgrows the capacities, or whose
+ * input is invalid, is redone by the ordinary path (which reports input
+ * errors with the reference's messages) and the bucket is recorded again.
+ * A handle keeps at most four buckets (least recently used dropped). A
+ * replayed call records no stage times (rgpu_stage_times keeps those of the
+ * last ordinary call). The reference has no counterpart: it prepares each
+ * manager on the host (structure_manager_collection.hh:178-184). */
+rgpu_status rgpu_structures_use_graphs(rgpu_structures * s, int enable);
+/* info[0] = recorded buckets held, info[1] = replays, info[2] = recordings,
+ * info[3] = kernels launched by the last replayed graph. */
+rgpu_status rgpu_structures_graph_info(const rgpu_structures * s, int64_t * info /* [4] */);
 /* Measured FMA throughput of the current device's CUDA cores in TFLOP/s,
  * FP32 (RGPU_PRECISION_FP32) or FP64 (RGPU_PRECISION_FP64) pipe: every SM
  * filled with independent FMA chains, best of five launches timed with CUDA

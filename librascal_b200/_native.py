@@ -76,6 +76,8 @@ SIGNATURES = {
     "rgpu_kernel_launches": (ctypes.c_int64, [ctypes.c_int]),
     "rgpu_stage_times": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p, ctypes.c_int32]),
     "rgpu_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, c_dbl_p]),
+    "rgpu_structures_use_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rgpu_structures_graph_info": (ctypes.c_int, [ctypes.c_void_p, c_i64_p]),
     "rgpu_debug_gemm_bf16x3": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

@@ -158,6 +158,27 @@ struct rgpu_calculator {
 
 struct GapLayout;
 
+// One FP32 prediction (rgpu_gap_predict / rgpu_gap_predict_stress) recorded
+// as a CUDA graph for one size bucket: the same model, output kind, numbers
+// of structures and atoms, species layout and centres per species, and the
+// same device buffers; the neighbour list inside is built to capacities
+// 12.5 % above the counts of the recording call.
+struct PredictGraph {
+  cudaGraph_t graph{nullptr};
+  cudaGraphExec_t exec{nullptr};
+  const rgpu_gap_model * model{nullptr};
+  bool stress{false}, outputs{false};
+  int n_struct{0};
+  int64_t n_atoms{0};
+  std::vector<int> species;
+  std::vector<int64_t> species_count;
+  NlCaps caps{};
+  std::vector<const void *> buffers;
+  double * out_h{nullptr};  // pinned: energies, forces, stress sums of a replay
+  int64_t kernels{0};
+  uint64_t used{0};
+};
+
 struct rgpu_structures {
   int device{-1};  // device current at creation: owns the stream and every buffer
   cudaStream_t st{nullptr};
@@ -214,6 +235,11 @@ struct rgpu_structures {
   double * md_pos_h{nullptr};  // pinned: positions in, outputs out
   double * md_out_h{nullptr};
   size_t md_pos_cap{0}, md_out_cap{0};
+  // FP32 predictions recorded as CUDA graphs, a few size buckets per handle
+  std::vector<PredictGraph> pgraphs;
+  bool use_graphs{true};
+  uint64_t pgraph_clock{0};
+  int64_t pgraph_replays{0}, pgraph_records{0}, pgraph_last_kernels{0};
   // autograd: the model whose forward (rgpu_gap_forward_dev) left W, the
   // features and the list in place for rgpu_gap_backward_dev (null: none)
   const rgpu_gap_model * fwd_model{nullptr};
@@ -1441,12 +1467,17 @@ static void md_drop(rgpu_structures * s) {
   s->md_model = nullptr;
 }
 
-// The step's work on the structures' stream, positions from s->md_pos_h.
-static void md_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress) {
+// The FP32 prediction on the structures' stream with no host
+// synchronisation, so that it can be recorded: positions from pinned
+// pos_h (null: those already on the device), the neighbour list to `caps`,
+// outputs (energies, forces, stress sums) into pinned out_h (null: left on
+// the device), and the status word copied to the host at the end.
+static void graph_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress, const double * pos_h,
+                          double * out_h, const NlCaps & caps) {
   rgpu_calculator * c = m->calc;
   cudaStream_t st = s->st;
   const int64_t na = s->n_atoms;
-  RGPU_CUDA(cudaMemcpyAsync(s->pos_d.p, s->md_pos_h, sizeof(double) * 3 * na, cudaMemcpyHostToDevice, st));
+  if (pos_h) RGPU_CUDA(cudaMemcpyAsync(s->pos_d.p, pos_h, sizeof(double) * 3 * na, cudaMemcpyHostToDevice, st));
   NlInputs in;
   in.n_struct = s->n_struct;
   in.n_atoms = na;
@@ -1460,7 +1491,7 @@ static void md_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress) {
   in.center_off = s->center_off_d.as<int64_t>();
   in.atom_struct = s->atom_struct_d.as<int32_t>();
   in.n_centers_total = s->center_off_h[s->n_struct];
-  build_neighbour_list(in, c->hy.cutoff, s->nlw, s->nl, s->status_d, s->status_h, st, &s->md_caps);
+  build_neighbour_list(in, c->hy.cutoff, s->nlw, s->nl, s->status_d, s->status_h, st, &caps);
   // features (the FP32 branch of compute_features, layout unchanged)
   sort_rows(s);
   const int64_t nc = s->nl.n_centers;
@@ -1478,13 +1509,34 @@ static void md_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress) {
   RGPU_CUDA(cudaMemsetAsync(s->F_d.p, 0, sizeof(double) * 3 * na, st));
   if (stress) RGPU_CUDA(cudaMemsetAsync(s->S_d.p, 0, sizeof(double) * 6 * s->n_struct, st));
   gap_fast(m, s, s->E_d.as<double>(), s->F_d.as<double>(), true, stress ? s->S_d.as<double>() : nullptr);
-  double * out = s->md_out_h;
-  RGPU_CUDA(cudaMemcpyAsync(out, s->E_d.p, sizeof(double) * s->n_struct, cudaMemcpyDeviceToHost, st));
-  RGPU_CUDA(cudaMemcpyAsync(out + s->n_struct, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, st));
-  if (stress)
-    RGPU_CUDA(cudaMemcpyAsync(out + s->n_struct + 3 * na, s->S_d.p, sizeof(double) * 6 * s->n_struct,
-                              cudaMemcpyDeviceToHost, st));
+  if (double * out = out_h) {
+    RGPU_CUDA(cudaMemcpyAsync(out, s->E_d.p, sizeof(double) * s->n_struct, cudaMemcpyDeviceToHost, st));
+    RGPU_CUDA(cudaMemcpyAsync(out + s->n_struct, s->F_d.p, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, st));
+    if (stress)
+      RGPU_CUDA(cudaMemcpyAsync(out + s->n_struct + 3 * na, s->S_d.p, sizeof(double) * 6 * s->n_struct,
+                                cudaMemcpyDeviceToHost, st));
+  }
   RGPU_CUDA(cudaMemcpyAsync(s->status_h, s->status_d, sizeof(DevStatus), cudaMemcpyDeviceToHost, st));
+}
+
+// The step's work on the structures' stream, positions from s->md_pos_h.
+static void md_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress) {
+  graph_enqueue(m, s, stress, s->md_pos_h, s->md_out_h, s->md_caps);
+}
+
+// Kernel nodes of a recorded graph (the kernels one replay launches).
+static int64_t graph_kernels(cudaGraph_t g) {
+  size_t n = 0;
+  int64_t k = 0;
+  if (cudaGraphGetNodes(g, nullptr, &n) == cudaSuccess && n > 0) {
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) == cudaSuccess)
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++k;
+      }
+  }
+  return k;
 }
 
 // Energy baseline and cell volume, as in gap_predict_impl.
@@ -1615,23 +1667,179 @@ static void md_step_impl(rgpu_gap_model * m, rgpu_structures * s, const double *
   s->md_stress = stress;
   s->md_buffers = md_buffers(m, s);
   s->md_species = s->species;
-  {
-    size_t n = 0;
-    s->md_kernels = 0;
-    if (cudaGraphGetNodes(s->md_graph, nullptr, &n) == cudaSuccess && n > 0) {
-      std::vector<cudaGraphNode_t> nodes(n);
-      if (cudaGraphGetNodes(s->md_graph, nodes.data(), &n) == cudaSuccess)
-        for (cudaGraphNode_t nd : nodes) {
-          cudaGraphNodeType t;
-          if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++s->md_kernels;
-        }
-    }
-  }
+  s->md_kernels = graph_kernels(s->md_graph);
   s->md_replays = 0;
   // the ordinary step above already produced this call's results; the
   // positions of the next step arrive in md_pos_h
   s->nl_valid = false;
   s->feat_valid = false;
+}
+
+// ------------------------------------------------- predictions as CUDA graphs
+static void pgraph_release(PredictGraph & g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  if (g.out_h) cudaFreeHost(g.out_h);
+  g = PredictGraph{};
+}
+
+static std::vector<int64_t> centres_per_species(const rgpu_structures * s) {
+  std::vector<int64_t> c(s->species.size());
+  for (size_t i = 0; i < s->species.size(); ++i) c[i] = s->centres_of_type[s->species[i]];
+  return c;
+}
+
+// Outputs of a replay, from its pinned copy: baseline added to the
+// energies, stress sums divided by the cell volumes (as gap_predict_impl).
+static void pgraph_outputs(const rgpu_gap_model * m, const rgpu_structures * s, const PredictGraph & g,
+                           double * energies, double * forces, double * neg_stress) {
+  const int64_t na = s->n_atoms;
+  const double * out = g.out_h;
+  if (energies) {
+    const std::vector<double> y0 = structure_baselines(m, s);
+    for (int k = 0; k < s->n_struct; ++k) energies[k] = out[k] + y0[k];
+  }
+  if (forces) std::memcpy(forces, out + s->n_struct, sizeof(double) * 3 * na);
+  if (neg_stress)
+    for (int k = 0; k < s->n_struct; ++k) {
+      const double v = cell_volume(&s->cells_h[9 * size_t(k)]);
+      for (int j = 0; j < 6; ++j) neg_stress[6 * k + j] = out[s->n_struct + 3 * na + 6 * k + j] / v;
+    }
+}
+
+// Replays the recorded graph of this call's size bucket, if there is one:
+// true when it produced the call's results. A replay whose neighbour list
+// outgrew its capacities, or whose input is invalid, drops the recording and
+// leaves the call to the ordinary path (which reports input errors with the
+// reference's messages).
+static bool pgraph_replay(rgpu_gap_model * m, rgpu_structures * s, bool stress, double * energies,
+                          double * forces, double * neg_stress) {
+  if (s->pgraphs.empty()) return false;
+  calculator_to_device(m->calc);
+  set_layout(s, m->calc->hy, m->species);
+  model_layout(m, s, true);
+  const bool outputs = energies || forces || neg_stress;
+  const std::vector<int64_t> cnt = centres_per_species(s);
+  std::vector<const void *> bufs;
+  for (PredictGraph & g : s->pgraphs) {
+    if (g.model != m || g.stress != stress || g.outputs != outputs || g.n_struct != s->n_struct ||
+        g.n_atoms != s->n_atoms || g.species != s->species || g.species_count != cnt)
+      continue;
+    if (bufs.empty()) bufs = md_buffers(m, s);
+    if (g.buffers != bufs) continue;
+    s->timed = false;
+    RGPU_CUDA(cudaGraphLaunch(g.exec, s->st));
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    // the list on the device is the capacity-bound one: nothing computed here
+    // is reused by a later call
+    s->nl_valid = false;
+    s->feat_valid = false;
+    s->fwd_model = nullptr;
+    const int where = gemm_tc_timeout(true);
+    if (where)
+      throw Error(RGPU_ERR_TIMEOUT, "tensor-core GEMM: a bounded pipeline wait gave up (stage " +
+                                        std::to_string(where) + ")");
+    if (s->status_h->code != 0) {
+      RGPU_CUDA(cudaMemsetAsync(s->status_d, 0, sizeof(DevStatus), s->st));
+      RGPU_CUDA(cudaStreamSynchronize(s->st));
+      s->status_h->code = 0;
+      pgraph_release(g);
+      s->pgraphs.erase(s->pgraphs.begin() + (&g - s->pgraphs.data()));
+      return false;
+    }
+    g.used = ++s->pgraph_clock;
+    ++s->pgraph_replays;
+    s->pgraph_last_kernels = g.kernels;
+    pgraph_outputs(m, s, g, energies, forces, neg_stress);
+    return true;
+  }
+  return false;
+}
+
+// Records this call's size bucket after an ordinary FP32 prediction: one run
+// to the new capacities without recording (it sizes every buffer, since
+// nothing may be allocated while recording, and checks that the call fits
+// them), then the recording. A failure leaves the handle on the ordinary
+// path for this bucket.
+static void pgraph_record(rgpu_gap_model * m, rgpu_structures * s, bool stress, bool outputs) {
+  constexpr size_t kMaxGraphs = 4;
+  PredictGraph g;
+  int64_t sites = 0, boxes = 0;
+  neighbour_list_counts(s->nlw, sites, boxes);
+  g.caps.sites = sites + sites / 8 + 64;
+  g.caps.boxes = boxes + boxes / 8 + 64;
+  g.caps.pairs = s->nl.n_pairs + s->nl.n_pairs / 8 + 256;
+  g.model = m;
+  g.stress = stress;
+  g.outputs = outputs;
+  g.n_struct = s->n_struct;
+  g.n_atoms = s->n_atoms;
+  g.species = s->species;
+  g.species_count = centres_per_species(s);
+  if (outputs) {
+    const size_t nout = size_t(s->n_struct) * 7 + 3 * size_t(s->n_atoms) + 1;
+    RGPU_CUDA(cudaMallocHost(&g.out_h, sizeof(double) * nout));
+  }
+  if (stress) s->S_d.ensure(sizeof(double) * 6 * (s->n_struct + 1));
+  s->timed = false;
+  bool ok = true;
+  try {
+    graph_enqueue(m, s, stress, nullptr, g.out_h, g.caps);
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    ok = s->status_h->code == 0 && gemm_tc_timeout(true) == 0;
+  } catch (...) {
+    ok = false;
+  }
+  if (ok) {
+    ok = cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      try {
+        graph_enqueue(m, s, stress, nullptr, g.out_h, g.caps);
+      } catch (...) {
+        ok = false;
+      }
+      cudaGraph_t gr = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(s->st, &gr);
+      ok = ok && e == cudaSuccess && gr != nullptr;
+      if (gr) g.graph = gr;
+      ok = ok && cudaGraphInstantiate(&g.exec, g.graph, 0) == cudaSuccess;
+    }
+  }
+  s->nl_valid = false;
+  s->feat_valid = false;
+  s->fwd_model = nullptr;
+  if (!ok) {
+    (void)cudaGetLastError();
+    RGPU_CUDA(cudaMemsetAsync(s->status_d, 0, sizeof(DevStatus), s->st));
+    RGPU_CUDA(cudaStreamSynchronize(s->st));
+    s->status_h->code = 0;
+    pgraph_release(g);
+    return;
+  }
+  g.buffers = md_buffers(m, s);
+  g.kernels = graph_kernels(g.graph);
+  g.used = ++s->pgraph_clock;
+  if (s->pgraphs.size() >= kMaxGraphs) {
+    auto lru = std::min_element(s->pgraphs.begin(), s->pgraphs.end(),
+                                [](const PredictGraph & a, const PredictGraph & b) { return a.used < b.used; });
+    pgraph_release(*lru);
+    s->pgraphs.erase(lru);
+  }
+  s->pgraphs.push_back(g);
+  ++s->pgraph_records;
+}
+
+// rgpu_gap_predict(_stress): FP32 calls go through the recorded graph of
+// their size bucket when one exists, otherwise through the ordinary path,
+// after which the bucket is recorded.
+static void gap_predict_entry(rgpu_gap_model * m, rgpu_structures * s, int precision, double * energies,
+                              double * forces, double * neg_stress) {
+  if (!m || !s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+  const bool graphs = precision == RGPU_PRECISION_FP32 && s->use_graphs && !s->has_mask;
+  const bool stress = neg_stress != nullptr;
+  if (graphs && pgraph_replay(m, s, stress, energies, forces, neg_stress)) return;
+  gap_predict_impl(m, s, precision, energies, forces, neg_stress);
+  if (graphs) pgraph_record(m, s, stress, energies || forces || neg_stress);
 }
 
 // ===================================================================== C ABI
@@ -1745,6 +1953,7 @@ rgpu_status rgpu_structures_destroy(rgpu_structures * s) {
     if (s->st) cudaStreamSynchronize(s->st);
     if (s->md_exec) cudaGraphExecDestroy(s->md_exec);
     if (s->md_graph) cudaGraphDestroy(s->md_graph);
+    for (PredictGraph & g : s->pgraphs) pgraph_release(g);
     if (s->md_pos_h) cudaFreeHost(s->md_pos_h);
     if (s->md_out_h) cudaFreeHost(s->md_out_h);
     if (s->pinned) cudaFreeHost(s->pinned);
@@ -2094,7 +2303,7 @@ rgpu_status rgpu_gap_predict(rgpu_gap_model * m, rgpu_structures * s, int precis
                              double * forces) {
   return guard([&] {
     OnDevice on_dev(s);
-    gap_predict_impl(m, s, precision, energies, forces, nullptr);
+    gap_predict_entry(m, s, precision, energies, forces, nullptr);
   });
 }
 
@@ -2103,7 +2312,7 @@ rgpu_status rgpu_gap_predict_stress(rgpu_gap_model * m, rgpu_structures * s, int
   return guard([&] {
     OnDevice on_dev(s);
     if (!neg_stress) throw Error(RGPU_ERR_INVALID_ARGUMENT, "neg_stress output is required");
-    gap_predict_impl(m, s, precision, energies, forces, neg_stress);
+    gap_predict_entry(m, s, precision, energies, forces, neg_stress);
   });
 }
 
@@ -2253,6 +2462,29 @@ rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K, co
 rgpu_status rgpu_gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const float * A, const float * B,
                                       const float * alpha, int32_t zeta, float * e, void * stream) {
   return guard([&] { gap_energies_noalloc(M, N, K, A, B, alpha, zeta, e, static_cast<cudaStream_t>(stream)); });
+}
+
+rgpu_status rgpu_structures_use_graphs(rgpu_structures * s, int enable) {
+  return guard([&] {
+    OnDevice on_dev(s);
+    if (!s) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    s->use_graphs = enable != 0;
+    if (!s->use_graphs) {
+      RGPU_CUDA(cudaStreamSynchronize(s->st));
+      for (PredictGraph & g : s->pgraphs) pgraph_release(g);
+      s->pgraphs.clear();
+    }
+  });
+}
+
+rgpu_status rgpu_structures_graph_info(const rgpu_structures * s, int64_t * info) {
+  return guard([&] {
+    if (!s || !info) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    info[0] = int64_t(s->pgraphs.size());
+    info[1] = s->pgraph_replays;
+    info[2] = s->pgraph_records;
+    info[3] = s->pgraph_last_kernels;
+  });
 }
 
 rgpu_status rgpu_measure_fma_peak(int precision, double * tflops) {

@@ -119,6 +119,18 @@ class StructureSet:
         N.check(N.lib().rgpu_structures_stream(self._h, ctypes.byref(p)))
         return p.value or 0
 
+    def use_graphs(self, enable=True):
+        """Record FP32 predictions as CUDA graphs per size bucket (the
+        default) or always run the ordinary path (rgpu_structures_use_graphs)."""
+        N.check(N.lib().rgpu_structures_use_graphs(self._h, int(bool(enable))))
+
+    def graph_info(self):
+        """(buckets held, replays, recordings, kernels of the last replayed
+        graph) of the recorded FP32 predictions."""
+        info = np.zeros(4, np.int64)
+        N.check(N.lib().rgpu_structures_graph_info(self._h, N.ptr(info, N.c_i64_p)))
+        return tuple(int(x) for x in info)
+
     def stage_times(self):
         """Device ms of the stages of the last GAP prediction (see the header)."""
         out = np.zeros(8)
