@@ -664,6 +664,21 @@ def run_gap(args):
         step_resident()
         stages += st.stage_times()
     stages /= 3
+    # the launch shapes in use (the autotuner's table, librascal_b200/tune.py)
+    # against the hand-picked defaults, stage by stage
+    from librascal_b200 import tune
+    shape = (len(species), hypers["max_radial"], hypers["max_angular"])
+    tiles_cfg = tune.get_config(shape)
+    tiles = dict(shape=list(shape), config=tiles_cfg, tuned=tiles_cfg != tune.DEFAULT)
+    if tiles["tuned"]:
+        tune.set_config(shape, None)
+        dstages = np.zeros(8)
+        for _ in range(3):
+            step_resident()
+            dstages += st.stage_times()
+        tune.set_config(shape, tiles_cfg)
+        tiles["default_stage_ms"] = [round(float(x) / 3, 4) for x in dstages]
+        tiles["tuned_stage_ms"] = [round(float(x), 4) for x in stages]
     st.use_graphs(True)
     # a small batch of the same workload (launch- and synchronisation-bound),
     # recorded against ordinary
@@ -786,6 +801,7 @@ def run_gap(args):
                         kernels_per_replay=g1[3], small_batch=small,
                         note="value is timed with the recorded CUDA graph of this size bucket; the ordinary "
                              "path runs the same kernels with host synchronisations that size its buffers"),
+            tiles=tiles,
             plain_fp64_ms_per_step=plain["ms"] if plain else None,
             plain_fp64_atoms_per_s=(n_atoms * world / (plain["ms"] * 1e-3)) if plain else None,
             plain_fp64_stage_ms=plain["stage_ms"] if plain else None,

@@ -76,6 +76,9 @@ SIGNATURES = {
     "rgpu_kernel_launches": (ctypes.c_int64, [ctypes.c_int]),
     "rgpu_stage_times": (ctypes.c_int, [ctypes.c_void_p, c_dbl_p, ctypes.c_int32]),
     "rgpu_measure_fma_peak": (ctypes.c_int, [ctypes.c_int, c_dbl_p]),
+    "rgpu_set_tile_config": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int_p,
+                                            ctypes.c_int32]),
+    "rgpu_get_tile_config": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_int_p]),
     "rgpu_structures_use_graphs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rgpu_structures_graph_info": (ctypes.c_int, [ctypes.c_void_p, c_i64_p]),
     "rgpu_debug_gemm_bf16x3": (ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
@@ -103,6 +106,9 @@ def lib():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+        # launch shapes chosen by the autotuner (tuned_tiles.json)
+        from . import tune
+        tune.install_table(L)
         _lib = L
     return _lib
 

@@ -15,6 +15,8 @@
 // calculator_spherical_expansion.hh:2354-2358).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace rgpu {
@@ -210,14 +212,20 @@ void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_cent
   if (a.n_centers == 0 || n_pairs == 0) return;
   sph_constants_tu();
   if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
-  const int grid = int(std::min<int64_t>((n_pairs + kThreads - 1) / kThreads, int64_t(148) * 64));
+  const TileConfig cfg = tile_config(a.fd.S, a.fd.n, a.fd.L);
+  const int threads = std::min(cfg.adj_threads, kThreads);
+  int dev = 0, sms = 148;
+  RGPU_CUDA(cudaGetDevice(&dev));
+  RGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int grid =
+      int(std::min<int64_t>((n_pairs + threads - 1) / threads, int64_t(sms) * cfg.adj_blocks_per_sm));
 #define RGPU_ADJ_LAUNCH(LL, NVV)                                                                     \
   if (stress)                                                                                        \
-    pair_adjoint_kernel<LL, NVV, true><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC, forces, \
-                                                                   center_struct, stress);           \
+    pair_adjoint_kernel<LL, NVV, true><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC, forces,  \
+                                                                  center_struct, stress);            \
   else                                                                                               \
-    pair_adjoint_kernel<LL, NVV, false><<<grid, kThreads, 0, st>>>(a, pair_center, n_pairs, dC,       \
-                                                                    forces, nullptr, nullptr);
+    pair_adjoint_kernel<LL, NVV, false><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC,        \
+                                                                   forces, nullptr, nullptr);
 #define RGPU_ADJ_CASE(LL)                                                                            \
   case LL:                                                                                           \
     if (a.fd.n <= 8) {                                                                               \

@@ -909,7 +909,7 @@ void gap_fast_forward(rgpu_gap_model * m, rgpu_structures * s, double * E_d) {
     }
     row0 += rows;
   }
-  gemm_bf16x3_grouped(fwd.data(), int(fwd.size()), st);
+  gemm_bf16x3_grouped(fwd.data(), int(fwd.size()), st, tile_config(fd.S, fd.n, fd.L).gemm_variant);
   row0 = 0;
   for (int sI = 0; sI < fd.S; ++sI) {
     const int64_t rows = s->species_count[sI];
@@ -965,7 +965,7 @@ void gap_fast_backward(rgpu_gap_model * m, rgpu_structures * s, double * F_d, do
     }
     row0 += rows;
   }
-  gemm_bf16x3_grouped(bwd.data(), int(bwd.size()), st);
+  gemm_bf16x3_grouped(bwd.data(), int(bwd.size()), st, tile_config(fd.S, fd.n, fd.L).gemm_variant);
   mark(s, 6);
   PsArgs pa;
   pa.fd = fd;
@@ -2462,6 +2462,27 @@ rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K, co
 rgpu_status rgpu_gap_energies_noalloc(int64_t M, int64_t N, int64_t K, const float * A, const float * B,
                                       const float * alpha, int32_t zeta, float * e, void * stream) {
   return guard([&] { gap_energies_noalloc(M, N, K, A, B, alpha, zeta, e, static_cast<cudaStream_t>(stream)); });
+}
+
+rgpu_status rgpu_set_tile_config(int32_t n_species, int32_t max_radial, int32_t max_angular, const int32_t * values,
+                                 int32_t n_values) {
+  return guard([&] {
+    if (n_values == 0) {
+      set_tile_config(n_species, max_radial, max_angular, nullptr);
+      return;
+    }
+    if (n_values != kTileFields || !values)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "tile config: " + std::to_string(kTileFields) + " values expected");
+    const TileConfig c = tile_config_from_array(values);
+    set_tile_config(n_species, max_radial, max_angular, &c);
+  });
+}
+
+rgpu_status rgpu_get_tile_config(int32_t n_species, int32_t max_radial, int32_t max_angular, int32_t * values) {
+  return guard([&] {
+    if (!values) throw Error(RGPU_ERR_INVALID_ARGUMENT, "null argument");
+    tile_config_to_array(tile_config(n_species, max_radial, max_angular), values);
+  });
 }
 
 rgpu_status rgpu_structures_use_graphs(rgpu_structures * s, int enable) {

@@ -21,10 +21,12 @@ namespace {
 
 constexpr int kWarps = 4;
 constexpr int kPad = 33;  // shared row stride of the per-pair tiles
-// The FP32 kernel takes pairs 16 at a time (most centres of the molecular
-// benchmark have fewer than 16 pairs), which halves its per-warp tiles and
-// doubles the warps that fit on an SM.
-constexpr int kChunkF = 16, kPadF = 17;
+// The FP32 kernel takes pairs CH at a time (8, 16 or 32; 16 by default, as
+// most centres of the molecular benchmark have fewer than 16 pairs, which
+// keeps the per-warp tiles small and the resident warps many) with one
+// centre per warp and up to kMaxWarpsF warps per block, both chosen per
+// feature shape by the tile configuration.
+constexpr int kMaxWarpsF = 8;
 
 template <typename T>
 struct Tab;
@@ -216,20 +218,22 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
 //   (c) lanes = lm, n accumulators each (NV >= n registers): per pair of a
 //       species one Y_lm load feeds the n radial products; the sums are
 //       written once into the padded row layout [S*n][row_stride(L)].
-template <int L, int NV>
-__global__ void __launch_bounds__(kWarps * 32)
+template <int L, int NV, int CH>
+__global__ void __launch_bounds__(kMaxWarpsF * 32)
 expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restrict__ present) {
   constexpr int K = (L + 1) * (L + 1);
   constexpr int L1 = L + 1;
   constexpr int RS = row_stride(L), NPAD = RS - K;
+  constexpr int kChunkF = CH, kPadF = CH + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;  // centres per block
   const int W = a.fd.W, S = a.fd.S, n = a.fd.n;
   float * RIf = reinterpret_cast<float *>(smem_raw) + size_t(wid) * (W + K) * kPadF;  // [W][kPadF]
   float * Y = RIf + W * kPadF;                                                         // [K][kPadF]
-  __shared__ float pa_s[kWarps][32], pb_s[kWarps][32], fc_s[kWarps][32];
-  __shared__ int pk_s[kWarps][32];
-  __shared__ uint8_t order_s[kWarps][32];
+  __shared__ float pa_s[kMaxWarpsF][32], pb_s[kMaxWarpsF][32], fc_s[kMaxWarpsF][32];
+  __shared__ int pk_s[kMaxWarpsF][32];
+  __shared__ uint8_t order_s[kMaxWarpsF][32];
   __shared__ uint8_t lofk[K];
   __shared__ int16_t colk[K];     // padded column of lm: offp(l) + m
   __shared__ int16_t padc[NPAD];  // the padding columns of a row
@@ -246,8 +250,7 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
     for (int c = offp(L + 1); c < RS; ++c) padc[j++] = int16_t(c);
   }
   __syncthreads();
-  for (int64_t ci = int64_t(blockIdx.x) * kWarps + wid; ci < a.n_centers;
-       ci += int64_t(gridDim.x) * kWarps) {
+  for (int64_t ci = int64_t(blockIdx.x) * nw + wid; ci < a.n_centers; ci += int64_t(gridDim.x) * nw) {
     float * Ci = C + size_t(ci) * S * n * RS;
     const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
     const int ti = a.species_lut[a.types[a.center_atom[ci]]];
@@ -483,22 +486,36 @@ void launch_exp_f32(const ExpansionArgs & a, float * C, uint32_t * present, cuda
   if (a.n_centers == 0) return;
   if (a.fd.n > 16) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
   sph_constants_tu();
-  const size_t smem = size_t(kWarps) * (a.fd.W + a.fd.K) * kPadF * sizeof(float);
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int grid = int(std::min<int64_t>((a.n_centers + kWarps - 1) / kWarps, int64_t(sms) * 16));
-#define RGPU_EXP_CASE(LL)                                                                   \
-  case LL:                                                                                  \
-    if (a.fd.n <= 8) {                                                                      \
-      RGPU_CUDA(cudaFuncSetAttribute(expansion_f32_kernel<LL, 8>,                           \
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-      expansion_f32_kernel<LL, 8><<<grid, kWarps * 32, smem, st>>>(a, C, present);          \
-    } else {                                                                                \
-      RGPU_CUDA(cudaFuncSetAttribute(expansion_f32_kernel<LL, 16>,                          \
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))); \
-      expansion_f32_kernel<LL, 16><<<grid, kWarps * 32, smem, st>>>(a, C, present);         \
-    }                                                                                       \
+  const TileConfig cfg = tile_config(a.fd.S, a.fd.n, a.fd.L);
+  const int CH = cfg.exp_chunk;
+  int dev = 0, sms = 148, optin = 0;
+  RGPU_CUDA(cudaGetDevice(&dev));
+  RGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  RGPU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const size_t per_warp = size_t(a.fd.W + a.fd.K) * (CH + 1) * sizeof(float);
+  const int warps = int(std::max<size_t>(1, std::min<size_t>(size_t(cfg.exp_warps), (size_t(optin) - 8192) / per_warp)));
+  const size_t smem = size_t(warps) * per_warp;
+  int grid = int(std::min<int64_t>((a.n_centers + warps - 1) / warps, int64_t(sms) * 16 * (4 / std::min(warps, 4))));
+#define RGPU_EXPF_LAUNCH(LL, NVV, CHH)                                                              \
+  {                                                                                                 \
+    RGPU_CUDA(cudaFuncSetAttribute(expansion_f32_kernel<LL, NVV, CHH>,                              \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));        \
+    expansion_f32_kernel<LL, NVV, CHH><<<grid, warps * 32, smem, st>>>(a, C, present);              \
+  }
+#define RGPU_EXPF_NV(LL, CHH)          \
+  if (a.fd.n <= 8)                     \
+    RGPU_EXPF_LAUNCH(LL, 8, CHH)       \
+  else                                 \
+    RGPU_EXPF_LAUNCH(LL, 16, CHH)
+#define RGPU_EXP_CASE(LL)              \
+  case LL:                             \
+    if (CH == 8) {                     \
+      RGPU_EXPF_NV(LL, 8)              \
+    } else if (CH == 32) {             \
+      RGPU_EXPF_NV(LL, 32)             \
+    } else {                           \
+      RGPU_EXPF_NV(LL, 16)             \
+    }                                  \
     break;
   switch (a.fd.L) {
     RGPU_EXP_CASE(0)
@@ -518,6 +535,8 @@ void launch_exp_f32(const ExpansionArgs & a, float * C, uint32_t * present, cuda
       throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
   }
 #undef RGPU_EXP_CASE
+#undef RGPU_EXPF_NV
+#undef RGPU_EXPF_LAUNCH
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }

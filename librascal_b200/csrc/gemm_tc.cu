@@ -711,9 +711,8 @@ void gemm_bf16x3_status(const Bf16x3Gemm & g, int * status_dev, cudaStream_t st)
 }
 
 
-void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
-  // K blocks of 32 bf16 (64-byte swizzle): 4 stages of 48 KB in flight
-  constexpr int BN = kTcTileN, STAGES = 4, BK = 32;
+template <int BN, int STAGES, int BK>
+void grouped_launch(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
   TcGroupedArgs p;
   std::memset(&p, 0, sizeof(p));
   int ng = 0;
@@ -726,7 +725,7 @@ void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
       throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: groups must share the epilogue");
     p.epilogue = g.epilogue;
     p.zeta = g.zeta;
-    if (g.K % BK != 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: K must be a multiple of 32");
+    if (g.K % BK != 0) throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: K must be a multiple of the K block");
     p.a_hi[ng] = make_map(g.A_hi, g.M, g.K, g.lda, kBM, BK);
     p.a_lo[ng] = make_map(g.A_lo, g.M, g.K, g.lda, kBM, BK);
     p.b_hi[ng] = make_map(g.B_hi, g.N, g.K, g.ldb, BN, BK);
@@ -764,6 +763,27 @@ void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
   gemm_tc_grouped_kernel<BN, STAGES, BK><<<grid, kThreads, smem, st>>>(p);
   RGPU_LAUNCHED();
   cuda_check(cudaGetLastError(), "gemm_tc_grouped launch");
+}
+
+// Pipelines of the grouped GEMM (tile 128 x kTcTileN): 0 = 4 stages of K
+// blocks of 32 (64-byte swizzle, 192 KB of stages), 1 = 3 stages of 32,
+// 2 = 2 stages of K blocks of 64 (128-byte swizzle), used only when every
+// group's K is a multiple of 64 (else variant 0 runs).
+void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st, int variant) {
+  if (variant == 2) {
+    for (int i = 0; i < n; ++i)
+      if (gs[i].M > 0 && gs[i].N > 0 && gs[i].K % 64 != 0) variant = 0;
+  }
+  switch (variant) {
+    case 1:
+      grouped_launch<kTcTileN, 3, 32>(gs, n, st);
+      break;
+    case 2:
+      grouped_launch<kTcTileN, 2, 64>(gs, n, st);
+      break;
+    default:
+      grouped_launch<kTcTileN, 4, 32>(gs, n, st);
+  }
 }
 
 int gemm_tc_timeout(bool reset) {

@@ -274,18 +274,18 @@ ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __n
   constexpr int kG = offp(L + 1) / 4;
   __shared__ int8_t grp_l[kG];
   __shared__ int16_t grp_off[kG];
-  if (threadIdx.x < kG) {
-    int g = threadIdx.x, l = L;
+  for (int t = threadIdx.x; t < kG; t += blockDim.x) {
+    int g = t, l = L;
     while (g >= pad4(2 * l + 1) / 4) {
       g -= pad4(2 * l + 1) / 4;
       --l;
     }
-    grp_l[threadIdx.x] = int8_t(l);
-    grp_off[threadIdx.x] = int16_t(offp_rt(l) + 4 * g);
+    grp_l[t] = int8_t(l);
+    grp_off[t] = int16_t(offp_rt(l) + 4 * g);
   }
   make_keys(kt, S);
-  if (threadIdx.x < n * n) {
-    const int n1 = threadIdx.x / n, n2 = threadIdx.x - n1 * n;
+  for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+    const int n1 = t / n, n2 = t - n1 * n;
     if (n1 < n2) {
       const int p = n1 * (2 * n - n1 - 1) / 2 + (n2 - n1 - 1);
       pair_n1[p] = int8_t(n1);
@@ -480,12 +480,13 @@ void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloa
                         __nv_bfloat16 * Xl, float * row_scale, cudaStream_t st) {
   if (a.n_centers == 0) return;
   if (!Xh || !Xl) throw Error(RGPU_ERR_INVALID_ARGUMENT, "FP32 power spectrum needs the BF16 outputs");
+  const int threads = std::min(tile_config(a.fd.S, a.fd.n, a.fd.L).psf_threads, kThreads);
 #define RGPU_PSF_CASE(LL)                                                                                     \
   case LL: {                                                                                                  \
     const size_t smem = fwd_smem<LL>(a.fd);                                                                   \
     RGPU_CUDA(cudaFuncSetAttribute(ps_fwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
-    ps_fwd_f32_kernel<LL><<<persistent_grid(ps_fwd_f32_kernel<LL>, kThreads, smem, a.n_centers), kThreads,   \
+    ps_fwd_f32_kernel<LL><<<persistent_grid(ps_fwd_f32_kernel<LL>, threads, smem, a.n_centers), threads,     \
                             smem, st>>>(a, C, X, Xh, Xl, row_scale);                                          \
     break;                                                                                                    \
   }
@@ -517,6 +518,7 @@ void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 *
   if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
   const BwdShape bs = bwd_shape(a.fd);
   constexpr size_t kMaxSmem = 227 * 1024 - 2048;
+  const int threads = std::min(tile_config(a.fd.S, a.fd.n, a.fd.L).psb_threads, kBwdThreads);
 #define RGPU_PSB_CASE(LL)                                                                                     \
   case LL: {                                                                                                  \
     const size_t smem = bwd_smem<LL>(a.fd, bs);                                                               \
@@ -525,8 +527,8 @@ void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 *
                   "species x max_radial too large for the FP32 power-spectrum backward; use FP64");           \
     RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
-    ps_bwd_f32_kernel<LL><<<persistent_grid(ps_bwd_f32_kernel<LL>, kBwdThreads, smem, a.n_centers),           \
-                            kBwdThreads, smem, st>>>(a, bs, C, Xh, Xl, row_scale, dX, dC);                    \
+    ps_bwd_f32_kernel<LL><<<persistent_grid(ps_bwd_f32_kernel<LL>, threads, smem, a.n_centers),               \
+                            threads, smem, st>>>(a, bs, C, Xh, Xl, row_scale, dX, dC);                        \
     break;                                                                                                    \
   }
   switch (a.fd.L) {

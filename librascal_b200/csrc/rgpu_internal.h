@@ -65,6 +65,27 @@ struct RadialSpline {
 };
 void build_radial_spline(const Hypers & hy, RadialSpline & out);
 
+// Launch shapes of the FP32 per-centre and per-pair kernels and of the
+// grouped tensor-core GEMM, per feature shape (species S, max_radial n,
+// max_angular L). The project's autotuner (librascal_b200/tune.py) times the
+// candidates with CUDA events and commits its choices as a table that the
+// package loads into the library; shapes without an entry use the defaults.
+struct TileConfig {
+  int exp_chunk = 16;          // neighbour pairs per chunk of the FP32 expansion: 8, 16 or 32
+  int exp_warps = 4;           // centres (one warp each) per block of the FP32 expansion: 1..8
+  int adj_threads = 128;       // threads per block of the pair adjoint: 32..128, multiple of 32
+  int adj_blocks_per_sm = 64;  // grid cap of the pair adjoint, in blocks per SM: 1..256
+  int psf_threads = 256;       // threads per block of the power-spectrum forward: 64..256, multiple of 32
+  int psb_threads = 320;       // threads per block of the power-spectrum backward: 64..320, multiple of 32
+  int gemm_variant = 0;        // grouped GEMM pipeline: 0 = 4 stages of K 32, 1 = 3 of K 32, 2 = 2 of K 64
+};
+constexpr int kTileFields = 7;
+TileConfig tile_config(int S, int n, int L);
+// Install (c != nullptr, validated) or remove the entry of one shape.
+void set_tile_config(int S, int n, int L, const TileConfig * c);
+void tile_config_to_array(const TileConfig & c, int32_t * v);
+TileConfig tile_config_from_array(const int32_t * v);
+
 // Growable device buffer (reused across calls; never shrinks).
 struct DevBuf {
   void * p{nullptr};
@@ -313,7 +334,7 @@ constexpr int kTcTileN = 256;
 void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st);
 // Several GEMMs of the same epilogue kind (up to 16; K may differ) in one
 // persistent launch with a double-buffered TMEM accumulator.
-void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st);
+void gemm_bf16x3_grouped(const Bf16x3Gemm * gs, int n, cudaStream_t st, int variant = 0);
 // 0 when no bounded wait of the tcgen05 GEMM gave up, else where it did.
 int gemm_tc_timeout(bool reset);
 // Polls of the tcgen05 GEMMs' MMA-warp operand waits (negative: the

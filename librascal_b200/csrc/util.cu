@@ -4,6 +4,10 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
 
 #include "common.cuh"
 
@@ -31,6 +35,57 @@ int current_device() {
     throw Error(RGPU_ERR_CUDA, "device ordinal " + std::to_string(dev) + " beyond the library's table of " +
                                    std::to_string(kMaxDevices) + " devices");
   return dev;
+}
+
+namespace {
+std::mutex g_tile_mutex;
+std::map<std::tuple<int, int, int>, TileConfig> g_tiles;
+}  // namespace
+
+TileConfig tile_config(int S, int n, int L) {
+  std::lock_guard<std::mutex> lock(g_tile_mutex);
+  auto it = g_tiles.find(std::make_tuple(S, n, L));
+  return it == g_tiles.end() ? TileConfig{} : it->second;
+}
+
+void tile_config_to_array(const TileConfig & c, int32_t * v) {
+  v[0] = c.exp_chunk;
+  v[1] = c.exp_warps;
+  v[2] = c.adj_threads;
+  v[3] = c.adj_blocks_per_sm;
+  v[4] = c.psf_threads;
+  v[5] = c.psb_threads;
+  v[6] = c.gemm_variant;
+}
+
+TileConfig tile_config_from_array(const int32_t * v) {
+  TileConfig c;
+  c.exp_chunk = v[0];
+  c.exp_warps = v[1];
+  c.adj_threads = v[2];
+  c.adj_blocks_per_sm = v[3];
+  c.psf_threads = v[4];
+  c.psb_threads = v[5];
+  c.gemm_variant = v[6];
+  return c;
+}
+
+void set_tile_config(int S, int n, int L, const TileConfig * c) {
+  if (c) {
+    auto bad = [](const char * what) { throw Error(RGPU_ERR_INVALID_ARGUMENT, std::string("tile config: ") + what); };
+    if (c->exp_chunk != 8 && c->exp_chunk != 16 && c->exp_chunk != 32) bad("exp_chunk must be 8, 16 or 32");
+    if (c->exp_warps < 1 || c->exp_warps > 8) bad("exp_warps must be in [1, 8]");
+    if (c->adj_threads < 32 || c->adj_threads > 128 || c->adj_threads % 32) bad("adj_threads must be 32, 64, 96 or 128");
+    if (c->adj_blocks_per_sm < 1 || c->adj_blocks_per_sm > 256) bad("adj_blocks_per_sm must be in [1, 256]");
+    if (c->psf_threads < 64 || c->psf_threads > 256 || c->psf_threads % 32) bad("psf_threads must be a multiple of 32 in [64, 256]");
+    if (c->psb_threads < 64 || c->psb_threads > 320 || c->psb_threads % 32) bad("psb_threads must be a multiple of 32 in [64, 320]");
+    if (c->gemm_variant < 0 || c->gemm_variant > 2) bad("gemm_variant must be 0, 1 or 2");
+  }
+  std::lock_guard<std::mutex> lock(g_tile_mutex);
+  if (c)
+    g_tiles[std::make_tuple(S, n, L)] = *c;
+  else
+    g_tiles.erase(std::make_tuple(S, n, L));
 }
 
 void DevBuf::ensure(size_t bytes) {

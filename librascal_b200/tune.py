@@ -1,0 +1,185 @@
+"""Autotuner for the launch shapes of the FP32 path.
+
+The per-centre and per-pair kernels and the grouped tensor-core GEMM take
+their launch shapes from a table keyed by the feature shape (species S,
+max_radial n, max_angular l): the neighbour chunk and the centres per block
+of the expansion, the block size and grid cap of the pair adjoint, the block
+sizes of the power-spectrum forward and backward, and the GEMM pipeline
+(rgpu_set_tile_config). This module measures the candidates of each field
+with CUDA events (the library's per-stage events of rgpu_gap_predict, on the
+ordinary path) by coordinate descent from the defaults, keeps for each field
+the value with the shortest stage time, and writes the winners to
+``tuned_tiles.json`` beside this file, which the package installs whenever it
+loads the library.
+
+    python -m librascal_b200.tune --workload gap      # the molecule clusters
+    python -m librascal_b200.tune --workload bulk     # the 100 000-atom box shape
+
+Each run replaces the table's entry for its shape and keeps the others.
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import _native as N
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+TABLE = os.path.join(HERE, "tuned_tiles.json")
+FIELDS = ["exp_chunk", "exp_warps", "adj_threads", "adj_blocks_per_sm", "psf_threads", "psb_threads",
+          "gemm_variant"]
+DEFAULT = dict(exp_chunk=16, exp_warps=4, adj_threads=128, adj_blocks_per_sm=64, psf_threads=256,
+               psb_threads=320, gemm_variant=0)
+CANDIDATES = dict(exp_chunk=[8, 16, 32], exp_warps=[2, 4, 8], adj_threads=[64, 96, 128],
+                  adj_blocks_per_sm=[8, 16, 32, 64, 128], psf_threads=[64, 96, 128, 192, 256],
+                  psb_threads=[160, 192, 224, 256, 288, 320], gemm_variant=[0, 1, 2])
+# stage_times index (rgpu_stage_times) each field acts on
+STAGES = dict(exp_chunk=(2,), exp_warps=(2,), adj_threads=(7,), adj_blocks_per_sm=(7,), psf_threads=(3,),
+              psb_threads=(6,), gemm_variant=(4, 5))
+
+
+def set_config(shape, cfg):
+    """Install cfg (dict of FIELDS) for shape (S, n, l); None removes it."""
+    S, n, l = (int(x) for x in shape)
+    if cfg is None:
+        N.check(N.lib().rgpu_set_tile_config(S, n, l, None, 0))
+        return
+    v = np.ascontiguousarray([int(cfg[f]) for f in FIELDS], dtype=np.int32)
+    N.check(N.lib().rgpu_set_tile_config(S, n, l, N.ptr(v, N.c_int_p), len(FIELDS)))
+
+
+def get_config(shape):
+    S, n, l = (int(x) for x in shape)
+    v = np.zeros(len(FIELDS), np.int32)
+    N.check(N.lib().rgpu_get_tile_config(S, n, l, N.ptr(v, N.c_int_p)))
+    return dict(zip(FIELDS, (int(x) for x in v)))
+
+
+def load_table(path=TABLE):
+    if not os.path.exists(path):
+        return []
+    with open(path) as f:
+        return json.load(f).get("entries", [])
+
+
+def install_table(lib=None, path=TABLE):
+    """Hand every entry of the table to the library (host-side only)."""
+    lib = lib or N.lib()
+    for e in load_table(path):
+        S, n, l = e["shape"]
+        v = np.ascontiguousarray([int(e["values"][f]) for f in FIELDS], dtype=np.int32)
+        lib.rgpu_set_tile_config(int(S), int(n), int(l), v.ctypes.data_as(N.c_int_p), len(FIELDS))
+
+
+def stage_ms(model, structures, repeats, precision="fp32"):
+    """Per-stage device ms of the prediction (rgpu_stage_times, which only
+    the ordinary path records, so the recorded graphs are switched off), the
+    minimum over `repeats` calls after one untimed call."""
+    structures.use_graphs(False)
+    structures.invalidate()
+    model.predict(structures, precision, energies=False, forces=False)
+    best = None
+    for _ in range(repeats):
+        structures.invalidate()
+        model.predict(structures, precision, energies=False, forces=False)
+        t = structures.stage_times()
+        best = t if best is None else np.minimum(best, t)
+    return best
+
+
+def tune(model, structures, shape, repeats=3, log=print):
+    """Coordinate descent over FIELDS from the defaults; returns the chosen
+    configuration and every measurement (field, value, stage ms)."""
+    structures.use_graphs(False)
+    cfg = dict(DEFAULT)
+    measured = []
+    for field in FIELDS:
+        times = {}
+        for cand in CANDIDATES[field]:
+            trial = dict(cfg, **{field: cand})
+            set_config(shape, trial)
+            t = stage_ms(model, structures, repeats)
+            ms = float(sum(t[i] for i in STAGES[field]))
+            times[cand] = ms
+            measured.append(dict(field=field, value=cand, stage_ms=round(ms, 4)))
+            if log:
+                log("%-18s %4d  %.4f ms" % (field, cand, ms))
+        cfg[field] = min(times, key=times.get)
+    set_config(shape, cfg)
+    structures.use_graphs(True)
+    return cfg, measured
+
+
+def _workload(name, seed=0):
+    """Model and structures of a benchmark workload (see bench.py)."""
+    import librascal_b200 as rb
+    from librascal_b200 import synthetic
+    if name == "gap":
+        hy = dict(interaction_cutoff=5.0, max_radial=8, max_angular=6, gaussian_sigma_constant=0.4)
+        batch = synthetic.molecule_clusters(n_struct=10000, seed=seed)
+        sel = {k: v for k, v in batch.items()}
+        off = batch["atom_offsets"]
+        k = 1000
+        sel = dict(atom_offsets=off[:k + 1], positions=batch["positions"][:off[k]],
+                   numbers=batch["numbers"][:off[k]], cells=batch["cells"][:k], pbc=batch["pbc"][:k])
+        n_sparse = 4000
+    elif name == "bulk":
+        hy = dict(interaction_cutoff=6.0, max_radial=12, max_angular=9, gaussian_sigma_constant=0.5)
+        batch = synthetic.bulk_box(n_atoms=100000, seed=seed)
+        sel = synthetic.bulk_box(n_atoms=8000, seed=seed + 17)
+        n_sparse = 4000
+    else:
+        raise ValueError(name)
+    calc = rb.SphericalInvariants(cutoff_smooth_width=0.5, gaussian_sigma_type="Constant",
+                                  optimization=dict(Spline=dict(accuracy=1e-8)), **hy)
+    species = sorted(set(int(z) for z in batch["numbers"]))
+    al = calc.transform(rb.AtomsList(rb.StructureSet(sel)))
+    keys = calc.get_keys(species)
+    X = al.get_features(calc, keys=keys)
+    info = al.get_representation_info()
+    counts = {s: int(np.sum(batch["numbers"] == s)) for s in species}
+    tot = sum(counts.values())
+    per = {s: int(round(n_sparse * c / tot)) for s, c in counts.items()}
+    per[species[0]] += n_sparse - sum(per.values())
+    idx = synthetic.select_sparse_points(X, info[:, 2], per, seed=seed)
+    sp = rb.SparsePoints(calc)
+    sp.add_dense(info[idx, 2], X[idx], keys)
+    alpha = np.random.default_rng(seed + 1).normal(size=len(idx))
+    model = rb.GAPModel(calc, sp, alpha, zeta=2)
+    shape = (len(species), hy["max_radial"], hy["max_angular"])
+    return model, rb.StructureSet(batch), shape
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    p.add_argument("--workload", default="gap", choices=["gap", "bulk"])
+    p.add_argument("--repeats", type=int, default=3)
+    p.add_argument("--out", default=TABLE)
+    args = p.parse_args()
+    import torch
+    torch.cuda.set_device(0)
+    model, st, shape = _workload(args.workload)
+    set_config(shape, None)
+    t0 = time.time()
+    default = stage_ms(model, st, args.repeats)
+    cfg, measured = tune(model, st, shape, args.repeats)
+    tuned = stage_ms(model, st, args.repeats)
+    entries = [e for e in load_table(args.out) if tuple(e["shape"]) != tuple(shape)]
+    props = torch.cuda.get_device_properties(0)
+    entries.append(dict(shape=list(shape), workload=args.workload, values=cfg, device=props.name,
+                        default_stage_ms=[round(float(x), 4) for x in default],
+                        tuned_stage_ms=[round(float(x), 4) for x in tuned],
+                        measurements=measured, seconds=round(time.time() - t0, 1)))
+    with open(args.out, "w") as f:
+        json.dump(dict(fields=FIELDS, defaults=DEFAULT,
+                       stages=["total", "neighbour_list", "expansion", "power_spectrum", "gemm_fwd", "gemm_bwd",
+                               "ps_backward", "pair_adjoint"],
+                       entries=entries), f, indent=1)
+    print(json.dumps(dict(shape=shape, values=cfg, default_total_ms=float(default[0]),
+                          tuned_total_ms=float(tuned[0]))))
+
+
+if __name__ == "__main__":
+    main()

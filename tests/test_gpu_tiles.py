@@ -1,0 +1,56 @@
+"""Every launch shape the autotuner can choose gives the same FP32 results:
+each candidate of each tile field, on the molecule-cluster shape (5
+species, n 8, l 6) and on the bulk shape (2 species, n 12, l 9), against
+the FP64 oracle at the FP32 bar (1e-4 of the largest value)."""
+import numpy as np
+import pytest
+
+import librascal_b200 as rb
+from librascal_b200 import synthetic, tune
+from test_gpu_parity import gap_setup, soap
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(batch, kw, n_sparse):
+    r, T, sps, alpha, species = gap_setup(batch, kw, n_sparse=n_sparse)
+    E_ref, F_ref = r.gap(sps, T, alpha, 2)
+    calc = soap(**kw)
+    sp = rb.SparsePoints(calc)
+    sp.add_dense(sps, T, calc.get_keys(species))
+    model = rb.GAPModel(calc, sp, alpha, 2)
+    return model, E_ref, F_ref, (len(species), kw["n"], kw["l"])
+
+
+def _check(model, batch, E_ref, F_ref, shape, cfg):
+    old = tune.get_config(shape)
+    try:
+        tune.set_config(shape, cfg)
+        st = rb.StructureSet(batch)
+        st.use_graphs(False)
+        E, F = model.predict(st, "fp32")
+    finally:
+        tune.set_config(shape, old)
+    assert np.abs(E - E_ref).max() <= 1e-4 * np.abs(E_ref).max()
+    assert np.abs(F - F_ref).max() <= 1e-4 * np.abs(F_ref).max()
+
+
+@pytest.fixture(scope="module")
+def clusters():
+    batch = synthetic.molecule_clusters(n_struct=40, seed=51)
+    return (batch,) + _case(batch, dict(rc=5.0, n=8, l=6, sigma=0.4), 40)
+
+
+@pytest.mark.parametrize("field,value", [(f, v) for f in tune.FIELDS for v in tune.CANDIDATES[f]])
+def test_cluster_shape_every_candidate(clusters, field, value):
+    batch, model, E_ref, F_ref, shape = clusters
+    _check(model, batch, E_ref, F_ref, shape, dict(tune.DEFAULT, **{field: value}))
+
+
+@pytest.mark.parametrize("cfg", [dict(exp_chunk=32, exp_warps=8, gemm_variant=2, psb_threads=160),
+                                 dict(exp_chunk=8, exp_warps=2, adj_threads=64, adj_blocks_per_sm=8,
+                                      psf_threads=128, gemm_variant=1)])
+def test_bulk_shape_extremes(cfg):
+    batch = synthetic.bulk_box(n_atoms=300, seed=52)
+    model, E_ref, F_ref, shape = _case(batch, dict(rc=6.0, n=12, l=9, sigma=0.5), 30)
+    _check(model, batch, E_ref, F_ref, shape, dict(tune.DEFAULT, **cfg))
