@@ -33,7 +33,13 @@ SOURCES = [
     ("gemm_tc.cu", [], "gemm_tc"),
     ("noalloc.cu", [], "noalloc"),
     ("peaks.cu", [], "peaks"),
-    ("adjoint.cu", [], "adjoint"),
+    # the adjoint's instantiations unroll the spherical-harmonics recurrence
+    # per max_angular: four translation units by range of L, compiled in
+    # parallel (the first also holds the dispatch)
+    ("adjoint.cu", ["-DRGPU_ADJ_L0=0", "-DRGPU_ADJ_L1=6", "-DRGPU_ADJ_DISPATCH"], "adjoint_l0"),
+    ("adjoint.cu", ["-DRGPU_ADJ_L0=7", "-DRGPU_ADJ_L1=9"], "adjoint_l7"),
+    ("adjoint.cu", ["-DRGPU_ADJ_L0=10", "-DRGPU_ADJ_L1=11"], "adjoint_l10"),
+    ("adjoint.cu", ["-DRGPU_ADJ_L0=12", "-DRGPU_ADJ_L1=12"], "adjoint_l12"),
     ("training.cu", [], "training"),
     ("api.cu", [], "api"),
     ("radial_gto.cpp", ["-Xcompiler", "-ffp-contract=off"], "radial_gto"),

@@ -19,6 +19,12 @@
 
 #include "common.cuh"
 
+#ifndef RGPU_ADJ_L0
+#define RGPU_ADJ_L0 0
+#define RGPU_ADJ_L1 12
+#define RGPU_ADJ_DISPATCH
+#endif
+
 namespace rgpu {
 namespace {
 
@@ -57,7 +63,7 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
   constexpr int K = (L + 1) * (L + 1);
   constexpr int L1 = L + 1;
   const int W = a.fd.W, n = a.fd.n, Sn = a.fd.S * a.fd.n;
-  const bool vec = (n == NV);
+  const bool vec = (n & 3) == 0;  // dE/dc rows of n floats as 16-byte loads
   const int lane = threadIdx.x & 31;
   const int64_t stride = int64_t(gridDim.x) * blockDim.x;
   // the list's own total bounds the loop (below n_pairs when the list was
@@ -108,9 +114,11 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
               const float4 * E4 = reinterpret_cast<const float4 *>(El);
 #pragma unroll
               for (int qq = 0; qq < NV / 4; ++qq) {
-                const float4 ev = __ldg(E4 + qq);
-                A += ev.x * pl[4 * qq] + ev.y * pl[4 * qq + 1] + ev.z * pl[4 * qq + 2] + ev.w * pl[4 * qq + 3];
-                B += ev.x * rl[4 * qq] + ev.y * rl[4 * qq + 1] + ev.z * rl[4 * qq + 2] + ev.w * rl[4 * qq + 3];
+                if (4 * qq < n) {
+                  const float4 ev = __ldg(E4 + qq);
+                  A += ev.x * pl[4 * qq] + ev.y * pl[4 * qq + 1] + ev.z * pl[4 * qq + 2] + ev.w * pl[4 * qq + 3];
+                  B += ev.x * rl[4 * qq] + ev.y * rl[4 * qq + 1] + ev.z * rl[4 * qq + 2] + ev.w * rl[4 * qq + 3];
+                }
               }
             } else {
 #pragma unroll
@@ -204,13 +212,123 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
   }
 }
 
+// One instantiation per (L, NV): compiled in the translation unit that owns
+// L (the library builds this file once per range of L, in parallel, since
+// each instantiation unrolls the spherical-harmonics recurrence).
+template <int L>
+void adjoint_launch(const ExpansionArgs & a, const int32_t * pair_center, int64_t n_pairs, const float * dC,
+                    double * forces, cudaStream_t st, const int32_t * center_struct, double * stress, int grid,
+                    int threads) {
+  sph_constants_tu();  // this translation unit's copy of the constants
+  if (a.fd.n <= 8) {
+    if (stress)
+      pair_adjoint_kernel<L, 8, true><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC, forces, center_struct,
+                                                              stress);
+    else
+      pair_adjoint_kernel<L, 8, false><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC, forces, nullptr,
+                                                               nullptr);
+  } else {
+    if (stress)
+      pair_adjoint_kernel<L, 16, true><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC, forces,
+                                                               center_struct, stress);
+    else
+      pair_adjoint_kernel<L, 16, false><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC, forces, nullptr,
+                                                                nullptr);
+  }
+}
+
 }  // namespace
 
+// Launch of the adjoint kernels of one L. Each translation unit
+// instantiates it for its own range of L (explicit instantiation below); the
+// dispatch refers to the others through extern declarations.
+template <int L>
+void adjoint_launch_l(const ExpansionArgs & a, const int32_t * pc, int64_t np, const float * dC, double * F,
+                      cudaStream_t st, const int32_t * cs, double * S, int grid, int threads) {
+  adjoint_launch<L>(a, pc, np, dC, F, st, cs, S, grid, threads);
+}
+
+#define RGPU_ADJ_SIG(LL)                                                                                  \
+  void adjoint_launch_l<LL>(const ExpansionArgs &, const int32_t *, int64_t, const float *, double *,     \
+                            cudaStream_t, const int32_t *, double *, int, int)
+#define RGPU_ADJ_INST(LL)                                             \
+  template RGPU_ADJ_SIG(LL);
+#define RGPU_ADJ_EXTERN(LL)                                           \
+  extern template RGPU_ADJ_SIG(LL);
+#if RGPU_ADJ_L0 <= 0 && 0 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(0)
+#else
+RGPU_ADJ_EXTERN(0)
+#endif
+#if RGPU_ADJ_L0 <= 1 && 1 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(1)
+#else
+RGPU_ADJ_EXTERN(1)
+#endif
+#if RGPU_ADJ_L0 <= 2 && 2 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(2)
+#else
+RGPU_ADJ_EXTERN(2)
+#endif
+#if RGPU_ADJ_L0 <= 3 && 3 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(3)
+#else
+RGPU_ADJ_EXTERN(3)
+#endif
+#if RGPU_ADJ_L0 <= 4 && 4 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(4)
+#else
+RGPU_ADJ_EXTERN(4)
+#endif
+#if RGPU_ADJ_L0 <= 5 && 5 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(5)
+#else
+RGPU_ADJ_EXTERN(5)
+#endif
+#if RGPU_ADJ_L0 <= 6 && 6 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(6)
+#else
+RGPU_ADJ_EXTERN(6)
+#endif
+#if RGPU_ADJ_L0 <= 7 && 7 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(7)
+#else
+RGPU_ADJ_EXTERN(7)
+#endif
+#if RGPU_ADJ_L0 <= 8 && 8 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(8)
+#else
+RGPU_ADJ_EXTERN(8)
+#endif
+#if RGPU_ADJ_L0 <= 9 && 9 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(9)
+#else
+RGPU_ADJ_EXTERN(9)
+#endif
+#if RGPU_ADJ_L0 <= 10 && 10 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(10)
+#else
+RGPU_ADJ_EXTERN(10)
+#endif
+#if RGPU_ADJ_L0 <= 11 && 11 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(11)
+#else
+RGPU_ADJ_EXTERN(11)
+#endif
+#if RGPU_ADJ_L0 <= 12 && 12 <= RGPU_ADJ_L1
+RGPU_ADJ_INST(12)
+#else
+RGPU_ADJ_EXTERN(12)
+#endif
+#undef RGPU_ADJ_EXTERN
+#undef RGPU_ADJ_INST
+#undef RGPU_ADJ_SIG
+
+#ifdef RGPU_ADJ_DISPATCH
 void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_center, int64_t n_pairs,
                               const float * dC, double * forces, cudaStream_t st,
                               const int32_t * center_struct, double * stress) {
   if (a.n_centers == 0 || n_pairs == 0) return;
-  sph_constants_tu();
   if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
   const TileConfig cfg = tile_config(a.fd.S, a.fd.n, a.fd.L);
   const int threads = std::min(cfg.adj_threads, kThreads);
@@ -219,20 +337,9 @@ void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_cent
   RGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   const int grid =
       int(std::min<int64_t>((n_pairs + threads - 1) / threads, int64_t(sms) * cfg.adj_blocks_per_sm));
-#define RGPU_ADJ_LAUNCH(LL, NVV)                                                                     \
-  if (stress)                                                                                        \
-    pair_adjoint_kernel<LL, NVV, true><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC, forces,  \
-                                                                  center_struct, stress);            \
-  else                                                                                               \
-    pair_adjoint_kernel<LL, NVV, false><<<grid, threads, 0, st>>>(a, pair_center, n_pairs, dC,        \
-                                                                   forces, nullptr, nullptr);
-#define RGPU_ADJ_CASE(LL)                                                                            \
-  case LL:                                                                                           \
-    if (a.fd.n <= 8) {                                                                               \
-      RGPU_ADJ_LAUNCH(LL, 8)                                                                         \
-    } else {                                                                                         \
-      RGPU_ADJ_LAUNCH(LL, 16)                                                                        \
-    }                                                                                                \
+#define RGPU_ADJ_CASE(LL)                                                                        \
+  case LL:                                                                                       \
+    adjoint_launch_l<LL>(a, pair_center, n_pairs, dC, forces, st, center_struct, stress, grid, threads); \
     break;
   switch (a.fd.L) {
     RGPU_ADJ_CASE(0)
@@ -252,9 +359,9 @@ void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_cent
       throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_angular above 12 is not supported on the GPU");
   }
 #undef RGPU_ADJ_CASE
-#undef RGPU_ADJ_LAUNCH
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
+#endif
 
 }  // namespace rgpu

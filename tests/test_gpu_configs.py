@@ -123,3 +123,14 @@ def test_cluster_model_at_full_size():
     assert len(T) == 4000 and T.shape[1] == 6720
     ev = synthetic.molecule_clusters(n_struct=50, seed=42)
     _gap_vs_oracle(ev, CLUSTERS, T, sps, alpha, species)
+
+
+@pytest.mark.parametrize("l", [3, 7, 10, 12])
+def test_fp32_gap_across_max_angular(l):
+    """The FP32 path at max_angular values whose kernels live in different
+    translation units of the library (each holds its own copy of the
+    spherical-harmonics constants)."""
+    kw = dict(rc=4.0, n=4, l=l, sigma=0.4)
+    batch = synthetic.molecule_clusters(n_struct=6, seed=60 + l)
+    T, sps, alpha, species = _model_from(batch, kw, 6, seed=l)
+    _gap_vs_oracle(batch, kw, T, sps, alpha, species)
