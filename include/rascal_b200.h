@@ -325,19 +325,20 @@ rgpu_status rgpu_stage_times(const rgpu_structures * s, double * ms_out,
  * max_angular), as chosen by the project's autotuner
  * (librascal_b200/tune.py, which times candidates with CUDA events and
  * commits its table; the Python package installs the table when it loads
- * the library). values[7] = neighbour pairs per chunk of the expansion (8,
+ * the library). values[8] = neighbour pairs per chunk of the expansion (8,
  * 16 or 32), centres per block of the expansion (1..8), threads per block of
  * the pair adjoint (32..128, multiple of 32), its grid cap in blocks per SM
  * (1..256), threads per block of the power-spectrum forward (64..256) and
- * backward (64..320), both multiples of 32, and the grouped GEMM pipeline
- * (0: 4 stages of K blocks of 32, 1: 3 of 32, 2: 2 of 64). n_values = 0
- * removes the shape's entry (back to the defaults 16, 4, 128, 64, 256, 320,
- * 0); values out of range are rejected. Process-wide; no counterpart in
+ * backward (64..320), both multiples of 32, the grouped GEMM pipeline
+ * (0: 4 stages of K blocks of 32, 1: 3 of 32, 2: 2 of 64), and the
+ * power-spectrum forward (0: FP32 pipe, 1: tcgen05 Gram products). n_values
+ * = 0 removes the shape's entry (back to the defaults 16, 4, 128, 64, 256,
+ * 320, 0, 0); values out of range are rejected. Process-wide; no counterpart in
  * the reference (its kernels are serial C++ loops). */
 rgpu_status rgpu_set_tile_config(int32_t n_species, int32_t max_radial, int32_t max_angular,
                                  const int32_t * values, int32_t n_values);
 rgpu_status rgpu_get_tile_config(int32_t n_species, int32_t max_radial, int32_t max_angular,
-                                 int32_t * values /* [7] */);
+                                 int32_t * values /* [8] */);
 
 /* FP32 predictions as recorded CUDA graphs. With graphs on (the default),
  * rgpu_gap_predict and rgpu_gap_predict_stress at RGPU_PRECISION_FP32 record

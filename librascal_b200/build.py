@@ -29,6 +29,7 @@ SOURCES = [
     ("expansion.cu", ["-DRGPU_PART_FP32"], "expansion_f32"),
     ("powerspectrum.cu", ["--fmad=false", "-DRGPU_PART_FP64"], "powerspectrum_f64"),
     ("ps_fast.cu", [], "ps_fast"),
+    ("ps_tc.cu", [], "ps_tc"),
     ("gemm.cu", [], "gemm"),
     ("gemm_tc.cu", [], "gemm_tc"),
     ("noalloc.cu", [], "noalloc"),

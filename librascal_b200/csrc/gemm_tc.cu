@@ -28,145 +28,15 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 namespace rgpu {
+using namespace tc;
 namespace {
 
 constexpr int kBM = 128;
 constexpr int kBK = 64;  // bf16 elements per K block = 128 bytes (one swizzle row)
 constexpr int kThreads = 192;
-// Polls of one mbarrier before giving up (each try_wait may also suspend
-// briefly in hardware): far beyond any legitimate pipeline wait, and short
-// enough that a stuck wait ends the kernel in seconds. A wait that gives up
-// sets the shared status flag, which every other wait checks.
-constexpr long long kSpinLimit = 1ll << 22;
-
-struct TcStatus {
-  int timeout;
-  int where;
-};
-
-// ---------------------------------------------------------------- PTX wrappers
-__device__ __forceinline__ uint32_t smem_u32(const void * p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t * bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void fence_barrier_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t * bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t * bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t * bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-// Bounded wait: false when `limit` polls were not enough (the status word
-// records it) or another wait of the launch already gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t * bar, uint32_t parity, TcStatus * st, int where,
-                                          long long limit = kSpinLimit) {
-  for (long long i = 0; i < limit; ++i) {
-    if (mbar_try_wait(bar, parity)) return true;
-    if ((i & 63) == 63 && *reinterpret_cast<volatile int *>(&st->timeout)) return false;
-  }
-  if (atomicCAS(&st->timeout, 0, 1) == 0) st->where = where;
-  return false;
-}
-// Wait for work this CTA itself started (TMA copies into its shared memory,
-// its own MMAs) before the CTA releases the memory they write. Unlike
-// mbar_wait it does not give up when another wait of the launch has: that
-// work completes on its own, and the shared memory and TMEM must not be
-// released under it. Still bounded, by kSpinLimit polls.
-__device__ __forceinline__ void mbar_drain(uint64_t * bar, uint32_t parity, TcStatus * st, int where) {
-  for (long long i = 0; i < kSpinLimit; ++i)
-    if (mbar_try_wait(bar, parity)) return;
-  if (atomicCAS(&st->timeout, 0, 1) == 0) st->where = where;
-}
-__device__ __forceinline__ void tma_load_2d(void * dst, const CUtensorMap * map, uint64_t * bar, int x, int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
-      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
-__device__ __forceinline__ void prefetch_map(const CUtensorMap * map) {
-  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (start, LBO, SBO in 16-byte units; version 1; layout 2).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= uint64_t((addr >> 4) & 0x3FFF);
-  d |= uint64_t(1) << 16;            // leading byte offset (unused for swizzled K-major)
-  d |= uint64_t(1024 >> 4) << 32;    // stride byte offset: next 8-row group
-  d |= uint64_t(1) << 46;            // descriptor version
-  d |= uint64_t(2) << 61;            // 128-byte swizzle
-  return d;
-}
-// The same descriptor for a K block of BK bf16 per row: 128-byte rows with
-// the 128-byte swizzle (BK = 64) or 64-byte rows with the 64-byte swizzle
-// (BK = 32, 8-row groups 512 bytes apart; layout type 4).
-template <int BK>
-__device__ __forceinline__ uint64_t smem_desc_k(uint32_t addr) {
-  static_assert(BK == 64 || BK == 32, "K block of 32 or 64 bf16");
-  if constexpr (BK == 64) {
-    return smem_desc(addr);
-  } else {
-    uint64_t d = 0;
-    d |= uint64_t((addr >> 4) & 0x3FFF);
-    d |= uint64_t(1) << 16;
-    d |= uint64_t(512 >> 4) << 32;
-    d |= uint64_t(1) << 46;
-    d |= uint64_t(4) << 61;
-    return d;
-  }
-}
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}"
-      ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc)
-      : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint64_t * bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float * v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// Instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16
-// (bits 7-9 = 1, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at
-// bits 17-22, M >> 4 at bits 24-28.
-__host__ __device__ constexpr uint32_t make_idesc(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
-}
-
 struct TcArgs {
   int64_t M, N, K;
   int epilogue;        // 0 store FP32 C; 1 GAP forward
@@ -643,6 +513,8 @@ static TcStatus * tc_status() {
     p = q;
   });
 }
+
+TcStatus * tc_status_word() { return tc_status(); }
 
 void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st) {
   if (g.M <= 0 || g.N <= 0) return;

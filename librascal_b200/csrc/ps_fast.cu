@@ -512,6 +512,14 @@ void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloa
   RGPU_CUDA(cudaGetLastError());
 }
 
+void launch_ps_fwd_fast(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh, __nv_bfloat16 * Xl,
+                        float * row_scale, cudaStream_t st) {
+  if (!X && tile_config(a.fd.S, a.fd.n, a.fd.L).psf_tc && ps_fwd_tc_supported(a.fd))
+    launch_ps_fwd_tc(a, C, Xh, Xl, row_scale, st);
+  else
+    launch_ps_fwd_fp32(a, C, X, Xh, Xl, row_scale, st);
+}
+
 void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh, const __nv_bfloat16 * Xl,
                         const float * row_scale, const float * dX, float * dC, cudaStream_t st) {
   if (a.n_centers == 0) return;

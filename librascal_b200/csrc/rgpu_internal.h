@@ -78,8 +78,9 @@ struct TileConfig {
   int psf_threads = 256;       // threads per block of the power-spectrum forward: 64..256, multiple of 32
   int psb_threads = 320;       // threads per block of the power-spectrum backward: 64..320, multiple of 32
   int gemm_variant = 0;        // grouped GEMM pipeline: 0 = 4 stages of K 32, 1 = 3 of K 32, 2 = 2 of K 64
+  int psf_tc = 0;              // power-spectrum forward: 0 = FP32 pipe, 1 = tcgen05 Gram products
 };
-constexpr int kTileFields = 7;
+constexpr int kTileFields = 8;
 TileConfig tile_config(int S, int n, int L);
 // Install (c != nullptr, validated) or remove the entry of one shape.
 void set_tile_config(int S, int n, int L, const TileConfig * c);
@@ -260,6 +261,16 @@ void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double *
 // 1/|p| (1 without normalisation); x = row_scale * p.
 void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
                         __nv_bfloat16 * Xl, float * row_scale, cudaStream_t st);
+// The same forward (without the FP32 copy) as tcgen05 Gram products of
+// the centres' l-blocks, BF16x3 with FP32 accumulation (ps_tc.cu), for
+// shapes it supports (S n <= 128, n a multiple of 4).
+bool ps_fwd_tc_supported(const FeatureDims & fd);
+void launch_ps_fwd_tc(const PsArgs & a, const float * C, __nv_bfloat16 * Xh, __nv_bfloat16 * Xl,
+                      float * row_scale, cudaStream_t st);
+// Forward used by the FP32 path: the tile configuration picks the tcgen05
+// kernel when it supports the shape and no FP32 copy is asked for.
+void launch_ps_fwd_fast(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh, __nv_bfloat16 * Xl,
+                        float * row_scale, cudaStream_t st);
 // Plain-path gradients of the normalised power spectrum for pairs of centres
 // [c0,c1): dX[p - p_base][3][D].
 void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, int64_t c1,

@@ -56,6 +56,7 @@ void tile_config_to_array(const TileConfig & c, int32_t * v) {
   v[4] = c.psf_threads;
   v[5] = c.psb_threads;
   v[6] = c.gemm_variant;
+  v[7] = c.psf_tc;
 }
 
 TileConfig tile_config_from_array(const int32_t * v) {
@@ -67,6 +68,7 @@ TileConfig tile_config_from_array(const int32_t * v) {
   c.psf_threads = v[4];
   c.psb_threads = v[5];
   c.gemm_variant = v[6];
+  c.psf_tc = v[7];
   return c;
 }
 
@@ -80,6 +82,7 @@ void set_tile_config(int S, int n, int L, const TileConfig * c) {
     if (c->psf_threads < 64 || c->psf_threads > 256 || c->psf_threads % 32) bad("psf_threads must be a multiple of 32 in [64, 256]");
     if (c->psb_threads < 64 || c->psb_threads > 320 || c->psb_threads % 32) bad("psb_threads must be a multiple of 32 in [64, 320]");
     if (c->gemm_variant < 0 || c->gemm_variant > 2) bad("gemm_variant must be 0, 1 or 2");
+    if (c->psf_tc < 0 || c->psf_tc > 1) bad("psf_tc must be 0 or 1");
   }
   std::lock_guard<std::mutex> lock(g_tile_mutex);
   if (c)

@@ -29,15 +29,15 @@ from . import _native as N
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "tuned_tiles.json")
 FIELDS = ["exp_chunk", "exp_warps", "adj_threads", "adj_blocks_per_sm", "psf_threads", "psb_threads",
-          "gemm_variant"]
+          "gemm_variant", "psf_tc"]
 DEFAULT = dict(exp_chunk=16, exp_warps=4, adj_threads=128, adj_blocks_per_sm=64, psf_threads=256,
-               psb_threads=320, gemm_variant=0)
+               psb_threads=320, gemm_variant=0, psf_tc=0)
 CANDIDATES = dict(exp_chunk=[8, 16, 32], exp_warps=[2, 4, 8], adj_threads=[64, 96, 128],
                   adj_blocks_per_sm=[8, 16, 32, 64, 128], psf_threads=[64, 96, 128, 192, 256],
-                  psb_threads=[160, 192, 224, 256, 288, 320], gemm_variant=[0, 1, 2])
+                  psb_threads=[160, 192, 224, 256, 288, 320], gemm_variant=[0, 1, 2], psf_tc=[0, 1])
 # stage_times index (rgpu_stage_times) each field acts on
 STAGES = dict(exp_chunk=(2,), exp_warps=(2,), adj_threads=(7,), adj_blocks_per_sm=(7,), psf_threads=(3,),
-              psb_threads=(6,), gemm_variant=(4, 5))
+              psb_threads=(6,), gemm_variant=(4, 5), psf_tc=(3,))
 
 
 def set_config(shape, cfg):
@@ -69,7 +69,7 @@ def install_table(lib=None, path=TABLE):
     lib = lib or N.lib()
     for e in load_table(path):
         S, n, l = e["shape"]
-        v = np.ascontiguousarray([int(e["values"][f]) for f in FIELDS], dtype=np.int32)
+        v = np.ascontiguousarray([int(e["values"].get(f, DEFAULT[f])) for f in FIELDS], dtype=np.int32)
         lib.rgpu_set_tile_config(int(S), int(n), int(l), v.ctypes.data_as(N.c_int_p), len(FIELDS))
 
 

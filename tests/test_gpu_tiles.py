@@ -54,3 +54,18 @@ def test_bulk_shape_extremes(cfg):
     batch = synthetic.bulk_box(n_atoms=300, seed=52)
     model, E_ref, F_ref, shape = _case(batch, dict(rc=6.0, n=12, l=9, sigma=0.5), 30)
     _check(model, batch, E_ref, F_ref, shape, dict(tune.DEFAULT, **cfg))
+
+
+@pytest.mark.parametrize("which", ["clusters", "triclinic", "bulk"])
+def test_tensor_core_power_spectrum_forward(which):
+    """The tcgen05 power-spectrum forward (psf_tc = 1) at tiles of 3, 4 and
+    5 centres (S n = 40, 32, 24), each batch ending in a partial tile."""
+    if which == "clusters":
+        batch, kw = synthetic.molecule_clusters(n_struct=23, seed=61), dict(rc=5.0, n=8, l=6, sigma=0.4)
+    elif which == "triclinic":
+        batch, kw = synthetic.triclinic_cells(n_struct=2, n_min=33, n_max=45, seed=62), dict(rc=5.0, n=8, l=6,
+                                                                                             sigma=0.4)
+    else:
+        batch, kw = synthetic.bulk_box(n_atoms=301, seed=63), dict(rc=6.0, n=12, l=9, sigma=0.5)
+    model, E_ref, F_ref, shape = _case(batch, kw, 20)
+    _check(model, batch, E_ref, F_ref, shape, dict(tune.DEFAULT, psf_tc=1))
