@@ -14,6 +14,7 @@ loads the library.
 
     python -m librascal_b200.tune --workload gap      # the molecule clusters
     python -m librascal_b200.tune --workload bulk     # the 100 000-atom box shape
+    python -m librascal_b200.tune --workload triclinic  # the 256 triclinic cells
 
 Each run replaces the table's entry for its shape and keeps the others.
 """
@@ -125,6 +126,14 @@ def _workload(name, seed=0):
         sel = dict(atom_offsets=off[:k + 1], positions=batch["positions"][:off[k]],
                    numbers=batch["numbers"][:off[k]], cells=batch["cells"][:k], pbc=batch["pbc"][:k])
         n_sparse = 4000
+    elif name == "triclinic":
+        hy = dict(interaction_cutoff=5.0, max_radial=8, max_angular=6, gaussian_sigma_constant=0.4)
+        batch = synthetic.triclinic_cells(n_struct=256, seed=seed)
+        off = batch["atom_offsets"]
+        k = 64
+        sel = dict(atom_offsets=off[:k + 1], positions=batch["positions"][:off[k]],
+                   numbers=batch["numbers"][:off[k]], cells=batch["cells"][:k], pbc=batch["pbc"][:k])
+        n_sparse = None  # 2 000 per species
     elif name == "bulk":
         hy = dict(interaction_cutoff=6.0, max_radial=12, max_angular=9, gaussian_sigma_constant=0.5)
         batch = synthetic.bulk_box(n_atoms=100000, seed=seed)
@@ -139,10 +148,13 @@ def _workload(name, seed=0):
     keys = calc.get_keys(species)
     X = al.get_features(calc, keys=keys)
     info = al.get_representation_info()
-    counts = {s: int(np.sum(batch["numbers"] == s)) for s in species}
-    tot = sum(counts.values())
-    per = {s: int(round(n_sparse * c / tot)) for s, c in counts.items()}
-    per[species[0]] += n_sparse - sum(per.values())
+    if n_sparse is None:
+        per = {s: 2000 for s in species}
+    else:
+        counts = {s: int(np.sum(batch["numbers"] == s)) for s in species}
+        tot = sum(counts.values())
+        per = {s: int(round(n_sparse * c / tot)) for s, c in counts.items()}
+        per[species[0]] += n_sparse - sum(per.values())
     idx = synthetic.select_sparse_points(X, info[:, 2], per, seed=seed)
     sp = rb.SparsePoints(calc)
     sp.add_dense(info[idx, 2], X[idx], keys)
@@ -154,7 +166,7 @@ def _workload(name, seed=0):
 
 def main():
     p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    p.add_argument("--workload", default="gap", choices=["gap", "bulk"])
+    p.add_argument("--workload", default="gap", choices=["gap", "bulk", "triclinic"])
     p.add_argument("--repeats", type=int, default=3)
     p.add_argument("--out", default=TABLE)
     args = p.parse_args()
