@@ -76,6 +76,19 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
   for (int64_t base = int64_t(blockIdx.x) * blockDim.x + threadIdx.x - lane; base < n_pairs; base += stride) {
     const int64_t p = base + lane;
     const int32_t ci = p < n_pairs ? pair_center[p] : -1;
+    {
+      // the lanes of one centre bring its dE/dc row (Sn K floats, read
+      // below one lm at a time) towards L2 together, before the spline and
+      // Y_lm work, so that the reads below wait on L2 rather than DRAM
+      const unsigned same = __match_any_sync(0xffffffffu, ci);
+      if (ci >= 0) {
+        const int rank = __popc(same & lanemask_lt()), run = __popc(same);
+        const char * row = reinterpret_cast<const char *>(dC + size_t(ci) * Sn * K);
+        const int lines = (Sn * K * 4 + 127) >> 7;
+        for (int k = rank; k < lines; k += run)
+          asm volatile("prefetch.global.L2 [%0];" ::"l"(row + (size_t(k) << 7)));
+      }
+    }
     float g0 = 0.f, g1 = 0.f, g2 = 0.f;
     float t6[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int32_t j = -1, self_atom = -1;

@@ -215,49 +215,53 @@ expansion_kernel(ExpansionArgs a, T * __restrict__ C, uint32_t * __restrict__ pr
 //   (a) lanes = pairs: f_c, the spline interval and Y_lm of one pair each;
 //   (b) lanes = radial channels: f_c RI_c(r_p) for the chunk's pairs one
 //       after the other, one 16-byte load of the interval table per channel;
-//   (c) lanes = lm, n accumulators each (NV >= n registers): per pair of a
-//       species one Y_lm load feeds the n radial products; the sums are
-//       written once into the padded row layout [S*n][row_stride(L)].
-template <int L, int NV, int CH>
+//   (c) lanes = (l, four columns m of the padded l-block, four radial
+//       channels): 16 accumulators per lane; per pair of a species one
+//       16-byte load of Y and four loads of f_c RI feed 16 products; the
+//       sums are written once, as 16-byte stores, into the padded row
+//       layout [S*n][row_stride(L)] (Y is zero in the padding columns, so
+//       the padding of every l-block is written as zero).
+template <int L, int CH>
 __global__ void __launch_bounds__(kMaxWarpsF * 32)
 expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restrict__ present) {
   constexpr int K = (L + 1) * (L + 1);
   constexpr int L1 = L + 1;
-  constexpr int RS = row_stride(L), NPAD = RS - K;
+  constexpr int RS = row_stride(L), OL = offp(L + 1), NG = OL / 4;
   constexpr int kChunkF = CH, kPadF = CH + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nw = blockDim.x >> 5;  // centres per block
   const int W = a.fd.W, S = a.fd.S, n = a.fd.n;
-  float * RIf = reinterpret_cast<float *>(smem_raw) + size_t(wid) * (W + K) * kPadF;  // [W][kPadF]
-  float * Y = RIf + W * kPadF;                                                         // [K][kPadF]
+  const int wpad = (W * kPadF + 3) & ~3;  // keeps Yp 16-byte aligned
+  float * RIf = reinterpret_cast<float *>(smem_raw) + size_t(wid) * (wpad + CH * RS);  // [W][kPadF]
+  float * Yp = RIf + wpad;  // [CH][RS]: Y_lm of each pair in the padded column layout
   __shared__ float pa_s[kMaxWarpsF][32], pb_s[kMaxWarpsF][32], fc_s[kMaxWarpsF][32];
   __shared__ int pk_s[kMaxWarpsF][32];
   __shared__ uint8_t order_s[kMaxWarpsF][32];
-  __shared__ uint8_t lofk[K];
-  __shared__ int16_t colk[K];     // padded column of lm: offp(l) + m
-  __shared__ int16_t padc[NPAD];  // the padding columns of a row
+  __shared__ int16_t colk[K];  // padded column of lm: offp(l) + m
+  __shared__ uint8_t grp_l[NG];
   for (int lm = threadIdx.x; lm < K; lm += blockDim.x) {
     int l = 0;
     while ((l + 1) * (l + 1) <= lm) ++l;
-    lofk[lm] = uint8_t(l);
     colk[lm] = int16_t(offp_rt(l) + (lm - l * l));
   }
-  if (threadIdx.x == 0) {
-    int j = 0;
-    for (int l = 0; l <= L; ++l)
-      for (int c = 2 * l + 1; c < pad4(2 * l + 1); ++c) padc[j++] = int16_t(offp_rt(l) + c);
-    for (int c = offp(L + 1); c < RS; ++c) padc[j++] = int16_t(c);
+  for (int g = threadIdx.x; g < NG; g += blockDim.x) {
+    int l = 0;
+    while (4 * g >= offp_rt(l + 1)) ++l;
+    grp_l[g] = uint8_t(l);
   }
+  for (int e = lane; e < CH * RS; e += 32) Yp[e] = 0.f;  // padding columns stay zero
   __syncthreads();
+  const int nblk = (n + 3) >> 2;  // blocks of four radial channels
   for (int64_t ci = int64_t(blockIdx.x) * nw + wid; ci < a.n_centers; ci += int64_t(gridDim.x) * nw) {
     float * Ci = C + size_t(ci) * S * n * RS;
     const int64_t p_lo = a.pair_off[ci] + 1, p_hi = a.pair_off[ci + 1];
     const int ti = a.species_lut[a.types[a.center_atom[ci]]];
     uint32_t mask_all = 1u << ti;
-    for (int j = lane; j < NPAD; j += 32) {
-      const int c = padc[j];
-      for (int row = 0; row < S * n; ++row) Ci[row * RS + c] = 0.f;
+    // the columns after the last l-block
+    for (int j = lane; j < S * n * (RS - OL); j += 32) {
+      const int row = j / (RS - OL), c = OL + (j - row * (RS - OL));
+      Ci[row * RS + c] = 0.f;
     }
     bool first = true;
     for (int64_t p0 = p_lo; p0 < p_hi || first; p0 += kChunkF) {
@@ -274,8 +278,9 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
         fc_s[wid][lane] = float(cutoff_fc(a, r));
         const float dx = float(a.pair_dir[3 * p]), dy = float(a.pair_dir[3 * p + 1]),
                     dz = float(a.pair_dir[3 * p + 2]);
+        float * yrow = Yp + lane * RS;
         spherical_harmonics<L, false, float>(dx, dy, dz, [&](int lm, float y, float, float, float) {
-          Y[lm * kPadF + lane] = y;
+          yrow[colk[lm]] = y;
         });
       }
       // stable order of the chunk's pairs by species
@@ -317,29 +322,45 @@ expansion_f32_kernel(ExpansionArgs a, float * __restrict__ C, uint32_t * __restr
         const int cnt = __popc(__ballot_sync(0xffffffffu, my_sp == s));
         if (cnt > 0 || first) {
           float * Cs = Ci + size_t(s) * n * RS;
-          for (int lm = lane; lm < K; lm += 32) {
-            const float * ri = RIf + lofk[lm] * kPadF;  // row nn*L1 + l at + nn*L1*kPadF
-            const float * yy = Y + lm * kPadF;
-            float acc[NV];
+          for (int t = lane; t < NG * nblk; t += 32) {
+            const int g = t % NG, n0 = 4 * (t / NG);
+            const int l = grp_l[g], col = 4 * g;
+            const float * ri = RIf + (n0 * L1 + l) * kPadF;  // channel (n0 + k) L1 + l at + k L1 kPadF
+            float acc[4][4];
 #pragma unroll
-            for (int nn = 0; nn < NV; ++nn) acc[nn] = 0.f;
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+              for (int e = 0; e < 4; ++e) acc[k][e] = 0.f;
             for (int q = 0; q < cnt; ++q) {
               const int pl = order_s[wid][start + q];
-              const float y = yy[pl];
+              const float4 y = *reinterpret_cast<const float4 *>(Yp + pl * RS + col);
 #pragma unroll
-              for (int nn = 0; nn < NV; ++nn)
-                if (nn < n) acc[nn] += ri[nn * L1 * kPadF + pl] * y;
+              for (int k = 0; k < 4; ++k) {
+                if (n0 + k < n) {
+                  const float rv = ri[k * L1 * kPadF + pl];
+                  acc[k][0] += rv * y.x;
+                  acc[k][1] += rv * y.y;
+                  acc[k][2] += rv * y.z;
+                  acc[k][3] += rv * y.w;
+                }
+              }
             }
-            float * dst = Cs + colk[lm];
 #pragma unroll
-            for (int nn = 0; nn < NV; ++nn) {
+            for (int k = 0; k < 4; ++k) {
+              const int nn = n0 + k;
               if (nn < n) {
+                float4 * dst = reinterpret_cast<float4 *>(Cs + nn * RS + col);
                 if (first) {
                   // centre contribution (calculator_spherical_expansion.hh:2244-2247)
-                  if (s == ti && lm == 0) acc[nn] += float(a.center_contrib[nn]);
-                  dst[nn * RS] = acc[nn];
+                  if (s == ti && col == 0) acc[k][0] += float(a.center_contrib[nn]);
+                  *dst = make_float4(acc[k][0], acc[k][1], acc[k][2], acc[k][3]);
                 } else {
-                  dst[nn * RS] += acc[nn];
+                  float4 o = *dst;
+                  o.x += acc[k][0];
+                  o.y += acc[k][1];
+                  o.z += acc[k][2];
+                  o.w += acc[k][3];
+                  *dst = o;
                 }
               }
             }
@@ -492,21 +513,17 @@ void launch_exp_f32(const ExpansionArgs & a, float * C, uint32_t * present, cuda
   RGPU_CUDA(cudaGetDevice(&dev));
   RGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   RGPU_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  const size_t per_warp = size_t(a.fd.W + a.fd.K) * (CH + 1) * sizeof(float);
+  const size_t per_warp =
+      ((size_t(a.fd.W) * (CH + 1) + 3) / 4 * 4 + size_t(CH) * row_stride(a.fd.L)) * sizeof(float);
   const int warps = int(std::max<size_t>(1, std::min<size_t>(size_t(cfg.exp_warps), (size_t(optin) - 8192) / per_warp)));
   const size_t smem = size_t(warps) * per_warp;
   int grid = int(std::min<int64_t>((a.n_centers + warps - 1) / warps, int64_t(sms) * 16 * (4 / std::min(warps, 4))));
-#define RGPU_EXPF_LAUNCH(LL, NVV, CHH)                                                              \
+#define RGPU_EXPF_NV(LL, CHH)                                                                       \
   {                                                                                                 \
-    RGPU_CUDA(cudaFuncSetAttribute(expansion_f32_kernel<LL, NVV, CHH>,                              \
+    RGPU_CUDA(cudaFuncSetAttribute(expansion_f32_kernel<LL, CHH>,                                   \
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));        \
-    expansion_f32_kernel<LL, NVV, CHH><<<grid, warps * 32, smem, st>>>(a, C, present);              \
+    expansion_f32_kernel<LL, CHH><<<grid, warps * 32, smem, st>>>(a, C, present);                   \
   }
-#define RGPU_EXPF_NV(LL, CHH)          \
-  if (a.fd.n <= 8)                     \
-    RGPU_EXPF_LAUNCH(LL, 8, CHH)       \
-  else                                 \
-    RGPU_EXPF_LAUNCH(LL, 16, CHH)
 #define RGPU_EXP_CASE(LL)              \
   case LL:                             \
     if (CH == 8) {                     \
@@ -536,7 +553,6 @@ void launch_exp_f32(const ExpansionArgs & a, float * C, uint32_t * present, cuda
   }
 #undef RGPU_EXP_CASE
 #undef RGPU_EXPF_NV
-#undef RGPU_EXPF_LAUNCH
   RGPU_LAUNCHED();
   RGPU_CUDA(cudaGetLastError());
 }
