@@ -229,15 +229,32 @@ __global__ void energy_reduce_kernel(int64_t rows, int n_parts, const float * __
                                      const int32_t * __restrict__ center_of_row,
                                      const int32_t * __restrict__ center_struct,
                                      double * __restrict__ E) {
-  int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (r >= rows) return;
+  const int64_t r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   double e = 0.;
-  if (e_row) {
-    e = e_row[r];
-  } else {
-    for (int t = 0; t < n_parts; ++t) e += double(e_part[int64_t(t) * ld + r]);
+  int key = -1;
+  if (r < rows) {
+    if (e_row) {
+      e = e_row[r];
+    } else {
+      for (int t = 0; t < n_parts; ++t) e += double(e_part[int64_t(t) * ld + r]);
+    }
+    key = center_struct[center_of_row[row0 + r]];
   }
-  atomicAdd(&E[center_struct[center_of_row[row0 + r]]], e);
+  // the warp's rows of one structure are summed first, so a structure with
+  // many centres (one large box) takes one atomic per warp, not per row
+  const int lane = threadIdx.x & 31;
+  double sum = 0.;
+  int leader = 32;
+#pragma unroll 4
+  for (int src = 0; src < 32; ++src) {
+    const double v = __shfl_sync(0xffffffffu, e, src);
+    const int k = __shfl_sync(0xffffffffu, key, src);
+    if (k == key) {
+      sum += v;
+      leader = min(leader, src);
+    }
+  }
+  if (key >= 0 && leader == lane) atomicAdd(&E[key], sum);
 }
 
 // Plain path: gradients[j] += dX_i(pair) . t_i, one warp per pair.
