@@ -305,19 +305,20 @@ def row_stride(L):
     return s if (s // 4) % 2 == 1 else s + 4
 
 
-def stage_roofline(stages, nc, n_pairs, n_atoms, S, n, L, Dpad, hbm, fp32):
+def stage_roofline(stages, nc, n_pairs, n_atoms, S, n, L, Dg, hbm, fp32):
     """Per-centre kernels of the FP32 path against HBM: algorithmic bytes each
     kernel must move in its layout (pair data read once, per-centre arrays
-    read or written once) over its CUDA-event time."""
+    read or written once; feature rows of Dg packed columns) over its
+    CUDA-event time."""
     K = (L + 1) ** 2
     C = 4.0 * nc * S * n * row_stride(L)   # FP32 expansion coefficients
     dC = 4.0 * nc * S * n * K              # dE/dC
-    X2 = 4.0 * nc * Dpad                   # BF16 hi + lo rows
+    X2 = 4.0 * nc * Dg                     # BF16 hi + lo rows
     pair = 36.0 * n_pairs                  # distance, direction, neighbour index
     rows = {
         "expansion": (2, pair + C),
         "power_spectrum": (3, C + X2 + 4.0 * nc),
-        "ps_backward": (6, C + X2 + 4.0 * nc * Dpad + dC + 4.0 * nc),
+        "ps_backward": (6, C + X2 + 4.0 * nc * Dg + dC + 4.0 * nc),
         "pair_adjoint": (7, pair + 4.0 * n_pairs + dC + 24.0 * n_atoms),
     }
     out = {}
@@ -729,9 +730,13 @@ def run_gap(args):
     counts = np.array([np.sum(batch["numbers"] == s) for s in species])
     msp = np.array([int(np.sum(np.asarray(sp.species) == s)) for s in species])
     S, n, L = len(species), hypers["max_radial"], hypers["max_angular"]
-    D = S * (S + 1) // 2 * n ** 2 * (L + 1)
-    Dpad = (D + 31) // 32 * 32
-    gemm_flops = 4.0 * float(np.sum(counts * msp)) * D  # forward + backward
+    # the FP32 path's rows hold the upper triangles of the per-l Gram
+    # matrices (one entry per symmetric pair of same-species entries), in
+    # 2 x 2 tiles: Dp values, Dg columns with padding
+    Sn = S * n
+    Dp = (L + 1) * Sn * (Sn + 1) // 2
+    Dg = ((L + 1) * ((2 * ((Sn + 1) // 2) * ((Sn + 1) // 2 + 1) + 7) // 8 * 8) + 31) // 32 * 32
+    gemm_flops = 4.0 * float(np.sum(counts * msp)) * Dp  # forward + backward
     gemm_ms = stages[4] + stages[5]
     bf16_peak, hbm_peak, peak_kind = peaks()
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
@@ -808,7 +813,7 @@ def run_gap(args):
             config=dict(workload=spec["desc"], n_structures=int(len(off) - 1), n_atoms=n_atoms,
                         n_pairs=int(n_pairs), sparse_points=int(sp.size()), precision=args.precision,
                         parallelism=parallelism,
-                        l2="inputs larger than L2: X and dE/dX are %.1f GB each" % (n_atoms * Dpad * 4 / 1e9),
+                        l2="inputs larger than L2: X and dE/dX are %.1f GB each" % (n_atoms * Dg * 4 / 1e9),
                         stage_ms=dict(zip(["total", "neighbour_list", "expansion", "power_spectrum",
                                            "gemm_fwd", "gemm_bwd", "ps_backward", "pair_adjoint"],
                                           [round(float(x), 4) for x in stages]))),
@@ -836,7 +841,7 @@ def run_gap(args):
                                     "3-term split issues 3x that on the tensor pipe" % peak_kind,
                           issued_frac=(3 * achieved / bf16_peak) if achieved else None,
                           flops_per_step=gemm_flops),
-            stage_roofline=stage_roofline(stages, n_centers, n_pairs, n_atoms, S, n, L, Dpad, hbm_peak,
+            stage_roofline=stage_roofline(stages, n_centers, n_pairs, n_atoms, S, n, L, Dg, hbm_peak,
                                           fma["fp32"] if fma else None),
             measured_fma_tflops=fma,
             cpu_baseline=cpu, e2e=e2e, gpu_launches=launches, clocks=clk.summary())

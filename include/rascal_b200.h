@@ -391,6 +391,17 @@ rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K,
  * restore the default after use. */
 rgpu_status rgpu_debug_set_gemm_wait_limit(int64_t polls);
 
+/* Test hook for the packed column layout of the FP32 path (no reference
+ * counterpart; host arithmetic only, no device needed). For S species,
+ * max_radial n and max_angular l: *D and *Dg receive the reference's row
+ * length and the packed row length; when `ref` is given (D values in the
+ * reference's dense order) `packed` receives its packed form (Dg values,
+ * same-species pairs (n1 n2) and (n2 n1) folded into one column) and
+ * `unpacked` that packed row mapped back to the reference's order through
+ * FP32, as the FP32 feature export does. */
+rgpu_status rgpu_debug_packed_layout(int32_t S, int32_t max_radial, int32_t max_angular, int64_t * D, int64_t * Dg,
+                                     const double * ref, double * packed, double * unpacked);
+
 /* ---------------------------------------------------------------------- */
 /* GAP energies without device allocation. No counterpart in the reference:
  * it is the per-row energy of the mode-1 GEMM above,

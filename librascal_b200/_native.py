@@ -85,6 +85,8 @@ SIGNATURES = {
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rgpu_debug_set_gemm_wait_limit": (ctypes.c_int, [ctypes.c_int64]),
+    "rgpu_debug_packed_layout": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, c_i64_p, c_i64_p,
+                                                c_dbl_p, c_dbl_p, c_dbl_p]),
     "rgpu_gap_energies_noalloc": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                                  ctypes.c_void_p, ctypes.c_void_p]),

@@ -385,6 +385,10 @@ FeatureDims make_dims(const Hypers & hy, int S) {
   f.P = S * (S + 1) / 2;
   f.D = f.P * f.n * f.n * (f.L + 1);
   f.Dpad = (f.D + 31) / 32 * 32;
+  f.Sn = S * f.n;
+  const int pairs = (f.Sn + 1) / 2;  // 2 x 2 tiles of the packed layout per row or column
+  f.Bp = (2 * pairs * (pairs + 1) + 7) / 8 * 8;
+  f.Dg = ((f.L + 1) * f.Bp + 31) / 32 * 32;
   return f;
 }
 
@@ -513,9 +517,9 @@ void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, b
     launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), s->st);
     mark(s, 3);
     if (c->hy.kind == "sphericalinvariants") {
-      if (need_x32) s->X32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
-      s->Xh.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dpad + 64);
-      s->Xl.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dpad + 64);
+      if (need_x32) s->X32.ensure(sizeof(float) * size_t(nc) * fd.Dg + 64);
+      s->Xh.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dg + 64);
+      s->Xl.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dg + 64);
       s->xscale32.ensure(sizeof(float) * (nc + 1));
       launch_ps_fwd_fast(pa, s->C32.as<float>(), need_x32 ? s->X32.as<float>() : nullptr,
                          s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(), s->xscale32.as<float>(), s->st);
@@ -676,7 +680,7 @@ void model_layout(rgpu_gap_model * m, rgpu_structures * s, bool bf16) {
     g.M = int(rows[sI].size());
     g.Mpad = (g.M + 31) / 32 * 32;
     m->tt_off[sI] = tt_total;
-    tt_total += int64_t(g.Mpad) * fd.Dpad;
+    tt_total += int64_t(g.Mpad) * fd.Dg;
     for (int r : rows[sI]) {
       user[pos] = r;
       al[pos] = m->alpha[r];
@@ -724,25 +728,26 @@ void model_layout_bf16(rgpu_gap_model * m, rgpu_structures * s) {
     std::memcpy(&f, &u, 4);
     return f;
   };
-  // the BF16 copies use the fast column order of the FP32 path (padding stays 0)
-  std::vector<int> fcol(fd.D);
-  for (int d = 0; d < fd.D; ++d) fcol[d] = fast_column(fd, d);
-  std::vector<uint16_t> Th(T.size(), 0), Tl(T.size(), 0);
-  for (int r = 0; r < m->M; ++r)
-    for (int d = 0; d < fd.D; ++d) {
-      const float v = float(T[size_t(r) * fd.Dpad + d]);
-      const size_t o = size_t(r) * fd.Dpad + fcol[d];
+  // the BF16 copies use the packed layout of the FP32 path (padding stays 0)
+  std::vector<uint16_t> Th(size_t(std::max(m->M, 1)) * fd.Dg, 0), Tl(Th.size(), 0);
+  std::vector<double> packed(fd.Dg);
+  for (int r = 0; r < m->M; ++r) {
+    pack_reference_row(fd, &T[size_t(r) * fd.Dpad], packed.data());
+    for (int d = 0; d < fd.Dg; ++d) {
+      const float v = float(packed[d]);
+      const size_t o = size_t(r) * fd.Dg + d;
       Th[o] = f2bf(v);
       Tl[o] = f2bf(v - bf2f(Th[o]));
     }
+  }
   std::vector<float> al32(al.size());
   for (size_t i = 0; i < al.size(); ++i) al32[i] = float(al[i]);
   std::vector<uint16_t> Tth(size_t(std::max<int64_t>(tt_total, 1)), 0), Ttl(Tth.size(), 0);
   for (int sI = 0; sI < fd.S; ++sI) {
     const GapSpecies & g = m->segs[sI];
     for (int mm = 0; mm < g.M; ++mm)
-      for (int d = 0; d < fd.D; ++d) {
-        const size_t src = size_t(g.m0 + mm) * fd.Dpad + d;
+      for (int d = 0; d < fd.Dg; ++d) {
+        const size_t src = size_t(g.m0 + mm) * fd.Dg + d;
         const size_t dst = size_t(m->tt_off[sI]) + size_t(d) * g.Mpad + mm;
         Tth[dst] = Th[src];
         Ttl[dst] = Tl[src];
@@ -875,7 +880,7 @@ void gap_fast_forward(rgpu_gap_model * m, rgpu_structures * s, double * E_d) {
   s->Wh.ensure(sizeof(uint16_t) * size_t(std::max<int64_t>(wtot, 1)) + 64);
   s->Wl.ensure(sizeof(uint16_t) * size_t(std::max<int64_t>(wtot, 1)) + 64);
   s->epart.ensure(sizeof(float) * size_t(std::max<int64_t>(eparts, 1)) + 64);
-  s->dX32.ensure(sizeof(float) * size_t(nc) * fd.Dpad + 64);
+  s->dX32.ensure(sizeof(float) * size_t(nc) * fd.Dg + 64);
   const __nv_bfloat16 * Xh = s->Xh.as<__nv_bfloat16>();
   const __nv_bfloat16 * Xl = s->Xl.as<__nv_bfloat16>();
   __nv_bfloat16 * Wh = s->Wh.as<__nv_bfloat16>();
@@ -890,13 +895,13 @@ void gap_fast_forward(rgpu_gap_model * m, rgpu_structures * s, double * E_d) {
       Bf16x3Gemm a{};
       a.M = rows;
       a.N = g.M;
-      a.K = fd.Dpad;
-      a.A_hi = Xh + size_t(row0) * fd.Dpad;
-      a.A_lo = Xl + size_t(row0) * fd.Dpad;
-      a.lda = fd.Dpad;
-      a.B_hi = m->Th.as<__nv_bfloat16>() + size_t(g.m0) * fd.Dpad;
-      a.B_lo = m->Tl.as<__nv_bfloat16>() + size_t(g.m0) * fd.Dpad;
-      a.ldb = fd.Dpad;
+      a.K = fd.Dg;
+      a.A_hi = Xh + size_t(row0) * fd.Dg;
+      a.A_lo = Xl + size_t(row0) * fd.Dg;
+      a.lda = fd.Dg;
+      a.B_hi = m->Th.as<__nv_bfloat16>() + size_t(g.m0) * fd.Dg;
+      a.B_lo = m->Tl.as<__nv_bfloat16>() + size_t(g.m0) * fd.Dg;
+      a.ldb = fd.Dg;
       a.epilogue = 1;
       a.W_hi = Wh + wofs[sI];
       a.W_lo = Wl + wofs[sI];
@@ -948,7 +953,7 @@ void gap_fast_backward(rgpu_gap_model * m, rgpu_structures * s, double * F_d, do
     if (rows > 0 && g.M > 0) {
       Bf16x3Gemm a{};
       a.M = rows;
-      a.N = fd.Dpad;
+      a.N = fd.Dg;
       a.K = g.Mpad;
       a.A_hi = Wh + wofs[sI];
       a.A_lo = Wl + wofs[sI];
@@ -957,11 +962,11 @@ void gap_fast_backward(rgpu_gap_model * m, rgpu_structures * s, double * F_d, do
       a.B_lo = m->Ttl.as<__nv_bfloat16>() + m->tt_off[sI];
       a.ldb = g.Mpad;
       a.epilogue = 0;
-      a.C = s->dX32.as<float>() + size_t(row0) * fd.Dpad;
-      a.ldc = fd.Dpad;
+      a.C = s->dX32.as<float>() + size_t(row0) * fd.Dg;
+      a.ldc = fd.Dg;
       bwd.push_back(a);
     } else if (rows > 0) {
-      launch_fill_f32(s->dX32.as<float>() + size_t(row0) * fd.Dpad, rows * fd.Dpad, 0.f, st);
+      launch_fill_f32(s->dX32.as<float>() + size_t(row0) * fd.Dg, rows * fd.Dg, 0.f, st);
     }
     row0 += rows;
   }
@@ -2160,20 +2165,18 @@ rgpu_status rgpu_get_features(const rgpu_calculator * calc, const rgpu_structure
     } else {
       // FP32 expansion rows are padded ([S*n][row_stride(L)])
       const size_t rs = size_t(row_stride(fd.L));
-      std::vector<float> tmp(ps ? dense.size() : size_t(nc) * fd.S * fd.n * rs);
+      std::vector<float> tmp(ps ? size_t(nc) * fd.Dg : size_t(nc) * fd.S * fd.n * rs);
       const void * src = ps ? s->X32.p : s->C32.p;
       RGPU_CUDA(cudaMemcpyAsync(tmp.data(), src, sizeof(float) * tmp.size(), cudaMemcpyDeviceToHost, s->st));
       RGPU_CUDA(cudaStreamSynchronize(s->st));
       if (ps) {
-        // FP32 rows hold the unnormalised p in the fast column order: scale
-        // by 1/|p| and map back to the reference's column order
+        // FP32 rows hold the unnormalised p in the packed layout: scale by
+        // 1/|p| and unfold into the reference's column order
         std::vector<float> scale(nc);
-        RGPU_CUDA(cudaMemcpy(scale.data(), s->xscale32.p, sizeof(float) * nc, cudaMemcpyDeviceToHost));
-        std::vector<int> fcol(fd.D);
-        for (int d = 0; d < fd.D; ++d) fcol[d] = fast_column(fd, d);
+        RGPU_CUDA(cudaMemcpyAsync(scale.data(), s->xscale32.p, sizeof(float) * nc, cudaMemcpyDeviceToHost, s->st));
+        RGPU_CUDA(cudaStreamSynchronize(s->st));
         for (int64_t r = 0; r < nc; ++r)
-          for (int d = 0; d < fd.D; ++d)
-            dense[size_t(r) * row_len + d] = double(tmp[size_t(r) * row_len + fcol[d]] * scale[r]);
+          unpack_to_reference(fd, &tmp[size_t(r) * fd.Dg], scale[r], &dense[size_t(r) * row_len]);
       } else {
         for (int64_t r = 0; r < nc; ++r)
           for (int row = 0; row < fd.S * fd.n; ++row)
@@ -2406,6 +2409,28 @@ static PerDevice<DebugGemmBuffers> g_debug_gemm_buffers;
 
 rgpu_status rgpu_debug_set_gemm_wait_limit(int64_t polls) {
   return guard([&] { set_gemm_wait_limit(polls); });
+}
+
+rgpu_status rgpu_debug_packed_layout(int32_t S, int32_t max_radial, int32_t max_angular, int64_t * D, int64_t * Dg,
+                                     const double * ref, double * packed, double * unpacked) {
+  return guard([&] {
+    if (S < 1 || S > kMaxSpecies || max_radial < 1 || max_angular < 0 || max_angular > kMaxL)
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "bad layout shape");
+    Hypers hy;
+    hy.max_radial = max_radial;
+    hy.max_angular = max_angular;
+    const FeatureDims fd = make_dims(hy, S);
+    if (D) *D = fd.D;
+    if (Dg) *Dg = fd.Dg;
+    if (!ref) return;
+    std::vector<double> pk(fd.Dg);
+    pack_reference_row(fd, ref, pk.data());
+    if (packed) std::copy(pk.begin(), pk.end(), packed);
+    if (unpacked) {
+      std::vector<float> pf(pk.begin(), pk.end());
+      unpack_to_reference(fd, pf.data(), 1.f, unpacked);
+    }
+  });
 }
 
 rgpu_status rgpu_debug_gemm_bf16x3(int mode, int64_t M, int64_t N, int64_t K, const float * A, const float * B,

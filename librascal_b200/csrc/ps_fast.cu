@@ -1,14 +1,16 @@
-// Power spectrum, FP32 fast path: forward (the unnormalised p as a BF16
-// hi/lo split for the tensor-core GEMMs, plus 1/|p| per row, which the GEMM
-// epilogue and the backward apply) and the adjoint dE/dx -> dE/dc.
+// Power spectrum, FP32 fast path: forward (the unnormalised p in the packed
+// layout of rgpu_internal.h, as a BF16 hi/lo split for the tensor-core
+// GEMMs, plus 1/|p| per row, which the GEMM epilogue and the backward apply)
+// and the adjoint dE/dx -> dE/dc.
 //
 // Same contractions as powerspectrum.cu (calculator_spherical_invariants.hh:
 // 747-794 forward, 588-652 and 796-921 for the gradient it replaces), laid
 // out for the SIMT pipes: the centre's coefficients sit in shared memory as
 // [species][n][l-block padded to a multiple of 4], so every length-(2l+1)
-// product over m is a few 16-byte loads; work items are ordered with l
-// slowest, so a warp shares l (uniform trip counts, broadcast loads) and the
-// dot products are unrolled per l.
+// product over m is a few 16-byte loads, and l is a compile-time constant
+// in every inner loop. The packed layout keeps one entry per symmetric pair
+// of same-species Gram entries, so both kernels touch S n(n-1)/2 (L+1)
+// fewer columns than the reference's layout holds.
 #include <algorithm>
 
 #include <cuda_bf16.h>
@@ -24,160 +26,114 @@ constexpr int kBwdThreads = 320;  // 16 column groups x 20 row pairs at L = 6, S
 constexpr int kMaxN = 16;  // largest max_radial of the FP32 backward
 constexpr float kSqrt2f = 1.41421356237309504880f;
 
-struct Keys {
-  int8_t ka[kMaxSpecies * (kMaxSpecies + 1) / 2];
-  int8_t kb[kMaxSpecies * (kMaxSpecies + 1) / 2];
-  int16_t kid[kMaxSpecies][kMaxSpecies];
-};
-__device__ __forceinline__ void make_keys(Keys & t, int S) {
-  if (threadIdx.x == 0) {
-    int k = 0;
-    for (int a = 0; a < S; ++a)
-      for (int b = a; b < S; ++b) {
-        t.ka[k] = int8_t(a);
-        t.kb[k] = int8_t(b);
-        t.kid[a][b] = t.kid[b][a] = int16_t(k);
-        ++k;
-      }
-  }
-}
-
+// Sum over the block, one barrier: every warp posts its partial sum, then
+// every thread adds the posts. `red` may be written again only after
+// another barrier.
 __device__ __forceinline__ float block_sum_f(float v, float * red) {
   v = warp_sum(v);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
   __syncthreads();
-  if (lane == 0) red[wid] = v;
-  __syncthreads();
-  float t = (threadIdx.x < blockDim.x / 32) ? red[threadIdx.x] : 0.f;
-  if (wid == 0) t = warp_sum(t);
-  if (threadIdx.x == 0) red[0] = t;
-  __syncthreads();
-  return red[0];
+  float t = 0.f;
+  for (int w = 0; w < int(blockDim.x >> 5); ++w) t += red[w];
+  return t;
 }
 
-// Copy c^i, already in the padded row layout [S*n][row_stride(L)] of the
-// FP32 expansion, into shared memory. Starts with a barrier so that tables
-// the block wrote before are visible afterwards.
-template <int L>
-__device__ __forceinline__ void load_padded(const float * __restrict__ Ci, float * Cp, int S, int n) {
-  constexpr int RS = row_stride(L);
-  __syncthreads();
-  const float4 * src = reinterpret_cast<const float4 *>(Ci);
-  float4 * dst = reinterpret_cast<float4 *>(Cp);
-  for (int e = threadIdx.x; e < S * n * (RS / 4); e += blockDim.x) dst[e] = __ldg(src + e);
+__device__ __forceinline__ uint32_t smem_addr(const void * p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only), and its
+// group commit / wait.
+__device__ __forceinline__ void cp_async16(void * smem, const void * gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+// Bulk prefetch of `bytes` (a multiple of 16, 16-byte aligned) into L2.
+__device__ __forceinline__ void prefetch_l2(const void * p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-template <int Q>
-__device__ __forceinline__ float dot4(const float4 * a, const float * b) {
-  const float4 * b4 = reinterpret_cast<const float4 *>(b);
-  float s = 0.f;
+// One 2 x 2 tile (i, j), i <= j, of the packed l-block: G_l over rows
+// 2i, 2i+1 and columns 2j, 2j+1, scaled by lf (sqrt2 lf off the diagonal),
+// the entry below the diagonal of a diagonal tile and rows or columns beyond
+// S n zero, stored as 4 consecutive columns (8 bytes of BF16 hi, 8 of lo,
+// 16 of FP32 when X is given). Returns the tile's sum of squares.
+template <int L, int l>
+__device__ __forceinline__ float fwd_tile(const float * Cp, int Sn, int i, int j, float * __restrict__ X,
+                                          __nv_bfloat16 * __restrict__ hr, __nv_bfloat16 * __restrict__ lr) {
+  constexpr int RS = row_stride(L), Q = pad4(2 * l + 1) / 4, O = offp(l);
+  const float lf = rsqrtf(float(2 * l + 1)), lf2 = lf * kSqrt2f;
+  const int I0 = 2 * i, J0 = 2 * j;
+  const bool i1 = I0 + 1 < Sn, j1 = J0 + 1 < Sn;
+  // Lanes with consecutive i read rows 2i apart; taking row 2i + 1 first when
+  // bit 2 of i is set spreads the 8 lanes of a 16-byte load phase over 8
+  // different bank groups (the row stride is an odd number of 16-byte units).
+  const int sw = (i >> 2) & 1 & int(i1);
+  const float4 * a0 = reinterpret_cast<const float4 *>(Cp + (I0 + sw) * RS + O);
+  const float4 * a1 = reinterpret_cast<const float4 *>(Cp + (i1 ? I0 + 1 - sw : I0) * RS + O);
+  const float4 * b0 = reinterpret_cast<const float4 *>(Cp + J0 * RS + O);
+  const float4 * b1 = reinterpret_cast<const float4 *>(Cp + (j1 ? J0 + 1 : J0) * RS + O);
+  float u00 = 0.f, u10 = 0.f, u01 = 0.f, u11 = 0.f;  // u_rc: row a_r, column J0 + c
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
-    const float4 y = b4[q];
-    s += a[q].x * y.x + a[q].y * y.y + a[q].z * y.z + a[q].w * y.w;
+    const float4 x0 = a0[q], x1 = a1[q], y0 = b0[q], y1 = b1[q];
+    u00 += x0.x * y0.x + x0.y * y0.y + x0.z * y0.z + x0.w * y0.w;
+    u10 += x1.x * y0.x + x1.y * y0.y + x1.z * y0.z + x1.w * y0.w;
+    u01 += x0.x * y1.x + x0.y * y1.y + x0.z * y1.z + x0.w * y1.w;
+    u11 += x1.x * y1.x + x1.y * y1.y + x1.z * y1.z + x1.w * y1.w;
   }
-  return s;
+  // v_rc: row I0 + r, column J0 + c
+  float v00 = sw ? u10 : u00, v10 = sw ? u00 : u10, v01 = sw ? u11 : u01, v11 = sw ? u01 : u11;
+  const bool diag = i == j;
+  v00 *= diag ? lf : lf2;
+  v10 = (diag || !i1) ? 0.f : v10 * lf2;
+  v01 = j1 ? v01 * lf2 : 0.f;
+  v11 = (i1 && j1) ? v11 * (diag ? lf : lf2) : 0.f;
+  const __nv_bfloat162 h0 = __floats2bfloat162_rn(v00, v10), h1 = __floats2bfloat162_rn(v01, v11);
+  const float2 f0 = __bfloat1622float2(h0), f1 = __bfloat1622float2(h1);
+  const __nv_bfloat162 l0 = __floats2bfloat162_rn(v00 - f0.x, v10 - f0.y);
+  const __nv_bfloat162 l1 = __floats2bfloat162_rn(v01 - f1.x, v11 - f1.y);
+  uint2 hw, lw;
+  hw.x = *reinterpret_cast<const uint32_t *>(&h0);
+  hw.y = *reinterpret_cast<const uint32_t *>(&h1);
+  lw.x = *reinterpret_cast<const uint32_t *>(&l0);
+  lw.y = *reinterpret_cast<const uint32_t *>(&l1);
+  *reinterpret_cast<uint2 *>(hr) = hw;
+  *reinterpret_cast<uint2 *>(lr) = lw;
+  if (X) *reinterpret_cast<float4 *>(X) = make_float4(v00, v10, v01, v11);
+  return v00 * v00 + v10 * v10 + v01 * v01 + v11 * v11;
 }
 
-// Output (key, n1, n2, l) is column key * n^2 + out of the row, with
-// out = l * P * n^2 + n2 * n + n1 (the fast column order): the 32 lanes of a
-// warp (consecutive n1, n2) store 32 consecutive columns for every key.
-// Values are the unnormalised p; the row's 1/|p| is applied by the consumers.
+// Every tile of l-block l of the row (tile r at columns l Bp + 4r; the task
+// table gives its (i, j)), then the blocks above l; returns their sum of
+// squares.
 template <int L, int l>
-__device__ __forceinline__ float fwd_task(const float * Cp, const Keys & kt, int S, int n, int n1, int n2,
-                                          int kstride, int out, float * __restrict__ X,
-                                          __nv_bfloat16 * __restrict__ Xh, __nv_bfloat16 * __restrict__ Xl) {
-  constexpr int RS = row_stride(L), Q = pad4(2 * l + 1) / 4, O = offp(l);
-  const float lf = rsqrtf(float(2 * l + 1));
-  float ss = 0.f;
-  for (int sa = 0; sa < S; ++sa) {
-    float4 c1[Q];
-    const float4 * p1 = reinterpret_cast<const float4 *>(Cp + (sa * n + n1) * RS + O);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) c1[q] = p1[q];
-    for (int sb = sa; sb < S; ++sb) {
-      float v = dot4<Q>(c1, Cp + (sb * n + n2) * RS + O) * lf;
-      if (sa < sb) v *= kSqrt2f;
-      const int pos = kt.kid[sa][sb] * kstride + out;
-      const __nv_bfloat16 h = __float2bfloat16_rn(v);
-      Xh[pos] = h;
-      Xl[pos] = __float2bfloat16_rn(v - __bfloat162float(h));
-      if (X) X[pos] = v;
-      ss += v * v;
-    }
-  }
-  return ss;
-}
-
-template <int L, int l>
-__device__ __forceinline__ float fwd_dispatch(int lrt, const float * Cp, const Keys & kt, int S, int n, int n1,
-                                              int n2, int kstride, int out, float * X, __nv_bfloat16 * Xh,
-                                              __nv_bfloat16 * Xl) {
+__device__ __forceinline__ float fwd_blocks(const float * Cp, int Sn, int Bp, int nt, const uint16_t * tiles,
+                                            float * X, __nv_bfloat16 * hr, __nv_bfloat16 * lr) {
   if constexpr (l > L) {
     return 0.f;
   } else {
-    if (lrt == l) return fwd_task<L, l>(Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
-    return fwd_dispatch<L, l + 1>(lrt, Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
-  }
-}
-
-// Two consecutive radial indices n1, n1+1 (n1 even) of one (l, n2): each
-// c_b load feeds both dot products, and the two outputs are consecutive
-// columns, stored as packed bf16 pairs (4-byte stores).
-template <int L, int l>
-__device__ __forceinline__ float fwd_task2(const float * Cp, const Keys & kt, int S, int n, int n1, int n2,
-                                           int kstride, int out, float * __restrict__ X,
-                                           __nv_bfloat16 * __restrict__ Xh, __nv_bfloat16 * __restrict__ Xl) {
-  constexpr int RS = row_stride(L), Q = pad4(2 * l + 1) / 4, O = offp(l);
-  const float lf = rsqrtf(float(2 * l + 1));
-  float ss = 0.f;
-  for (int sa = 0; sa < S; ++sa) {
-    float4 ca[Q], cb[Q];
-    const float4 * pa = reinterpret_cast<const float4 *>(Cp + (sa * n + n1) * RS + O);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) {
-      ca[q] = pa[q];
-      cb[q] = pa[q + RS / 4];
+    float ss = 0.f;
+    for (int r = threadIdx.x; r < nt; r += blockDim.x) {
+      const uint32_t ij = tiles[r];
+      const int o = l * Bp + 4 * r;
+      ss += fwd_tile<L, l>(Cp, Sn, int(ij & 0xFFu), int(ij >> 8), X ? X + o : nullptr, hr + o, lr + o);
     }
-    for (int sb = sa; sb < S; ++sb) {
-      const float4 * p2 = reinterpret_cast<const float4 *>(Cp + (sb * n + n2) * RS + O);
-      float va = 0.f, vb = 0.f;
-#pragma unroll
-      for (int q = 0; q < Q; ++q) {
-        const float4 y = p2[q];
-        va += ca[q].x * y.x + ca[q].y * y.y + ca[q].z * y.z + ca[q].w * y.w;
-        vb += cb[q].x * y.x + cb[q].y * y.y + cb[q].z * y.z + cb[q].w * y.w;
-      }
-      const float sc = (sa < sb) ? lf * kSqrt2f : lf;
-      va *= sc;
-      vb *= sc;
-      const int pos = kt.kid[sa][sb] * kstride + out;
-      const __nv_bfloat162 hh = __floats2bfloat162_rn(va, vb);
-      const float2 hf = __bfloat1622float2(hh);
-      *reinterpret_cast<__nv_bfloat162 *>(Xh + pos) = hh;
-      *reinterpret_cast<__nv_bfloat162 *>(Xl + pos) = __floats2bfloat162_rn(va - hf.x, vb - hf.y);
-      if (X) *reinterpret_cast<float2 *>(X + pos) = make_float2(va, vb);
-      ss += va * va + vb * vb;
-    }
-  }
-  return ss;
-}
-
-template <int L, int l>
-__device__ __forceinline__ float fwd_dispatch2(int lrt, const float * Cp, const Keys & kt, int S, int n, int n1,
-                                               int n2, int kstride, int out, float * X, __nv_bfloat16 * Xh,
-                                               __nv_bfloat16 * Xl) {
-  if constexpr (l > L) {
-    return 0.f;
-  } else {
-    if (lrt == l) return fwd_task2<L, l>(Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
-    return fwd_dispatch2<L, l + 1>(lrt, Cp, kt, S, n, n1, n2, kstride, out, X, Xh, Xl);
+    return ss + fwd_blocks<L, l + 1>(Cp, Sn, Bp, nt, tiles, X, hr, lr);
   }
 }
 
-// p of a centre's row as a BF16 hi/lo split (and in FP32 when X is given),
-// straight from the dot products to HBM, and the row's scale 1/|p| (1
-// without normalisation). Persistent: each block loops over centres.
+// p of a centre's row in the packed layout as a BF16 hi/lo split (and in
+// FP32 when X is given), one 2 x 2 tile per task straight to HBM, and the
+// row's scale 1/|p| (1 without normalisation); the packed values keep |p|.
+// The block walks the l-blocks in turn (l a compile-time constant in each
+// loop); consecutive lanes take consecutive tiles (mostly of one column
+// pair, whose coefficient rows they then read as broadcasts). Persistent:
+// each block loops over centres, prefetching the next centre's coefficient
+// tile with cp.async while it works on the current one.
 template <int L>
 __global__ void __launch_bounds__(kThreads)
 ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X,
@@ -186,281 +142,245 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
   constexpr int L1 = L + 1, RS = row_stride(L);
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
-  const int n = fd.n, S = fd.S, nn2 = n * n, blk = nn2 * L1;
-  float * Cp = smf;  // [S*n][RS]
-  __shared__ Keys kt;
+  const int Sn = fd.Sn, Bp = fd.Bp, tile = Sn * RS;
+  float * cbuf = smf;  // two coefficient tiles [Sn][RS]
+  uint16_t * tiles = reinterpret_cast<uint16_t *>(smf + 2 * tile);  // i | j << 8 of each task
   __shared__ float red[32];
-  make_keys(kt, S);
-  const bool paired = (n % 2) == 0;
-  const int half = n / 2;
-  for (int64_t ci = blockIdx.x; ci < a.n_centers; ci += gridDim.x) {
+  const int np = (Sn + 1) >> 1, nt = np * (np + 1) / 2;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    int j = int((sqrtf(8.f * float(t) + 1.f) - 1.f) * 0.5f);
+    while (j > 0 && j * (j + 1) / 2 > t) --j;
+    while ((j + 1) * (j + 2) / 2 <= t) ++j;
+    tiles[t] = uint16_t((t - j * (j + 1) / 2) | (j << 8));
+  }
+  // zero columns: the end of every l-block after its tiles, then the row's tail
+  const int padb = Bp - 4 * nt, tail = fd.Dg - L1 * Bp;
+  auto prefetch = [&](int64_t c, float * dst) {
+    const float4 * src = reinterpret_cast<const float4 *>(C + size_t(c) * tile);
+    for (int e = threadIdx.x; e < tile / 4; e += blockDim.x) cp_async16(dst + 4 * e, src + e);
+  };
+  int64_t ci = blockIdx.x;
+  if (ci < a.n_centers) prefetch(ci, cbuf);
+  cp_async_commit();
+  for (int buf = 0; ci < a.n_centers; ci += gridDim.x, buf ^= 1) {
+    const int64_t next = ci + gridDim.x;
+    if (next < a.n_centers) prefetch(next, cbuf + (buf ^ 1) * tile);
+    cp_async_commit();
+    cp_async_wait<1>();  // this centre's copies (and the task table) are done ...
+    __syncthreads();     // ... for every thread
+    const float * Cp = cbuf + buf * tile;
     const int64_t row = a.row_of_center[ci];
-    load_padded<L>(C + size_t(ci) * S * n * RS, Cp, S, n);
-    __syncthreads();
-    const size_t roff = size_t(row) * fd.Dpad;
+    const size_t roff = size_t(row) * fd.Dg;
     float * Xr = X ? X + roff : nullptr;
     __nv_bfloat16 * hr = Xh + roff;
     __nv_bfloat16 * lr = Xl + roff;
-    float ss = 0.f;
-    if (paired) {
-      // tasks (l, n2, n1 pair): consecutive lanes store consecutive pairs
-      for (int t = threadIdx.x; t < L1 * n * half; t += blockDim.x) {
-        const int l = t / (n * half);
-        const int r = t - l * (n * half);
-        const int n2 = r / half, n1 = 2 * (r - n2 * half);
-        ss += fwd_dispatch2<L, 0>(l, Cp, kt, S, n, n1, n2, nn2, l * fd.P * nn2 + n2 * n + n1, Xr, hr, lr);
+    float ss = fwd_blocks<L, 0>(Cp, Sn, Bp, nt, tiles, Xr, hr, lr);
+    for (int e = threadIdx.x; e < L1 * padb + tail; e += blockDim.x) {
+      int d;
+      if (e < L1 * padb) {
+        const int l = e / padb;
+        d = l * Bp + 4 * nt + (e - l * padb);
+      } else {
+        d = L1 * Bp + (e - L1 * padb);
       }
-    } else {
-      for (int t = threadIdx.x; t < blk; t += blockDim.x) {
-        const int l = t / nn2;
-        const int r = t - l * nn2;
-        const int n2 = r / n, n1 = r - n2 * n;  // consecutive lanes: consecutive n1 and columns
-        ss += fwd_dispatch<L, 0>(l, Cp, kt, S, n, n1, n2, nn2, l * fd.P * nn2 + r, Xr, hr, lr);
-      }
-    }
-    for (int d = fd.D + threadIdx.x; d < fd.Dpad; d += blockDim.x) {
       hr[d] = __float2bfloat16_rn(0.f);
       lr[d] = __float2bfloat16_rn(0.f);
       if (Xr) Xr[d] = 0.f;
     }
-    ss = block_sum_f(ss, red);  // ends with a barrier: Cp may be refilled
+    ss = block_sum_f(ss, red);  // its barrier follows every tile: this buffer may be refilled
     if (threadIdx.x == 0) {
       const float nrm = sqrtf(ss);
       row_scale[row] = (a.normalize && nrm > 0.f) ? 1.f / nrm : 1.f;
     }
   }
+  cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------- backward
-// Quotient x / d for a runtime divisor d >= 1, exact whenever x * d < 2^32
-// (multiply by the rounded-up reciprocal 2^32 / d).
-struct FastDiv {
-  uint32_t d, m;
-  FastDiv() = default;
-  __host__ __device__ explicit FastDiv(uint32_t dd) : d(dd), m(dd > 1 ? 0xFFFFFFFFu / dd + 1u : 0u) {}
-  __device__ __forceinline__ uint32_t div(uint32_t x) const { return d > 1 ? __umulhi(x, m) : x; }
-};
-
-struct BwdShape {
-  FastDiv n, P, npair, Snp;  // n, key count, n(n-1)/2, S n(n-1)/2
-  int SnP;                   // row stride of H_l: S n rounded up to even
-  int LS;                    // floats per H_l block in shared memory
-  bool vec;                  // n and S n multiples of 4: 16-byte stores of 4 n1
-};
-
-// One CTA per centre. The projected gradient G = (g - x (x.g)) / |p| (x as
-// BF16 hi + lo, g = dE/dx, both in the fast column order) is formed in two
-// passes over the row: the first reduces x.g, the second (an L2 re-read)
-// scatters G into the symmetric matrices
-//   H_l[(a n1)][(b n2)] = s_ab G_(ab)(n1 n2 l)   (a < b, both triangles)
-//   H_l[(a n1)][(a n2)] = G(n1 n2 l) + G(n2 n1 l)
-// then each thread computes one (l, row) of dE/dc = lf_l H_l c_l.
+// Per centre: the projected gradient G = (g - x (x.g)) / |p| of the packed
+// row (x as BF16 hi + lo, g = dE/dx) is formed in shared memory in two
+// passes (the first stores g and reduces x.g, the second, an L2 re-read of
+// x, projects in place), then dE/dc = lf_l H_l c_l with the symmetric
+//   H_l[I][J] = sqrt2 G_l(I J)  (I != J),   H_l[I][I] = 2 G_l(I I),
+// the derivative of E through the packed entries sqrt2 G_l[I][J] (I < J) and
+// G_l[I][I] of the Gram matrix, read straight from the packed tiles: tile
+// (i, j), i <= j, holds rows 2i, 2i+1 and columns 2j, 2j+1.
+//
+// Contraction tasks are (row pair 2ip, 2ip+1; 4-wide column group g of the
+// padded coefficient rows) with g fastest, so the lanes of a half-warp share
+// their rows (one broadcast 16-byte load per tile, uniform trip counts) and
+// read consecutive 16-byte chunks of a coefficient row. The centre's dE/dc
+// rows are staged in shared memory with an odd row stride and stored
+// coalesced. The next centre's coefficients are copied in with cp.async, and
+// its x and dE/dx rows prefetched into L2, while this one is worked on.
 template <int L>
 __global__ void __launch_bounds__(kBwdThreads, 4)
-ps_bwd_f32_kernel(PsArgs a, BwdShape bs, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
+ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
                   const __nv_bfloat16 * __restrict__ Xl, const float * __restrict__ row_scale,
                   const float * __restrict__ dX, float * __restrict__ dC) {
   constexpr int L1 = L + 1, RS = row_stride(L), K = L1 * L1;
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
-  const int n = fd.n, S = fd.S, Sn = S * n, SnP = bs.SnP, LS = bs.LS, P = fd.P;
-  float * Cp = smf;             // [Sn][RS]
-  float * Hs = Cp + Sn * RS;    // H_l[j][i] at l*LS + j*SnP + i
-  __shared__ Keys kt;
+  const int Sn = fd.Sn, Bp = fd.Bp, OS = Sn | 1;
+  const int tile = Sn * RS, tileP = (Sn + (Sn & 1)) * RS;  // a coefficient tile; its buffer
+  float * Cb = smf;                // two coefficient buffers [Sn rounded up to even][RS]
+  float * Ts = Cb + 2 * tileP;     // packed G: L1 blocks of Bp
+  float * Os = Ts + L1 * Bp;       // dE/dc of the centre: [K][OS]
   __shared__ float red[32];
-  __shared__ int8_t pair_n1[kMaxN * (kMaxN - 1) / 2], pair_n2[kMaxN * (kMaxN - 1) / 2];
-  // column groups of the contraction: every 4-wide chunk q of every padded
-  // l-block, l descending; group g covers padded columns grp_off[g] + 0..3
+  // column groups of the contraction: the 4-wide chunks of the padded
+  // coefficient row in order (group g covers columns 4g .. 4g+3, of block
+  // l = grp_l[g]), so the 8 lanes of a 16-byte load phase read 8 consecutive
+  // chunks of one row
   constexpr int kG = offp(L + 1) / 4;
   __shared__ int8_t grp_l[kG];
-  __shared__ int16_t grp_off[kG];
   for (int t = threadIdx.x; t < kG; t += blockDim.x) {
-    int g = t, l = L;
-    while (g >= pad4(2 * l + 1) / 4) {
-      g -= pad4(2 * l + 1) / 4;
-      --l;
-    }
+    int l = 0;
+    while (offp_rt(l + 1) <= 4 * t) ++l;
     grp_l[t] = int8_t(l);
-    grp_off[t] = int16_t(offp_rt(l) + 4 * g);
   }
-  make_keys(kt, S);
-  for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
-    const int n1 = t / n, n2 = t - n1 * n;
-    if (n1 < n2) {
-      const int p = n1 * (2 * n - n1 - 1) / 2 + (n2 - n1 - 1);
-      pair_n1[p] = int8_t(n1);
-      pair_n2[p] = int8_t(n2);
-    }
-  }
+  // the row after an odd S n's last row stays zero in both buffers
+  for (int e = tile + threadIdx.x; e < tileP; e += blockDim.x) Cb[e] = Cb[tileP + e] = 0.f;
+  const int nq = (L1 * Bp) >> 2;  // 4-column chunks holding packed entries (the rest of the row is zero)
+  const int NP = (Sn + 1) >> 1;
+  float4 * T4 = reinterpret_cast<float4 *>(Ts);
+  auto prefetch = [&](int64_t c, float * dst) {
+    const float4 * src = reinterpret_cast<const float4 *>(C + size_t(c) * tile);
+    for (int e = threadIdx.x; e < tile / 4; e += blockDim.x) cp_async16(dst + 4 * e, src + e);
+  };
+  int64_t ci = blockIdx.x;
+  if (ci < a.n_centers) prefetch(ci, Cb);
+  cp_async_commit();
   // persistent: the tables above serve every centre of this block
-  for (int64_t ci = blockIdx.x; ci < a.n_centers; ci += gridDim.x) {
-  const int64_t row = a.row_of_center[ci];
-  load_padded<L>(C + size_t(ci) * S * n * RS, Cp, S, n);
-  const uint2 * xh = reinterpret_cast<const uint2 *>(Xh + size_t(row) * fd.Dpad);
-  const uint2 * xl = reinterpret_cast<const uint2 *>(Xl + size_t(row) * fd.Dpad);
-  const float4 * g4 = reinterpret_cast<const float4 *>(dX + size_t(row) * fd.Dpad);
-  const int nq = (fd.D + 3) >> 2;
-  const float rs = row_scale[row];  // x = rs * p; G = rs * (g - x (x.g))
-  float dot = 0.f;
-  if (a.normalize) {
-    for (int c = threadIdx.x; c < nq; c += blockDim.x) {
-      const uint2 hv = xh[c], lv = xl[c];
-      const float4 gq = g4[c];
-      const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
-      const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
-      dot += (__bfloat162float(hb[0]) + __bfloat162float(lb[0])) * gq.x;
-      dot += (__bfloat162float(hb[1]) + __bfloat162float(lb[1])) * gq.y;
-      dot += (__bfloat162float(hb[2]) + __bfloat162float(lb[2])) * gq.z;
-      dot += (__bfloat162float(hb[3]) + __bfloat162float(lb[3])) * gq.w;
-    }
-    dot = block_sum_f(dot, red) * rs;  // padding columns are zero in p and g
-  }
-  for (int c = threadIdx.x; c < nq; c += blockDim.x) {
-    const uint2 hv = __ldcs(xh + c), lv = __ldcs(xl + c);
-    const float4 gq = __ldcs(g4 + c);
-    const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
-    const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
-    const float gv[4] = {gq.x, gq.y, gq.z, gq.w};
-    float G[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) G[e] = (gv[e] - (__bfloat162float(hb[e]) + __bfloat162float(lb[e])) * rs * dot) * rs;
-    // decode the first column of the chunk: ((l*P + key)*n + n2)*n + n1
-    const uint32_t d0 = 4u * uint32_t(c);
-    const uint32_t q1 = bs.n.div(d0);
-    int n1 = int(d0 - q1 * bs.n.d);
-    const uint32_t q2 = bs.n.div(q1);
-    int n2 = int(q1 - q2 * bs.n.d);
-    const uint32_t q3 = bs.P.div(q2);
-    int key = int(q2 - q3 * bs.P.d);
-    int l = int(q3);
-    if (bs.vec) {
-      // the 4 columns share (l, key, n2) and n1 % 4 == 0: one 16-byte store
-      // for H[(b n2)][(a n1..n1+3)], four for the mirrored column
-      const int sa = kt.ka[key], sb = kt.kb[key];
-      const int i = sa * n + n1, j = sb * n + n2;
-      float * Hl = Hs + l * LS;
-      if (sa != sb) {
-        float v[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) v[e] = kSqrt2f * G[e];
-        *reinterpret_cast<float4 *>(Hl + j * SnP + i) = make_float4(v[0], v[1], v[2], v[3]);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) Hl[(i + e) * SnP + j] = v[e];
-      } else {
-        float v[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) v[e] = (n1 + e == n2) ? 2.f * G[e] : G[e];
-        *reinterpret_cast<float4 *>(Hl + j * SnP + i) = make_float4(v[0], v[1], v[2], v[3]);
+  for (int buf = 0; ci < a.n_centers; ci += gridDim.x, buf ^= 1) {
+    const int64_t next = ci + gridDim.x;
+    if (next < a.n_centers) {
+      prefetch(next, Cb + (buf ^ 1) * tileP);
+      if (threadIdx.x == 0) {  // and the next centre's x and dE/dx rows into L2
+        const size_t nrow = size_t(a.row_of_center[next]) * fd.Dg;
+        prefetch_l2(Xh + nrow, uint32_t(fd.Dg) * 2u);
+        prefetch_l2(Xl + nrow, uint32_t(fd.Dg) * 2u);
+        prefetch_l2(dX + nrow, uint32_t(fd.Dg) * 4u);
       }
-    } else {
+    }
+    cp_async_commit();
+    const float * Cp = Cb + buf * tileP;
+    const int64_t row = a.row_of_center[ci];
+    const uint2 * xh = reinterpret_cast<const uint2 *>(Xh + size_t(row) * fd.Dg);
+    const uint2 * xl = reinterpret_cast<const uint2 *>(Xl + size_t(row) * fd.Dg);
+    const float4 * g4 = reinterpret_cast<const float4 *>(dX + size_t(row) * fd.Dg);
+    const float rs = row_scale[row];  // x = rs * p; G = rs * (g - x (x.g))
+    float dot = 0.f;
+#pragma unroll 4
+    for (int c = threadIdx.x; c < nq; c += blockDim.x) {
+      const float4 gq = __ldcs(g4 + c);
+      T4[c] = gq;
+      if (a.normalize) {
+        const uint2 hv = xh[c], lv = xl[c];
+        const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
+        const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
+        dot += (__bfloat162float(hb[0]) + __bfloat162float(lb[0])) * gq.x;
+        dot += (__bfloat162float(hb[1]) + __bfloat162float(lb[1])) * gq.y;
+        dot += (__bfloat162float(hb[2]) + __bfloat162float(lb[2])) * gq.z;
+        dot += (__bfloat162float(hb[3]) + __bfloat162float(lb[3])) * gq.w;
+      }
+    }
+    if (a.normalize) {
+      dot = block_sum_f(dot, red) * rs;  // padding columns are zero in p and g
+      const float k = rs * dot;
+      // each thread projects the chunks it stored
+#pragma unroll 4
+      for (int c = threadIdx.x; c < nq; c += blockDim.x) {
+        const uint2 hv = __ldcs(xh + c), lv = __ldcs(xl + c);
+        const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
+        const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
+        float4 t = T4[c];
+        t.x = (t.x - (__bfloat162float(hb[0]) + __bfloat162float(lb[0])) * k) * rs;
+        t.y = (t.y - (__bfloat162float(hb[1]) + __bfloat162float(lb[1])) * k) * rs;
+        t.z = (t.z - (__bfloat162float(hb[2]) + __bfloat162float(lb[2])) * k) * rs;
+        t.w = (t.w - (__bfloat162float(hb[3]) + __bfloat162float(lb[3])) * k) * rs;
+        T4[c] = t;
+      }
+    }
+    cp_async_wait<1>();  // this centre's coefficients have landed ...
+    __syncthreads();     // ... for every thread, and G is complete
+    // dE/dc_(i l m) = lf_l sqrt2 (sum_j G(i j) c_(j l m) + (sqrt2 - 1) G(i i) c_(i l m)),
+    // over the tiles of row pair ip: (j, ip) for j < ip (transposed), the
+    // diagonal tile, then (ip, j) for j > ip
+    for (int t = threadIdx.x; t < kG * NP; t += blockDim.x) {
+      const int ip = t / kG, g = t - ip * kG;
+      const int l = grp_l[g];
+      const float4 * Tl = reinterpret_cast<const float4 *>(Ts + l * Bp);
+      const float * cb = Cp + 4 * g;
+      const int i0 = 2 * ip;
+      float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
+      // h_rc = G(i0 + r, J0 + c), cj = row J0 of the coefficients (row S n of
+      // an odd S n is the buffer's zero row, and its h are zero)
+      auto acc = [&](float h00, float h10, float h01, float h11, const float * cj) {
+        const float4 c0 = *reinterpret_cast<const float4 *>(cj);
+        const float4 c1 = *reinterpret_cast<const float4 *>(cj + RS);
+        a0.x += h00 * c0.x + h01 * c1.x;
+        a0.y += h00 * c0.y + h01 * c1.y;
+        a0.z += h00 * c0.z + h01 * c1.z;
+        a0.w += h00 * c0.w + h01 * c1.w;
+        a1.x += h10 * c0.x + h11 * c1.x;
+        a1.y += h10 * c0.y + h11 * c1.y;
+        a1.z += h10 * c0.z + h11 * c1.z;
+        a1.w += h10 * c0.w + h11 * c1.w;
+      };
+      const float4 * tp = Tl + ip * (ip + 1) / 2;  // tile (0, ip)
+      const float * cj = cb;
+#pragma unroll 2
+      for (int j = 0; j < ip; ++j, cj += 2 * RS) {
+        const float4 v = tp[j];  // (2j, i0), (2j+1, i0), (2j, i0+1), (2j+1, i0+1)
+        acc(v.x, v.z, v.y, v.w, cj);
+      }
+      {
+        const float4 v = tp[ip];  // (i0, i0), zero, (i0, i0+1), (i0+1, i0+1)
+        acc(kSqrt2f * v.x, v.z, v.z, kSqrt2f * v.w, cj);
+        cj += 2 * RS;
+      }
+      const float4 * tq = Tl + (ip + 1) * (ip + 2) / 2 + ip;  // tile (ip, ip + 1)
+#pragma unroll 2
+      for (int j = ip + 1; j < NP; ++j, cj += 2 * RS) {
+        const float4 v = *tq;  // (i0, 2j), (i0+1, 2j), (i0, 2j+1), (i0+1, 2j+1)
+        acc(v.x, v.y, v.z, v.w, cj);
+        tq += j + 1;
+      }
+      const int M = 2 * l + 1, m0 = 4 * g - offp_rt(l);
+      const float sc = rsqrtf(float(M)) * kSqrt2f;
+      const float v0[4] = {a0.x, a0.y, a0.z, a0.w}, v1[4] = {a1.x, a1.y, a1.z, a1.w};
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        if (int(d0) + e < fd.D) {
-          const int sa = kt.ka[key], sb = kt.kb[key];
-          const int i = sa * n + n1, j = sb * n + n2;
-          float * Hl = Hs + l * LS;
-          if (sa != sb) {
-            Hl[j * SnP + i] = kSqrt2f * G[e];
-            Hl[i * SnP + j] = kSqrt2f * G[e];
-          } else {
-            Hl[j * SnP + i] = (n1 == n2) ? 2.f * G[e] : G[e];
-          }
-        }
-        if (++n1 == n) {
-          n1 = 0;
-          if (++n2 == n) {
-            n2 = 0;
-            if (++key == P) {
-              key = 0;
-              ++l;
-            }
-          }
+        if (m0 + e < M) {
+          float * o = Os + (l * l + m0 + e) * OS + i0;
+          o[0] = v0[e] * sc;
+          if (i0 + 1 < Sn) o[1] = v1[e] * sc;
         }
       }
     }
+    __syncthreads();
+    // rows lm of the centre's dE/dc, one warp per row (consecutive lanes:
+    // consecutive (species, radial) entries)
+    float * out = dC + size_t(ci) * Sn * K;
+    for (int lm = threadIdx.x >> 5; lm < K; lm += blockDim.x >> 5)
+      for (int i = threadIdx.x & 31; i < Sn; i += 32) out[lm * Sn + i] = Os[lm * OS + i];
   }
-  __syncthreads();
-  // same-species blocks: H[(a n1)][(a n2)] = H[(a n2)][(a n1)] = G(n1 n2) + G(n2 n1)
-  const int nsym = L1 * int(bs.Snp.d);
-  for (int t = threadIdx.x; t < nsym; t += blockDim.x) {
-    const uint32_t l = bs.Snp.div(uint32_t(t));
-    const uint32_t r = uint32_t(t) - l * bs.Snp.d;
-    const uint32_t sa = bs.npair.div(r);
-    const int p = int(r - sa * bs.npair.d);
-    const int i = int(sa) * n + pair_n1[p], j = int(sa) * n + pair_n2[p];
-    float * Hl = Hs + l * LS;
-    const float s = Hl[j * SnP + i] + Hl[i * SnP + j];
-    Hl[j * SnP + i] = s;
-    Hl[i * SnP + j] = s;
-  }
-  __syncthreads();
-  // dE/dc_{i l m} = lf_l sum_j H_l[i][j] c_{j l m}: each task is one pair of
-  // rows (2ip, 2ip+1) and one 4-wide column group (l, q). H_l is read from
-  // the transposed slots H_l[j][2ip..2ip+1] (consecutive lanes: consecutive
-  // 8-byte words), c_j from the broadcast 16-byte chunk of the padded tile.
-  float * out = dC + size_t(ci) * Sn * K;
-  const int NP = (Sn + 1) >> 1;
-  for (int t = threadIdx.x; t < kG * NP; t += blockDim.x) {
-    const int g = t / NP;
-    const int ip = t - g * NP;
-    const int l = grp_l[g];
-    const float * h = Hs + l * LS + 2 * ip;
-    const float * cb = Cp + grp_off[g];
-    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
-#pragma unroll 4
-    for (int j = 0; j < Sn; ++j) {
-      const float2 hv = *reinterpret_cast<const float2 *>(h + j * SnP);
-      const float4 c = *reinterpret_cast<const float4 *>(cb + j * RS);
-      a0.x += hv.x * c.x;
-      a0.y += hv.x * c.y;
-      a0.z += hv.x * c.z;
-      a0.w += hv.x * c.w;
-      a1.x += hv.y * c.x;
-      a1.y += hv.y * c.y;
-      a1.z += hv.y * c.z;
-      a1.w += hv.y * c.w;
-    }
-    const int M = 2 * l + 1, m0 = grp_off[g] - offp_rt(l);
-    const float lf = rsqrtf(float(M));
-    const float v0[4] = {a0.x, a0.y, a0.z, a0.w}, v1[4] = {a1.x, a1.y, a1.z, a1.w};
-    const int i = 2 * ip;
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      if (m0 + e < M) {
-        float * o = out + (l * l + m0 + e) * Sn + i;
-        o[0] = v0[e] * lf;
-        if (i + 1 < Sn) o[1] = v1[e] * lf;
-      }
-    }
-  }
-  }
+  cp_async_wait<0>();
 }
 
+// Shared memory of the forward: two coefficient tiles and the task table.
 template <int L>
 size_t fwd_smem(const FeatureDims & fd) {
-  return sizeof(float) * size_t(fd.S) * fd.n * row_stride(L);
+  const size_t np = size_t(fd.Sn + 1) / 2;
+  return sizeof(float) * 2 * size_t(fd.Sn) * row_stride(L) + sizeof(uint16_t) * np * (np + 1) / 2 + 16;
 }
 
-BwdShape bwd_shape(const FeatureDims & fd) {
-  BwdShape b;
-  const uint32_t n = uint32_t(fd.n), Sn = uint32_t(fd.S) * n, npair = n * (n - 1) / 2;
-  b.n = FastDiv(n);
-  b.P = FastDiv(uint32_t(fd.P));
-  b.npair = FastDiv(npair > 0 ? npair : 1u);
-  b.Snp = FastDiv(npair > 0 ? uint32_t(fd.S) * npair : 1u);
-  if (npair == 0) b.Snp.d = 0;  // no off-diagonal pairs: the symmetrisation loop is empty
-  b.SnP = int(Sn + (Sn & 1u));
-  // a multiple of 4 (16-byte rows) that is not a multiple of 32, so the
-  // L+1 blocks start on different banks
-  b.LS = int((Sn * uint32_t(b.SnP) + 3) / 4 * 4);
-  if (b.LS % 32 == 0) b.LS += 4;
-  b.vec = (n % 4 == 0) && (Sn % 4 == 0);
-  return b;
-}
-
+// Shared memory of the backward: two coefficient buffers, the packed G row
+// and the staged dE/dc rows.
 template <int L>
-size_t bwd_smem(const FeatureDims & fd, const BwdShape & b) {
-  return sizeof(float) * (size_t(fd.S) * fd.n * row_stride(L) + size_t(L + 1) * b.LS);
+size_t bwd_smem(const FeatureDims & fd) {
+  const size_t Sn = size_t(fd.Sn), K = size_t(L + 1) * (L + 1);
+  return sizeof(float) * (2 * (Sn + (Sn & 1)) * row_stride(L) + size_t(L + 1) * fd.Bp + K * (Sn | 1));
 }
 
 // Blocks of a persistent kernel: as many as fit on the device at once (at
@@ -524,19 +444,18 @@ void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 *
                         const float * row_scale, const float * dX, float * dC, cudaStream_t st) {
   if (a.n_centers == 0) return;
   if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
-  const BwdShape bs = bwd_shape(a.fd);
   constexpr size_t kMaxSmem = 227 * 1024 - 2048;
   const int threads = std::min(tile_config(a.fd.S, a.fd.n, a.fd.L).psb_threads, kBwdThreads);
 #define RGPU_PSB_CASE(LL)                                                                                     \
   case LL: {                                                                                                  \
-    const size_t smem = bwd_smem<LL>(a.fd, bs);                                                               \
+    const size_t smem = bwd_smem<LL>(a.fd);                                                                   \
     if (smem > kMaxSmem)                                                                                      \
       throw Error(RGPU_ERR_INVALID_ARGUMENT,                                                                  \
                   "species x max_radial too large for the FP32 power-spectrum backward; use FP64");           \
     RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
     ps_bwd_f32_kernel<LL><<<persistent_grid(ps_bwd_f32_kernel<LL>, threads, smem, a.n_centers),               \
-                            threads, smem, st>>>(a, bs, C, Xh, Xl, row_scale, dX, dC);                        \
+                            threads, smem, st>>>(a, C, Xh, Xl, row_scale, dX, dC);                            \
     break;                                                                                                    \
   }
   switch (a.fd.L) {

@@ -18,10 +18,10 @@
 //   * thread 0 issues the MMAs of l + 1 into one TMEM buffer while the
 //     warps drain l from the other (two 128-column buffers);
 //   * each warp reads its 32 rows (tcgen05.ld, 32 lanes x 4 columns at a
-//     time), keeps the columns of its own centre with b >= a, scales, splits
-//     into BF16 hi/lo and writes the centre's l-block of the output row into
-//     shared memory, from where the block is copied to HBM with 16-byte
-//     stores (in the fast column order the l-block of a row is contiguous);
+//     time), keeps the upper triangle J >= I of its own centre's block,
+//     scales, splits into BF16 hi/lo and writes the centre's packed l-block
+//     (the layout of rgpu_internal.h) into shared memory, from where the
+//     block is copied to HBM with 16-byte stores;
 //   * |p|^2 is summed per centre and 1/|p| stored per row, as the SIMT
 //     forward does.
 // Every mbarrier wait is bounded; a wait that gives up records it in the
@@ -98,7 +98,7 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 struct TcPsPlan {
   int T;         // centres per tile
   int ops;       // bytes of the operand tiles
-  int stage;     // bytes of one staging buffer: T x P n^2 x (hi, lo) BF16
+  int stage;     // bytes of one staging buffer: T x Bp x (hi, lo) BF16
 };
 
 template <int L>
@@ -113,26 +113,21 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ uint32_t tmem_slot;
   __shared__ float nrm_s[kRows];
-  __shared__ int16_t kid[kMaxSpecies][kMaxSpecies];
   const FeatureDims fd = a.fd;
-  const int n = fd.n, S = fd.S, Sn = S * n, P = fd.P, T = plan.T;
-  const int blk = P * n * n;  // one l-block of a row
+  const int n = fd.n, S = fd.S, Sn = S * n, T = plan.T;
+  const int blk = fd.Bp;  // one packed l-block of a row
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    int k = 0;
-    for (int x = 0; x < S; ++x)
-      for (int y = x; y < S; ++y) {
-        kid[x][y] = kid[y][x] = int16_t(k);
-        ++k;
-      }
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
     fence_barrier_init();
   }
   // the operand tiles start at zero: rows beyond T S n and columns beyond
-  // 2l + 1 are never written again
-  for (int e = threadIdx.x; e < plan.ops / 16; e += blockDim.x)
+  // 2l + 1 are never written again; so do the staging buffers, whose zero
+  // entries (below the diagonal of the diagonal tiles, and the l-block
+  // padding) no epilogue writes
+  for (int e = threadIdx.x; e < (plan.ops + 2 * plan.stage) / 16; e += blockDim.x)
     reinterpret_cast<uint4 *>(ops)[e] = make_uint4(0u, 0u, 0u, 0u);
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
@@ -219,14 +214,16 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
             float v[4];
             tmem_ld4(tq + uint32_t(tt * Sn + sb * n + 4 * q), v);
             if (row_ok && tt == my_t && sb >= my_a) {
-              const float sc = sb > my_a ? lf * kSqrt2 : lf;
-              const int base = my_t * blk + (kid[my_a][sb] * n + 4 * q) * n + my_n1;
 #pragma unroll
               for (int e = 0; e < 4; ++e) {
-                const float x = v[e] * sc;
+                const int J = sb * n + 4 * q + e;  // column of the centre's Gram block
+                if (J < my_i) continue;
+                const float x = v[e] * (J > my_i ? lf * kSqrt2 : lf);
+                const int jp = J >> 1;  // packed position of (I, J), 2 x 2 tiles
+                const int idx = my_t * blk + 4 * (jp * (jp + 1) / 2 + (my_i >> 1)) + (my_i & 1) + 2 * (J & 1);
                 const __nv_bfloat16 h = __float2bfloat16_rn(x);
-                sh[base + e * n] = h;
-                sl[base + e * n] = __float2bfloat16_rn(x - __bfloat162float(h));
+                sh[idx] = h;
+                sl[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
                 nrm += x * x;
               }
             }
@@ -235,14 +232,14 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
       }
       tc_fence_before();
       __syncthreads();
-      // the centres' l-blocks: contiguous in their rows (fast column order)
+      // the centres' packed l-blocks: contiguous in their rows
       const int chunks = blk / 8;  // 16-byte chunks of one block
       for (int e = threadIdx.x; e < 2 * nt * chunks; e += blockDim.x) {
         const int half = e / (nt * chunks), rem = e - half * (nt * chunks);
         const int t = rem / chunks, cch = rem - t * chunks;
         const int64_t row = a.row_of_center[c0 + t];
         const uint4 * src = reinterpret_cast<const uint4 *>((half ? sl : sh) + t * blk) + cch;
-        __nv_bfloat16 * dstb = (half ? Xl : Xh) + size_t(row) * fd.Dpad + size_t(l) * blk;
+        __nv_bfloat16 * dstb = (half ? Xl : Xh) + size_t(row) * fd.Dg + size_t(l) * blk;
         reinterpret_cast<uint4 *>(dstb)[cch] = *src;
       }
     }
@@ -255,12 +252,12 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
       row_scale[row] = (a.normalize && nv > 0.f) ? 1.f / nv : 1.f;
     }
     // padding columns of the rows
-    const int padc = fd.Dpad - fd.D;
+    const int used = (L + 1) * blk, padc = fd.Dg - used;
     for (int e = threadIdx.x; e < nt * padc; e += blockDim.x) {
-      const int t = e / padc, c = fd.D + (e - t * padc);
+      const int t = e / padc, c = used + (e - t * padc);
       const int64_t row = a.row_of_center[c0 + t];
-      Xh[size_t(row) * fd.Dpad + c] = __float2bfloat16_rn(0.f);
-      Xl[size_t(row) * fd.Dpad + c] = __float2bfloat16_rn(0.f);
+      Xh[size_t(row) * fd.Dg + c] = __float2bfloat16_rn(0.f);
+      Xl[size_t(row) * fd.Dg + c] = __float2bfloat16_rn(0.f);
     }
     __syncthreads();  // nrm_s and the operands are rewritten by the next tile
   }
@@ -287,7 +284,7 @@ bool ps_fwd_tc_supported(const FeatureDims & fd) {
   if (Sn > kRows || fd.n % 4 != 0 || fd.L > kMaxL) return false;
   const int T = kRows / Sn;
   const size_t ops = size_t(op_off(fd.L + 1));
-  const size_t stage = 2 * size_t(T) * fd.P * fd.n * fd.n * 2 * sizeof(__nv_bfloat16);
+  const size_t stage = 2 * size_t(T) * fd.Bp * 2 * sizeof(__nv_bfloat16);
   return ops + stage + 256 <= size_t(227 * 1024 - 4096);
 }
 
@@ -298,7 +295,7 @@ void launch_ps_fwd_tc(const PsArgs & a, const float * C, __nv_bfloat16 * Xh, __n
   TcPsPlan plan;
   plan.T = kRows / (a.fd.S * a.fd.n);
   plan.ops = op_off(a.fd.L + 1);
-  plan.stage = 2 * plan.T * a.fd.P * a.fd.n * a.fd.n * int(sizeof(__nv_bfloat16));  // hi + lo of one l
+  plan.stage = 2 * plan.T * a.fd.Bp * int(sizeof(__nv_bfloat16));  // hi + lo of one l
   const size_t smem = std::max(kMinSmem, size_t(plan.ops) + 2 * size_t(plan.stage) + 256);
   int dev = 0, sms = 0;
   RGPU_CUDA(cudaGetDevice(&dev));

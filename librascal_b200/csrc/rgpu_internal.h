@@ -195,6 +195,9 @@ struct FeatureDims {
   int P;      // species pairs S(S+1)/2
   int D;      // P*n*n*(L+1)
   int Dpad;   // D rounded up to 32
+  int Sn;     // S*n: rows of a centre's per-l Gram matrix (packed layout below)
+  int Bp;     // columns of one l-block of the packed layout: 2 ceil(Sn/2)(ceil(Sn/2)+1) rounded up to 8
+  int Dg;     // row length of the packed layout: (L+1) Bp rounded up to 32
 };
 
 // RadialScaling cutoff parameters (on = 0: plain shifted cosine).
@@ -233,19 +236,43 @@ void launch_expansion_selfgrad_fp64(const ExpansionArgs & a, int64_t c0, int64_t
                                     int64_t p_base, const double * dCp, double * dCs,
                                     cudaStream_t st);
 
-// Column order of the FP32 fast path's feature rows (x and its BF16 split,
-// dE/dx, and the model's BF16 copies of T): ((l*P + key)*n + n2)*n + n1, the
-// first radial index fastest. The reference's dense order, used by the FP64
-// path and by every export, is ((key*n + n1)*n + n2)*(L+1) + l
-// (property_block_sparse.hh:911-931). A dot product x . t is the same in
-// either order as long as both operands use it.
-inline int fast_column(const FeatureDims & fd, int d_ref) {
-  const int L1 = fd.L + 1, blk = fd.n * fd.n * L1;
-  const int key = d_ref / blk, r = d_ref - key * blk;
-  const int q = r / L1, l = r - q * L1;
-  const int n1 = q / fd.n, n2 = q - n1 * fd.n;
-  return ((l * fd.P + key) * fd.n + n2) * fd.n + n1;
+// Packed column layout of the FP32 fast path's feature rows (x and its BF16
+// split, dE/dx, and the model's BF16 copies of T).
+//
+// For each l, a centre's coefficients form an S n x (2l+1) matrix C_l (row
+// I = a n + n1 for species a, radial n1), and the reference's features are
+// entries of its Gram matrix G_l = lf_l C_l C_l^T (lf_l = (2l+1)^-1/2):
+// p_(ab)(n1 n2 l) = s_ab G_l[a n1][b n2] for a <= b, s_ab = sqrt2 for a < b
+// (calculator_spherical_invariants.hh:747-794). The packed layout stores the
+// upper triangle of each G_l in 2 x 2 tiles: tile (i, j), i <= j, holds rows
+// 2i, 2i+1 and columns 2j, 2j+1 as four consecutive columns
+//   l Bp + 4 (j (j + 1) / 2 + i) + (I & 1) + 2 (J & 1),
+// entries with I < J multiplied by sqrt2, and the one entry below the
+// diagonal of a diagonal tile (and any row or column beyond S n) zero. That is
+// the reference's feature itself for a < b. For a = b the reference keeps
+// both p(n1 n2) and p(n2 n1), which are equal, and the packed layout one
+// entry sqrt2 p(n1 n2) (n1 < n2): the sum of squares of a packed row is the
+// reference's |p|^2, and its dot product with a sparse point packed the same
+// way (the two entries folded into (t(n1 n2) + t(n2 n1)) / sqrt2) is the
+// reference's x . t, with S n(n-1)/2 (L+1) fewer columns (less the zeros of
+// the diagonal tiles). A tile is 8 bytes of BF16, so every store of the
+// forward is aligned, and the backward reads a tile with one 16-byte load.
+// The reference's dense order, used by the FP64 path and by every export, is
+// ((key*n + n1)*n + n2)*(L+1) + l (property_block_sparse.hh:911-931).
+inline int packed_column(const FeatureDims & fd, int l, int I, int J) {
+  const int j = J >> 1;
+  return l * fd.Bp + 4 * (j * (j + 1) / 2 + (I >> 1)) + (I & 1) + 2 * (J & 1);
 }
+// Column of (key(a, b), n1, n2, l), a <= b, in the reference's dense order.
+inline int reference_column(const FeatureDims & fd, int a, int n1, int b, int n2, int l) {
+  const int key = a * fd.S - a * (a - 1) / 2 + (b - a);
+  return ((key * fd.n + n1) * fd.n + n2) * (fd.L + 1) + l;
+}
+// A row in the reference's dense order (D values) to the packed layout (Dg
+// values, zeros in the padding).
+void pack_reference_row(const FeatureDims & fd, const double * ref, double * packed);
+// A packed row, times `scale`, to the reference's dense order.
+void unpack_to_reference(const FeatureDims & fd, const float * packed, float scale, double * ref);
 
 struct PsArgs {
   FeatureDims fd;
@@ -256,9 +283,9 @@ struct PsArgs {
 // X rows (normalised) and inverse norms.
 void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double * inv_norm,
                         cudaStream_t st);
-// FP32 forward: rows of the unnormalised p (fast column order) as a BF16
-// hi/lo split, optionally also in FP32 (X may be null), and row_scale[row] =
-// 1/|p| (1 without normalisation); x = row_scale * p.
+// FP32 forward: rows (packed layout, Dg columns) of the unnormalised p as a
+// BF16 hi/lo split, optionally also in FP32 (X may be null), and
+// row_scale[row] = 1/|p| (1 without normalisation); x = row_scale * p.
 void launch_ps_fwd_fp32(const PsArgs & a, const float * C, float * X, __nv_bfloat16 * Xh,
                         __nv_bfloat16 * Xl, float * row_scale, cudaStream_t st);
 // The same forward (without the FP32 copy) as tcgen05 Gram products of
@@ -277,7 +304,7 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
                          int64_t p_base, const double * C, const double * X,
                          const double * inv_norm, const double * dCp, const double * dCs,
                          double * dX, cudaStream_t st);
-// Adjoint: dE/dC from dE/dX rows (species-sorted) for all centres, written
+// Adjoint: dE/dC from dE/dX rows (species-sorted, packed layout) for all centres, written
 // as dC[i][lm][s*n + n'] (lm = l^2 + m; the (species, radial) index is the
 // fastest so that the centre's 32 consecutive rows store coalesced).
 // x is read back as row_scale * (hi + lo) of the forward's BF16 split.

@@ -1,6 +1,7 @@
 // Scans, the stable species sort of centres, fills and small utilities.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -362,6 +363,49 @@ void launch_scale_rows_by_group(float * x, int64_t rows, int64_t cols, const int
   if (rows * cols <= 0) return;
   scale_rows_by_group_kernel<<<div_up(rows * cols, 256), 256, 0, st>>>(x, rows, cols, group, scale);
   RGPU_LAUNCHED();
+}
+
+// ------------------------------------------------------------ packed layout
+namespace {
+constexpr double kSqrt2 = 1.41421356237309504880;
+}
+
+void pack_reference_row(const FeatureDims & fd, const double * ref, double * packed) {
+  std::fill(packed, packed + fd.Dg, 0.);
+  const int n = fd.n;
+  for (int l = 0; l <= fd.L; ++l)
+    for (int J = 0; J < fd.Sn; ++J)
+      for (int I = 0; I <= J; ++I) {
+        const int a = I / n, n1 = I - a * n, b = J / n, n2 = J - b * n;
+        double v;
+        if (a < b)
+          v = ref[reference_column(fd, a, n1, b, n2, l)];
+        else if (n1 < n2)  // both orders of a same-species pair, folded
+          v = (ref[reference_column(fd, a, n1, a, n2, l)] + ref[reference_column(fd, a, n2, a, n1, l)]) / kSqrt2;
+        else
+          v = ref[reference_column(fd, a, n1, a, n1, l)];
+        packed[packed_column(fd, l, I, J)] = v;
+      }
+}
+
+void unpack_to_reference(const FeatureDims & fd, const float * packed, float scale, double * ref) {
+  const int n = fd.n;
+  const float inv_sqrt2 = float(1. / kSqrt2);
+  for (int a = 0; a < fd.S; ++a)
+    for (int b = a; b < fd.S; ++b)
+      for (int n1 = 0; n1 < n; ++n1)
+        for (int n2 = 0; n2 < n; ++n2)
+          for (int l = 0; l <= fd.L; ++l) {
+            float v;
+            if (a < b) {
+              v = packed[packed_column(fd, l, a * n + n1, b * n + n2)] * scale;
+            } else {
+              const int lo = std::min(n1, n2), hi = std::max(n1, n2);
+              v = packed[packed_column(fd, l, a * n + lo, a * n + hi)] * scale;
+              if (n1 != n2) v *= inv_sqrt2;  // the packed entry is sqrt2 p(n1 n2)
+            }
+            ref[reference_column(fd, a, n1, b, n2, l)] = double(v);
+          }
 }
 
 }  // namespace rgpu

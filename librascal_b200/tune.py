@@ -34,7 +34,7 @@ FIELDS = ["exp_chunk", "exp_warps", "adj_threads", "adj_blocks_per_sm", "psf_thr
 DEFAULT = dict(exp_chunk=16, exp_warps=4, adj_threads=128, adj_blocks_per_sm=64, psf_threads=256,
                psb_threads=320, gemm_variant=0, psf_tc=0)
 CANDIDATES = dict(exp_chunk=[8, 16, 32], exp_warps=[2, 4, 8], adj_threads=[64, 96, 128],
-                  adj_blocks_per_sm=[8, 16, 32, 64, 128], psf_threads=[64, 96, 128, 192, 256],
+                  adj_blocks_per_sm=[8, 16, 32, 64, 128], psf_threads=[64, 96, 128, 192, 224, 256],
                   psb_threads=[160, 192, 224, 256, 288, 320], gemm_variant=[0, 1, 2], psf_tc=[0, 1])
 # stage_times index (rgpu_stage_times) each field acts on
 STAGES = dict(exp_chunk=(2,), exp_warps=(2,), adj_threads=(7,), adj_blocks_per_sm=(7,), psf_threads=(3,),
