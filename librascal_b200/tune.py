@@ -7,8 +7,10 @@ of the expansion, the block size and grid cap of the pair adjoint, the block
 sizes of the power-spectrum forward and backward, and the GEMM pipeline
 (rgpu_set_tile_config). This module measures the candidates of each field
 with CUDA events (the library's per-stage events of rgpu_gap_predict, on the
-ordinary path) by coordinate descent from the defaults, keeps for each field
-the value with the shortest stage time, and writes the winners to
+ordinary path), interleaved so that clock drift hits them alike, by
+coordinate descent from the defaults, keeps for each field
+the value with the shortest stage time, keeps the defaults instead when the
+whole step is not faster with the winners, and writes the result to
 ``tuned_tiles.json`` beside this file, which the package installs whenever it
 loads the library.
 
@@ -90,24 +92,36 @@ def stage_ms(model, structures, repeats, precision="fp32"):
     return best
 
 
+def interleaved(model, structures, shape, configs, rounds):
+    """Stage times of each configuration, the minimum over `rounds` rounds
+    that measure every configuration once in turn, so that a drift of the
+    clocks during the sweep (the GPU warming up under its power cap) weighs
+    on all of them alike."""
+    best = [None] * len(configs)
+    for _ in range(rounds):
+        for k, cfg in enumerate(configs):
+            set_config(shape, cfg)
+            t = stage_ms(model, structures, 1)
+            best[k] = t if best[k] is None else np.minimum(best[k], t)
+    return best
+
+
 def tune(model, structures, shape, repeats=3, log=print):
-    """Coordinate descent over FIELDS from the defaults; returns the chosen
-    configuration and every measurement (field, value, stage ms)."""
+    """Coordinate descent over FIELDS from the defaults, each field's
+    candidates measured interleaved; returns the chosen configuration and
+    every measurement (field, value, stage ms)."""
     structures.use_graphs(False)
     cfg = dict(DEFAULT)
     measured = []
     for field in FIELDS:
-        times = {}
-        for cand in CANDIDATES[field]:
-            trial = dict(cfg, **{field: cand})
-            set_config(shape, trial)
-            t = stage_ms(model, structures, repeats)
-            ms = float(sum(t[i] for i in STAGES[field]))
-            times[cand] = ms
-            measured.append(dict(field=field, value=cand, stage_ms=round(ms, 4)))
+        cands = CANDIDATES[field]
+        times = interleaved(model, structures, shape, [dict(cfg, **{field: c}) for c in cands], repeats)
+        ms = {c: float(sum(t[i] for i in STAGES[field])) for c, t in zip(cands, times)}
+        for c in cands:
+            measured.append(dict(field=field, value=c, stage_ms=round(ms[c], 4)))
             if log:
-                log("%-18s %4d  %.4f ms" % (field, cand, ms))
-        cfg[field] = min(times, key=times.get)
+                log("%-18s %4d  %.4f ms" % (field, c, ms[c]))
+        cfg[field] = min(ms, key=ms.get)
     set_config(shape, cfg)
     structures.use_graphs(True)
     return cfg, measured
@@ -175,12 +189,18 @@ def main():
     model, st, shape = _workload(args.workload)
     set_config(shape, None)
     t0 = time.time()
-    default = stage_ms(model, st, args.repeats)
     cfg, measured = tune(model, st, shape, args.repeats)
-    tuned = stage_ms(model, st, args.repeats)
+    # the choices were made field by field; the whole step decides whether
+    # they are kept (the defaults stay when they are not slower)
+    default, tuned = interleaved(model, st, shape, [dict(DEFAULT), cfg], args.repeats + 2)
+    kept_default = bool(tuned[0] >= default[0])
+    if kept_default:
+        cfg = dict(DEFAULT)
+    set_config(shape, cfg)
     entries = [e for e in load_table(args.out) if tuple(e["shape"]) != tuple(shape)]
     props = torch.cuda.get_device_properties(0)
-    entries.append(dict(shape=list(shape), workload=args.workload, values=cfg, device=props.name,
+    entries.append(dict(shape=list(shape), workload=args.workload, values=cfg, kept_default=kept_default,
+                        device=props.name,
                         default_stage_ms=[round(float(x), 4) for x in default],
                         tuned_stage_ms=[round(float(x), 4) for x in tuned],
                         measurements=measured, seconds=round(time.time() - t0, 1)))
