@@ -732,10 +732,14 @@ def run_gap(args):
     S, n, L = len(species), hypers["max_radial"], hypers["max_angular"]
     # the FP32 path's rows hold the upper triangles of the per-l Gram
     # matrices (one entry per symmetric pair of same-species entries), in
-    # 2 x 2 tiles: Dp values, Dg columns with padding
+    # 2 x 2 tiles grouped into species-pair segments of 32-column multiples:
+    # Dp values, Dg columns with padding
     Sn = S * n
     Dp = (L + 1) * Sn * (Sn + 1) // 2
-    Dg = ((L + 1) * ((2 * ((Sn + 1) // 2) * ((Sn + 1) // 2 + 1) + 7) // 8 * 8) + 31) // 32 * 32
+    G, npg = (S, n // 2) if n % 2 == 0 else (1, (Sn + 1) // 2)
+    lenD = (4 * (L + 1) * npg * (npg + 1) // 2 + 31) // 32 * 32
+    lenO = (4 * (L + 1) * npg * npg + 31) // 32 * 32
+    Dg = G * lenD + G * (G - 1) // 2 * lenO
     gemm_flops = 4.0 * float(np.sum(counts * msp)) * Dp  # forward + backward
     gemm_ms = stages[4] + stages[5]
     bf16_peak, hbm_peak, peak_kind = peaks()

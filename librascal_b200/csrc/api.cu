@@ -208,14 +208,14 @@ struct rgpu_structures {
   DevBuf lut;
   FeatureDims fd{};
   std::vector<int64_t> species_count;
-  DevBuf row_of_center, center_of_row, species_count_d, sort_tmp, present;
+  DevBuf row_of_center, center_of_row, species_count_d, sort_tmp, present, tile_mask;
   DevBuf C64, X64, invn64, C32, X32, xscale32;  // xscale32[row] = 1/|p| (FP32 path)
   int feat_precision{-1};
   const rgpu_calculator * feat_calc{nullptr};
   bool feat_gradients{false};
   bool feat_valid{false};
   // GAP work
-  DevBuf E_d, F_d, S_d, K64, t64, erow64, Wh, Wl, dX32, dC32, epart, Xh, Xl;
+  DevBuf E_d, F_d, S_d, K64, t64, erow64, Wh, Wl, dX32, dC32, epart, Xh, Xl, chunk_map;
   bool feat_x32{false};  // FP32 features also kept unsplit (for export)
   DevBuf dCp, dCs, dXp;
   DevBuf knm, W64, plist, Vvir;  // sparse kernel matrices for training
@@ -386,9 +386,18 @@ FeatureDims make_dims(const Hypers & hy, int S) {
   f.D = f.P * f.n * f.n * (f.L + 1);
   f.Dpad = (f.D + 31) / 32 * 32;
   f.Sn = S * f.n;
-  const int pairs = (f.Sn + 1) / 2;  // 2 x 2 tiles of the packed layout per row or column
-  f.Bp = (2 * pairs * (pairs + 1) + 7) / 8 * 8;
-  f.Dg = ((f.L + 1) * f.Bp + 31) / 32 * 32;
+  if (f.n % 2 == 0) {  // row pairs never straddle two species
+    f.G = S;
+    f.npg = f.n / 2;
+  } else {
+    f.G = 1;
+    f.npg = (f.Sn + 1) / 2;
+  }
+  f.TD = f.npg * (f.npg + 1) / 2;
+  f.TO = f.npg * f.npg;
+  f.lenD = (4 * (f.L + 1) * f.TD + 31) / 32 * 32;
+  f.lenO = (4 * (f.L + 1) * f.TO + 31) / 32 * 32;
+  f.Dg = f.G * f.lenD + f.G * (f.G - 1) / 2 * f.lenO;
   return f;
 }
 
@@ -482,6 +491,17 @@ void sort_rows(rgpu_structures * s) {
   for (int sI = 0; sI < s->fd.S; ++sI) s->species_count[sI] = s->centres_of_type[s->species[sI]];
 }
 
+// After the FP32 expansion (which writes the presence masks): rows of one
+// species ordered by their neighbour species, so that the GEMM tiles of the
+// packed layout's species segments can skip what none of their rows holds.
+// Only layouts with more than one segment group need it.
+void sort_rows_by_mask(rgpu_structures * s) {
+  if (s->fd.G < 2) return;
+  launch_mask_sort(s->nl.n_centers, s->types_d.as<int32_t>(), s->nl.center_atom, s->lut.as<int8_t>(),
+                   s->present.as<uint32_t>(), s->fd.S, s->row_of_center.as<int32_t>(), s->center_of_row.as<int32_t>(),
+                   s->sort_tmp, s->st);
+}
+
 void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, bool grads,
                       const std::vector<int> & extra_species, bool need_x32 = true) {
   build_nl(s, c->hy.cutoff);
@@ -515,6 +535,7 @@ void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, b
   } else {
     s->C32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.n * row_stride(fd.L) + 64);
     launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), s->st);
+    if (c->hy.kind == "sphericalinvariants") sort_rows_by_mask(s);
     mark(s, 3);
     if (c->hy.kind == "sphericalinvariants") {
       if (need_x32) s->X32.ensure(sizeof(float) * size_t(nc) * fd.Dg + 64);
@@ -862,6 +883,34 @@ std::vector<int64_t> w_offsets(const rgpu_gap_model * m, const rgpu_structures *
   return wofs;
 }
 
+// Rows and 128-row tiles of each central species (rows in species order).
+TileMaskArgs tile_mask_args(const rgpu_structures * s) {
+  TileMaskArgs a{};
+  a.S = s->fd.S;
+  int64_t r = 0, t = 0;
+  for (int sI = 0; sI < s->fd.S; ++sI) {
+    a.row0[sI] = r;
+    a.rows[sI] = s->species_count[sI];
+    a.tile_off[sI] = t;
+    r += s->species_count[sI];
+    t += (s->species_count[sI] + 127) / 128;
+  }
+  a.tile_off[s->fd.S] = t;
+  return a;
+}
+
+// Species skipping of a grouped GEMM over the packed columns (mode 1: K, the
+// forward; 2: N, the backward), for layouts of more than one species group.
+void set_segments(Bf16x3Gemm & a, const rgpu_structures * s, const TileMaskArgs & tm, int sI, int mode) {
+  const FeatureDims & fd = s->fd;
+  if (fd.G < 2) return;
+  a.seg_mode = mode;
+  a.seg_G = fd.G;
+  a.seg_LD = fd.lenD / 32;
+  a.seg_LO = fd.lenO / 32;
+  a.tile_mask = s->tile_mask.as<uint32_t>() + tm.tile_off[sI];
+}
+
 // Fast path, forward half: the grouped tcgen05 GEMM with the GAP epilogue
 // (energy partials and W = alpha zeta k^(zeta-1) as a BF16 pair), then the
 // per-structure energies (baseline not included).
@@ -881,6 +930,12 @@ void gap_fast_forward(rgpu_gap_model * m, rgpu_structures * s, double * E_d) {
   s->Wl.ensure(sizeof(uint16_t) * size_t(std::max<int64_t>(wtot, 1)) + 64);
   s->epart.ensure(sizeof(float) * size_t(std::max<int64_t>(eparts, 1)) + 64);
   s->dX32.ensure(sizeof(float) * size_t(nc) * fd.Dg + 64);
+  // species present in each 128-row tile (rows sorted by species and mask)
+  const TileMaskArgs tm = tile_mask_args(s);
+  if (fd.G > 1) {
+    s->tile_mask.ensure(sizeof(uint32_t) * size_t(std::max<int64_t>(tm.tile_off[fd.S], 1)) + 64);
+    launch_tile_masks(tm, s->center_of_row.as<int32_t>(), s->present.as<uint32_t>(), s->tile_mask.as<uint32_t>(), st);
+  }
   const __nv_bfloat16 * Xh = s->Xh.as<__nv_bfloat16>();
   const __nv_bfloat16 * Xl = s->Xl.as<__nv_bfloat16>();
   __nv_bfloat16 * Wh = s->Wh.as<__nv_bfloat16>();
@@ -910,6 +965,7 @@ void gap_fast_forward(rgpu_gap_model * m, rgpu_structures * s, double * E_d) {
       a.zeta = m->zeta;
       a.e_part = s->epart.as<float>() + eofs_of(s, m, sI);
       a.row_scale = s->xscale32.as<float>() + row0;  // k = (p . t) / |p|
+      set_segments(a, s, tm, sI, 1);  // K blocks of species pairs absent from a tile are skipped
       fwd.push_back(a);
     }
     row0 += rows;
@@ -964,6 +1020,9 @@ void gap_fast_backward(rgpu_gap_model * m, rgpu_structures * s, double * F_d, do
       a.epilogue = 0;
       a.C = s->dX32.as<float>() + size_t(row0) * fd.Dg;
       a.ldc = fd.Dg;
+      // N tiles of species pairs absent from a tile are not computed; the
+      // power-spectrum backward reads zeros for them (chunk map)
+      set_segments(a, s, tile_mask_args(s), sI, 2);
       bwd.push_back(a);
     } else if (rows > 0) {
       launch_fill_f32(s->dX32.as<float>() + size_t(row0) * fd.Dg, rows * fd.Dg, 0.f, st);
@@ -978,8 +1037,9 @@ void gap_fast_backward(rgpu_gap_model * m, rgpu_structures * s, double * F_d, do
   pa.normalize = c->hy.normalize;
   pa.row_of_center = s->row_of_center.as<int32_t>();
   s->dC32.ensure(sizeof(float) * size_t(nc) * fd.S * fd.nK + 64);
+  s->chunk_map.ensure(sizeof(uint32_t) * size_t(fd.Dg / 4) + 64);
   launch_ps_bwd_fp32(pa, s->C32.as<float>(), Xh, Xl, s->xscale32.as<float>(), s->dX32.as<float>(),
-                     s->dC32.as<float>(), st);
+                     s->chunk_map.as<uint32_t>(), s->present.as<uint32_t>(), s->dC32.as<float>(), st);
   if (struct_scale)
     launch_scale_rows_by_group(s->dC32.as<float>(), nc, int64_t(fd.S) * fd.nK, s->nl.center_struct, struct_scale,
                                st);
@@ -1445,10 +1505,11 @@ static std::vector<const void *> md_buffers(const rgpu_gap_model * m, const rgpu
   std::vector<const void *> v;
   for (const DevBuf * b : {&s->atom_off_d, &s->pos_d, &s->types_d, &s->cells_d, &s->pbc_d, &s->tag2idx_d,
                            &s->ncent_d, &s->center_off_d, &s->atom_struct_d, &s->lut, &s->row_of_center,
-                           &s->center_of_row, &s->species_count_d, &s->sort_tmp, &s->present, &s->C64, &s->X64,
+                           &s->center_of_row, &s->species_count_d, &s->sort_tmp, &s->present, &s->tile_mask,
+                           &s->C64, &s->X64,
                            &s->invn64, &s->C32, &s->X32, &s->xscale32, &s->E_d, &s->F_d, &s->S_d, &s->K64,
                            &s->t64, &s->erow64, &s->Wh, &s->Wl, &s->dX32, &s->dC32, &s->epart, &s->Xh, &s->Xl,
-                           &s->dCp, &s->dCs, &s->dXp, &s->knm, &s->W64, &s->plist, &s->Vvir})
+                           &s->chunk_map, &s->dCp, &s->dCs, &s->dXp, &s->knm, &s->W64, &s->plist, &s->Vvir})
     v.push_back(b->p);
   const NlWork & w = s->nlw;
   for (const DevBuf * b : {&w.geom, &w.counts64, &w.scan_tmp, &w.ghost_off, &w.site_x, &w.site_type, &w.site_real,
@@ -1508,6 +1569,7 @@ static void graph_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress, 
   pa.normalize = c->hy.normalize;
   pa.row_of_center = s->row_of_center.as<int32_t>();
   launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), st);
+  sort_rows_by_mask(s);
   launch_ps_fwd_fast(pa, s->C32.as<float>(), nullptr, s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(),
                      s->xscale32.as<float>(), st);
   RGPU_CUDA(cudaMemsetAsync(s->E_d.p, 0, sizeof(double) * s->n_struct, st));

@@ -239,6 +239,53 @@ struct TcGroup {
   const float * row_scale;  // may be null
   int64_t tile0;            // first tile of this group in the launch
   int64_t n_tiles;          // tiles along N
+  const uint32_t * tile_mask;  // per M-tile: species present in any of its rows (null: all)
+};
+
+// Species segments of the packed feature columns (rgpu_internal.h): G groups,
+// segment (A, B), A <= B in A-major order, LD (A = B) or LO (A < B) units of
+// 32 columns long. A unit is needed by an M-tile when both of its segment's
+// groups are in the tile's mask; the other units hold zeros in every row of
+// the tile (forward: skipped K blocks add nothing) or are never read for
+// them (backward: skipped N tiles are columns of species the rows lack).
+struct SegGeom {
+  int mode;  // 0: no skipping; 1: K (forward); 2: N (backward)
+  int G, LD, LO;
+};
+struct SegWalk {
+  SegGeom sg;
+  uint32_t mask;
+  int A, B, end;
+  bool on;
+  __device__ __forceinline__ void start(const SegGeom & g, uint32_t m) {
+    sg = g;
+    mask = m ? m : 0xFFFFFFFFu;  // a tile always holds its rows' own species
+    A = 0;
+    B = 0;
+    end = g.LD;
+    on = mask & 1u;
+  }
+  // whether unit u is needed; u must not decrease between calls
+  __device__ __forceinline__ bool need(int u) {
+    while (u >= end && A < sg.G) {
+      if (B + 1 < sg.G) {
+        ++B;
+        end += sg.LO;
+      } else {
+        ++A;
+        B = A;
+        end += sg.LD;
+      }
+      on = ((mask >> A) & 1u) && ((mask >> B) & 1u);
+    }
+    return A >= sg.G || on;
+  }
+  // whether any unit of [u0, u0 + n) is needed
+  __device__ __forceinline__ bool any(int u0, int n) {
+    bool r = false;
+    for (int u = u0; u < u0 + n; ++u) r |= need(u);
+    return r;
+  }
 };
 
 struct TcGroupedArgs {
@@ -250,7 +297,17 @@ struct TcGroupedArgs {
   int64_t n_tiles;
   TcStatus * status;
   long long mma_wait_limit;  // polls of the MMA warp's operand waits
+  SegGeom seg;
 };
+
+// Whether N-mode skipping drops tile (mt, nt) of group G (every role asks).
+template <int BN>
+__device__ __forceinline__ bool skip_tile(const TcGroupedArgs & p, const TcGroup & G, int64_t mt, int64_t nt) {
+  if (p.seg.mode != 2 || !G.tile_mask) return false;
+  SegWalk w;
+  w.start(p.seg, G.tile_mask[mt]);
+  return !w.any(int(nt * (BN / 32)), BN / 32);
+}
 
 __device__ __forceinline__ int find_group(const TcGroupedArgs & p, int64_t t) {
   int g = 0;
@@ -303,9 +360,14 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         const int g = find_group(p, t);
         const TcGroup & G = p.grp[g];
         const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
+        if (skip_tile<BN>(p, G, mt, nt)) continue;
         const int m0 = int(mt * kBM), n0 = int(nt * BN);
         const int nk = int((G.K + BK - 1) / BK);
+        const bool kskip = p.seg.mode == 1 && G.tile_mask;
+        SegWalk w;
+        if (kskip) w.start(p.seg, G.tile_mask[mt]);
         for (int kb = 0; kb < nk; ++kb) {
+          if (kskip && !w.any(kb * (BK / 32), BK / 32)) continue;
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1u;
           if (!mbar_wait(&empty[s], ph ^ 1u, status, 1)) {
@@ -333,9 +395,12 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
       uint32_t it = 0;
       int i = 0;
       bool ok = true;
-      for (int64_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x, ++i) {
+      for (int64_t t = blockIdx.x; t < p.n_tiles && ok; t += gridDim.x) {
         const int g = find_group(p, t);
-        const int nk = int((p.grp[g].K + BK - 1) / BK);
+        const TcGroup & G = p.grp[g];
+        const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
+        if (skip_tile<BN>(p, G, mt, nt)) continue;
+        const int nk = int((G.K + BK - 1) / BK);
         const int b = i & 1;
         const uint32_t use = uint32_t(i >> 1);
         if (!mbar_wait(&tempty[b], (use & 1u) ^ 1u, status, 5)) {
@@ -344,7 +409,12 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         }
         tc_fence_after();
         const uint32_t acc = tmem + uint32_t(b * BN);
+        const bool kskip = p.seg.mode == 1 && G.tile_mask;
+        SegWalk w;
+        if (kskip) w.start(p.seg, G.tile_mask[mt]);
+        bool first = true;  // the tile's first MMA overwrites the accumulator
         for (int kb = 0; kb < nk; ++kb) {
+          if (kskip && !w.any(kb * (BK / 32), BK / 32)) continue;
           const int s = int(it % STAGES);
           const uint32_t ph = (it / STAGES) & 1u;
           if (!mbar_wait(&full[s], ph, status, 2, p.mma_wait_limit)) {
@@ -358,15 +428,17 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k) {
             const uint32_t off = uint32_t(k) * 32u;
-            const uint32_t acc0 = (kb > 0 || k > 0) ? 1u : 0u;
+            const uint32_t acc0 = (first && k == 0) ? 0u : 1u;
             mma_bf16(acc, smem_desc_k<BK>(a_lo + off), smem_desc_k<BK>(b_hi + off), idesc, acc0);
             mma_bf16(acc, smem_desc_k<BK>(a_hi + off), smem_desc_k<BK>(b_lo + off), idesc, 1u);
             mma_bf16(acc, smem_desc_k<BK>(a_hi + off), smem_desc_k<BK>(b_hi + off), idesc, 1u);
           }
           mma_commit(&empty[s]);
           ++it;
+          first = false;
         }
         mma_commit(&tfull[b]);  // also after a failed wait, so the epilogue moves on
+        ++i;
       }
       mma_commit(done);  // completes when every MMA issued above has finished
       mbar_drain(done, 0u, status, 6);
@@ -374,10 +446,11 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
   } else {
     const int q = warp & 3;  // TMEM lane quadrant of this warp
     int i = 0;
-    for (int64_t t = blockIdx.x; t < p.n_tiles; t += gridDim.x, ++i) {
+    for (int64_t t = blockIdx.x; t < p.n_tiles; t += gridDim.x) {
       const int g = find_group(p, t);
       const TcGroup & G = p.grp[g];
       const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
+      if (skip_tile<BN>(p, G, mt, nt)) continue;
       const int64_t m0 = mt * kBM, n0 = nt * BN;
       const int b = i & 1;
       const uint32_t use = uint32_t(i >> 1);
@@ -387,46 +460,64 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
       const int64_t row = m0 + q * 32 + lane;
       const float rs = (p.epilogue == 1 && G.row_scale && row < G.M) ? __ldg(G.row_scale + row) : 1.f;
       float e_acc = 0.f;
-      for (int c0 = 0; c0 < BN; c0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + (uint32_t(q * 32) << 16) + uint32_t(b * BN + c0), v);
+      const float zf = float(p.zeta);
+      const int zm1 = p.zeta - 1;
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        float v[32];
+        tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(b * BN + c0), v);
         const int64_t col = n0 + c0;
-        if (row >= G.M) continue;
         if (p.epilogue == 0) {
-          if (col >= G.N) continue;
+          if (row >= G.M || col >= G.N) continue;
           float * out = G.C + row * G.ldc + col;
-          if (col + 16 <= G.N) {
+          if (col + 32 <= G.N) {
 #pragma unroll
-            for (int k = 0; k < 16; k += 4)
+            for (int k = 0; k < 32; k += 4)
               *reinterpret_cast<float4 *>(out + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
           } else {
-            for (int k = 0; k < 16; ++k)
+            for (int k = 0; k < 32; ++k)
               if (col + k < G.N) out[k] = v[k];
           }
         } else {
-          if (col >= G.ldw) continue;
-          __align__(16) __nv_bfloat16 hi[16], lo[16];
+          if (col >= G.ldw) continue;  // uniform over the warp: ldw is a multiple of 32
+          // lane j holds alpha of column col + j; every lane takes them all by shuffles
+          const float my_al = (col + lane < G.N) ? __ldg(G.alpha + col + lane) : 0.f;
+          uint32_t hw[16], lw[16];
 #pragma unroll
-          for (int k = 0; k < 16; ++k) {
-            const float x = v[k] * rs;
-            const float al = (col + k < G.N) ? __ldg(G.alpha + col + k) : 0.f;
-            e_acc += al * powz(x, p.zeta);
-            const float w = al * (float(p.zeta) * powz(x, p.zeta - 1));
-            hi[k] = __float2bfloat16_rn(w);
-            lo[k] = __float2bfloat16_rn(w - __bfloat162float(hi[k]));
+          for (int k = 0; k < 32; k += 2) {
+            const float a0 = __shfl_sync(0xffffffffu, my_al, k), a1 = __shfl_sync(0xffffffffu, my_al, k + 1);
+            const float x0 = v[k] * rs, x1 = v[k + 1] * rs;
+            float p0 = x0, p1 = x1;  // x^(zeta-1)
+            if (zm1 != 1) {
+              p0 = 1.f;
+              p1 = 1.f;
+              for (int z = 0; z < zm1; ++z) {
+                p0 *= x0;
+                p1 *= x1;
+              }
+            }
+            e_acc += a0 * (p0 * x0) + a1 * (p1 * x1);
+            const float w0 = a0 * zf * p0, w1 = a1 * zf * p1;
+            const __nv_bfloat162 h = __floats2bfloat162_rn(w0, w1);
+            const float2 hf = __bfloat1622float2(h);
+            const __nv_bfloat162 l = __floats2bfloat162_rn(w0 - hf.x, w1 - hf.y);
+            hw[k / 2] = *reinterpret_cast<const uint32_t *>(&h);
+            lw[k / 2] = *reinterpret_cast<const uint32_t *>(&l);
           }
+          if (row >= G.M) continue;
           uint4 * dh = reinterpret_cast<uint4 *>(G.W_hi + row * G.ldw + col);
           uint4 * dl = reinterpret_cast<uint4 *>(G.W_lo + row * G.ldw + col);
-          dh[0] = reinterpret_cast<uint4 *>(hi)[0];
-          dh[1] = reinterpret_cast<uint4 *>(hi)[1];
-          dl[0] = reinterpret_cast<uint4 *>(lo)[0];
-          dl[1] = reinterpret_cast<uint4 *>(lo)[1];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            dh[k] = make_uint4(hw[4 * k], hw[4 * k + 1], hw[4 * k + 2], hw[4 * k + 3]);
+            dl[k] = make_uint4(lw[4 * k], lw[4 * k + 1], lw[4 * k + 2], lw[4 * k + 3]);
+          }
         }
       }
       if (p.epilogue == 1 && row < G.M) G.e_part[nt * G.M + row] = e_acc;
       tc_fence_before();  // the TMEM reads above are complete before the buffer is released
       __syncwarp();
       if (lane == 0) mbar_arrive(&tempty[b]);
+      ++i;
     }
   }
   tc_fence_before();
@@ -616,7 +707,22 @@ void grouped_launch(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
     G.row_scale = g.row_scale;
     G.n_tiles = (g.N + BN - 1) / BN;
     G.tile0 = tiles;
+    G.tile_mask = g.seg_mode ? g.tile_mask : nullptr;
     tiles += G.n_tiles * ((g.M + kBM - 1) / kBM);
+    if (ng == 0) {
+      p.seg.mode = g.seg_mode;
+      p.seg.G = g.seg_G;
+      p.seg.LD = g.seg_LD;
+      p.seg.LO = g.seg_LO;
+    } else if (g.seg_mode != p.seg.mode || g.seg_G != p.seg.G || g.seg_LD != p.seg.LD || g.seg_LO != p.seg.LO) {
+      throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: groups must share the species segments");
+    }
+    if (g.seg_mode) {
+      const int64_t units = int64_t(g.seg_G) * g.seg_LD + int64_t(g.seg_G) * (g.seg_G - 1) / 2 * g.seg_LO;
+      if (g.seg_mode < 0 || g.seg_mode > 2 || g.seg_G < 1 || g.seg_G > 32 || g.seg_LD < 1 || g.seg_LO < 1 ||
+          32 * units != (g.seg_mode == 1 ? g.K : g.N))
+        throw Error(RGPU_ERR_INVALID_ARGUMENT, "grouped GEMM: species segments do not tile the feature columns");
+    }
     ++ng;
   }
   if (ng == 0) return;

@@ -107,33 +107,36 @@ __device__ __forceinline__ float fwd_tile(const float * Cp, int Sn, int i, int j
   return v00 * v00 + v10 * v10 + v01 * v01 + v11 * v11;
 }
 
-// Every tile of l-block l of the row (tile r at columns l Bp + 4r; the task
-// table gives its (i, j)), then the blocks above l; returns their sum of
-// squares.
+// Every tile of l-block l of the row (task r: row pair i, column pair j and
+// T, the tiles per l of its segment, in tab[r].x = i | j << 8 | T << 16; its
+// first column at l = L in tab[r].y), then the blocks above l; returns their
+// sum of squares.
 template <int L, int l>
-__device__ __forceinline__ float fwd_blocks(const float * Cp, int Sn, int Bp, int nt, const uint16_t * tiles,
-                                            float * X, __nv_bfloat16 * hr, __nv_bfloat16 * lr) {
+__device__ __forceinline__ float fwd_blocks(const float * Cp, int Sn, int nt, const int2 * tab, float * X,
+                                            __nv_bfloat16 * hr, __nv_bfloat16 * lr) {
   if constexpr (l > L) {
     return 0.f;
   } else {
     float ss = 0.f;
     for (int r = threadIdx.x; r < nt; r += blockDim.x) {
-      const uint32_t ij = tiles[r];
-      const int o = l * Bp + 4 * r;
-      ss += fwd_tile<L, l>(Cp, Sn, int(ij & 0xFFu), int(ij >> 8), X ? X + o : nullptr, hr + o, lr + o);
+      const int2 e = tab[r];
+      const uint32_t ij = uint32_t(e.x);
+      const int o = e.y + 4 * (L - l) * int(ij >> 16);
+      ss += fwd_tile<L, l>(Cp, Sn, int(ij & 0xFFu), int((ij >> 8) & 0xFFu), X ? X + o : nullptr, hr + o, lr + o);
     }
-    return ss + fwd_blocks<L, l + 1>(Cp, Sn, Bp, nt, tiles, X, hr, lr);
+    return ss + fwd_blocks<L, l + 1>(Cp, Sn, nt, tab, X, hr, lr);
   }
 }
 
 // p of a centre's row in the packed layout as a BF16 hi/lo split (and in
-// FP32 when X is given), one 2 x 2 tile per task straight to HBM, and the
-// row's scale 1/|p| (1 without normalisation); the packed values keep |p|.
-// The block walks the l-blocks in turn (l a compile-time constant in each
-// loop); consecutive lanes take consecutive tiles (mostly of one column
-// pair, whose coefficient rows they then read as broadcasts). Persistent:
-// each block loops over centres, prefetching the next centre's coefficient
-// tile with cp.async while it works on the current one.
+// FP32 when X is given), one 2 x 2 tile per task straight to HBM, the
+// segments' padding set to zero, and the row's scale 1/|p| (1 without
+// normalisation); the packed values keep |p|. The block walks the l-blocks
+// in turn (l a compile-time constant in each loop); consecutive lanes take
+// consecutive tiles (mostly of one column pair, whose coefficient rows they
+// then read as broadcasts). Persistent: each block loops over centres,
+// prefetching the next centre's coefficient tile with cp.async while it
+// works on the current one.
 template <int L>
 __global__ void __launch_bounds__(kThreads)
 ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X,
@@ -142,19 +145,23 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
   constexpr int L1 = L + 1, RS = row_stride(L);
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
-  const int Sn = fd.Sn, Bp = fd.Bp, tile = Sn * RS;
-  float * cbuf = smf;  // two coefficient tiles [Sn][RS]
-  uint16_t * tiles = reinterpret_cast<uint16_t *>(smf + 2 * tile);  // i | j << 8 of each task
+  const int Sn = fd.Sn, tile = Sn * RS;
+  float * cbuf = smf;                                          // two coefficient tiles [Sn][RS]
+  int2 * tab = reinterpret_cast<int2 *>(smf + 2 * tile);       // task table
   __shared__ float red[32];
   const int np = (Sn + 1) >> 1, nt = np * (np + 1) / 2;
   for (int t = threadIdx.x; t < nt; t += blockDim.x) {
     int j = int((sqrtf(8.f * float(t) + 1.f) - 1.f) * 0.5f);
     while (j > 0 && j * (j + 1) / 2 > t) --j;
     while ((j + 1) * (j + 2) / 2 <= t) ++j;
-    tiles[t] = uint16_t((t - j * (j + 1) / 2) | (j << 8));
+    const int i = t - j * (j + 1) / 2;
+    int base, lstep;
+    tile_column(fd, i, j, base, lstep);
+    tab[t] = make_int2(int(uint32_t(i) | (uint32_t(j) << 8) | (uint32_t(lstep / 4) << 16)), base);
   }
-  // zero columns: the end of every l-block after its tiles, then the row's tail
-  const int padb = Bp - 4 * nt, tail = fd.Dg - L1 * Bp;
+  // zero columns: the end of every segment after its tiles
+  const int padD = fd.lenD - 4 * L1 * fd.TD, padO = fd.lenO - 4 * L1 * fd.TO;
+  const int nD = fd.G * padD, npad = nD + fd.G * (fd.G - 1) / 2 * padO;
   auto prefetch = [&](int64_t c, float * dst) {
     const float4 * src = reinterpret_cast<const float4 *>(C + size_t(c) * tile);
     for (int e = threadIdx.x; e < tile / 4; e += blockDim.x) cp_async16(dst + 4 * e, src + e);
@@ -174,14 +181,20 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
     float * Xr = X ? X + roff : nullptr;
     __nv_bfloat16 * hr = Xh + roff;
     __nv_bfloat16 * lr = Xl + roff;
-    float ss = fwd_blocks<L, 0>(Cp, Sn, Bp, nt, tiles, Xr, hr, lr);
-    for (int e = threadIdx.x; e < L1 * padb + tail; e += blockDim.x) {
+    float ss = fwd_blocks<L, 0>(Cp, Sn, nt, tab, Xr, hr, lr);
+    for (int e = threadIdx.x; e < npad; e += blockDim.x) {
       int d;
-      if (e < L1 * padb) {
-        const int l = e / padb;
-        d = l * Bp + 4 * nt + (e - l * padb);
+      if (e < nD) {
+        const int A = e / padD;
+        d = segment_offset(fd, A, A) + 4 * L1 * fd.TD + (e - A * padD);
       } else {
-        d = L1 * Bp + (e - L1 * padb);
+        int k = (e - nD) / padO, A = 0;
+        const int r = (e - nD) - k * padO;
+        while (k >= fd.G - 1 - A) {
+          k -= fd.G - 1 - A;
+          ++A;
+        }
+        d = segment_offset(fd, A, A + 1 + k) + 4 * L1 * fd.TO + r;
       }
       hr[d] = __float2bfloat16_rn(0.f);
       lr[d] = __float2bfloat16_rn(0.f);
@@ -197,14 +210,64 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
 }
 
 // ---------------------------------------------------------------- backward
+// Every 4-column chunk (one 2 x 2 tile) of a packed row: its slot in the
+// per-centre triangle order of the backward's shared memory (tile (i, j) of
+// l at l NT + j(j+1)/2 + i, NT tiles per l) in bits 0-23 and its segment's
+// groups A, B in bits 24-27 and 28-31; kNoChunk for segment padding.
+constexpr uint32_t kNoChunk = 0xFFFFFFFFu;
+__global__ void chunk_map_kernel(FeatureDims fd, uint32_t * __restrict__ map) {
+  const int c = int(blockIdx.x) * int(blockDim.x) + int(threadIdx.x);
+  if (c >= fd.Dg / 4) return;
+  const int LD = fd.lenD / 4, LO = fd.lenO / 4, L1 = fd.L + 1;
+  const int np = (fd.Sn + 1) / 2, NT = np * (np + 1) / 2;
+  int q = c, A = 0;
+  while (q >= LD + (fd.G - 1 - A) * LO) {  // segments (A, A..G-1) in turn
+    q -= LD + (fd.G - 1 - A) * LO;
+    ++A;
+  }
+  int B, T;
+  if (q < LD) {
+    B = A;
+    T = fd.TD;
+  } else {
+    q -= LD;
+    const int k = q / LO;
+    B = A + 1 + k;
+    q -= k * LO;
+    T = fd.TO;
+  }
+  const int lr = q / T;  // 0 for l = L (l descends inside a segment)
+  if (lr >= L1) {
+    map[c] = kNoChunk;
+    return;
+  }
+  const int t = q - lr * T;
+  int ii, jj;
+  if (A < B) {
+    jj = t / fd.npg;
+    ii = t - jj * fd.npg;
+  } else {
+    jj = 0;
+    while ((jj + 1) * (jj + 2) / 2 <= t) ++jj;
+    ii = t - jj * (jj + 1) / 2;
+  }
+  const int i = A * fd.npg + ii, j = B * fd.npg + jj;
+  map[c] = uint32_t((fd.L - lr) * NT + j * (j + 1) / 2 + i) | (uint32_t(A) << 24) | (uint32_t(B) << 28);
+}
+
 // Per centre: the projected gradient G = (g - x (x.g)) / |p| of the packed
 // row (x as BF16 hi + lo, g = dE/dx) is formed in shared memory in two
 // passes (the first stores g and reduces x.g, the second, an L2 re-read of
-// x, projects in place), then dE/dc = lf_l H_l c_l with the symmetric
+// x, projects in place), each 16-byte chunk (one 2 x 2 tile) going to its
+// slot of the per-l triangles (chunk_map). A chunk of a species pair the
+// centre has no neighbour of is neither read nor trusted (x is zero there,
+// and the GAP backward leaves such columns unwritten when no row of the GEMM
+// tile holds the pair): its slot is set to zero. Then dE/dc = lf_l H_l c_l with the
+// symmetric
 //   H_l[I][J] = sqrt2 G_l(I J)  (I != J),   H_l[I][I] = 2 G_l(I I),
 // the derivative of E through the packed entries sqrt2 G_l[I][J] (I < J) and
-// G_l[I][I] of the Gram matrix, read straight from the packed tiles: tile
-// (i, j), i <= j, holds rows 2i, 2i+1 and columns 2j, 2j+1.
+// G_l[I][I] of the Gram matrix, read straight from the tiles: tile (i, j),
+// i <= j, holds rows 2i, 2i+1 and columns 2j, 2j+1.
 //
 // Contraction tasks are (row pair 2ip, 2ip+1; 4-wide column group g of the
 // padded coefficient rows) with g fastest, so the lanes of a half-warp share
@@ -217,15 +280,17 @@ template <int L>
 __global__ void __launch_bounds__(kBwdThreads, 4)
 ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
                   const __nv_bfloat16 * __restrict__ Xl, const float * __restrict__ row_scale,
-                  const float * __restrict__ dX, float * __restrict__ dC) {
+                  const float * __restrict__ dX, const uint32_t * __restrict__ chunk_map,
+                  const uint32_t * __restrict__ present, float * __restrict__ dC) {
   constexpr int L1 = L + 1, RS = row_stride(L), K = L1 * L1;
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
-  const int Sn = fd.Sn, Bp = fd.Bp, OS = Sn | 1;
+  const int Sn = fd.Sn, OS = Sn | 1;
+  const int NP = (Sn + 1) >> 1, NT = NP * (NP + 1) / 2;
   const int tile = Sn * RS, tileP = (Sn + (Sn & 1)) * RS;  // a coefficient tile; its buffer
   float * Cb = smf;                // two coefficient buffers [Sn rounded up to even][RS]
-  float * Ts = Cb + 2 * tileP;     // packed G: L1 blocks of Bp
-  float * Os = Ts + L1 * Bp;       // dE/dc of the centre: [K][OS]
+  float * Ts = Cb + 2 * tileP;     // G: L1 triangles of NT tiles
+  float * Os = Ts + 4 * L1 * NT;   // dE/dc of the centre: [K][OS]
   __shared__ float red[32];
   // column groups of the contraction: the 4-wide chunks of the padded
   // coefficient row in order (group g covers columns 4g .. 4g+3, of block
@@ -240,8 +305,7 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
   }
   // the row after an odd S n's last row stays zero in both buffers
   for (int e = tile + threadIdx.x; e < tileP; e += blockDim.x) Cb[e] = Cb[tileP + e] = 0.f;
-  const int nq = (L1 * Bp) >> 2;  // 4-column chunks holding packed entries (the rest of the row is zero)
-  const int NP = (Sn + 1) >> 1;
+  const int nq = fd.Dg >> 2;  // 4-column chunks of the row (one tile each)
   float4 * T4 = reinterpret_cast<float4 *>(Ts);
   auto prefetch = [&](int64_t c, float * dst) {
     const float4 * src = reinterpret_cast<const float4 *>(C + size_t(c) * tile);
@@ -269,11 +333,21 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
     const uint2 * xl = reinterpret_cast<const uint2 *>(Xl + size_t(row) * fd.Dg);
     const float4 * g4 = reinterpret_cast<const float4 *>(dX + size_t(row) * fd.Dg);
     const float rs = row_scale[row];  // x = rs * p; G = rs * (g - x (x.g))
+    const uint32_t pm = fd.G > 1 ? present[ci] : 0xFFFFFFFFu;  // species with neighbours (the groups)
+    auto live = [&](uint32_t e) {
+      return e != kNoChunk && ((pm >> ((e >> 24) & 15u)) & 1u) && ((pm >> (e >> 28)) & 1u);
+    };
     float dot = 0.f;
 #pragma unroll 4
     for (int c = threadIdx.x; c < nq; c += blockDim.x) {
+      const uint32_t e = __ldg(chunk_map + c);
+      if (e == kNoChunk) continue;
+      if (!live(e)) {
+        T4[e & 0xFFFFFFu] = make_float4(0.f, 0.f, 0.f, 0.f);
+        continue;
+      }
       const float4 gq = __ldcs(g4 + c);
-      T4[c] = gq;
+      T4[e & 0xFFFFFFu] = gq;
       if (a.normalize) {
         const uint2 hv = xh[c], lv = xl[c];
         const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
@@ -285,20 +359,23 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
       }
     }
     if (a.normalize) {
-      dot = block_sum_f(dot, red) * rs;  // padding columns are zero in p and g
+      dot = block_sum_f(dot, red) * rs;  // x is zero in the chunks left out
       const float k = rs * dot;
       // each thread projects the chunks it stored
 #pragma unroll 4
       for (int c = threadIdx.x; c < nq; c += blockDim.x) {
+        const uint32_t e = __ldg(chunk_map + c);
+        if (!live(e)) continue;
+        const int d = int(e & 0xFFFFFFu);
         const uint2 hv = __ldcs(xh + c), lv = __ldcs(xl + c);
         const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
         const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
-        float4 t = T4[c];
+        float4 t = T4[d];
         t.x = (t.x - (__bfloat162float(hb[0]) + __bfloat162float(lb[0])) * k) * rs;
         t.y = (t.y - (__bfloat162float(hb[1]) + __bfloat162float(lb[1])) * k) * rs;
         t.z = (t.z - (__bfloat162float(hb[2]) + __bfloat162float(lb[2])) * k) * rs;
         t.w = (t.w - (__bfloat162float(hb[3]) + __bfloat162float(lb[3])) * k) * rs;
-        T4[c] = t;
+        T4[d] = t;
       }
     }
     cp_async_wait<1>();  // this centre's coefficients have landed ...
@@ -309,11 +386,10 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
     for (int t = threadIdx.x; t < kG * NP; t += blockDim.x) {
       const int ip = t / kG, g = t - ip * kG;
       const int l = grp_l[g];
-      const float4 * Tl = reinterpret_cast<const float4 *>(Ts + l * Bp);
-      const float * cb = Cp + 4 * g;
+      const float4 * Tl = T4 + l * NT;
       const int i0 = 2 * ip;
       float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
-      // h_rc = G(i0 + r, J0 + c), cj = row J0 of the coefficients (row S n of
+      // h_rc = G(i0 + r, 2j + c), cj = row 2j of the coefficients (row S n of
       // an odd S n is the buffer's zero row, and its h are zero)
       auto acc = [&](float h00, float h10, float h01, float h11, const float * cj) {
         const float4 c0 = *reinterpret_cast<const float4 *>(cj);
@@ -328,7 +404,7 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
         a1.w += h10 * c0.w + h11 * c1.w;
       };
       const float4 * tp = Tl + ip * (ip + 1) / 2;  // tile (0, ip)
-      const float * cj = cb;
+      const float * cj = Cp + 4 * g;
 #pragma unroll 2
       for (int j = 0; j < ip; ++j, cj += 2 * RS) {
         const float4 v = tp[j];  // (2j, i0), (2j+1, i0), (2j, i0+1), (2j+1, i0+1)
@@ -372,15 +448,15 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
 template <int L>
 size_t fwd_smem(const FeatureDims & fd) {
   const size_t np = size_t(fd.Sn + 1) / 2;
-  return sizeof(float) * 2 * size_t(fd.Sn) * row_stride(L) + sizeof(uint16_t) * np * (np + 1) / 2 + 16;
+  return sizeof(float) * 2 * size_t(fd.Sn) * row_stride(L) + sizeof(int2) * np * (np + 1) / 2 + 16;
 }
 
-// Shared memory of the backward: two coefficient buffers, the packed G row
-// and the staged dE/dc rows.
+// Shared memory of the backward: two coefficient buffers, the per-l
+// triangles of G and the staged dE/dc rows.
 template <int L>
 size_t bwd_smem(const FeatureDims & fd) {
-  const size_t Sn = size_t(fd.Sn), K = size_t(L + 1) * (L + 1);
-  return sizeof(float) * (2 * (Sn + (Sn & 1)) * row_stride(L) + size_t(L + 1) * fd.Bp + K * (Sn | 1));
+  const size_t Sn = size_t(fd.Sn), K = size_t(L + 1) * (L + 1), np = (Sn + 1) / 2;
+  return sizeof(float) * (2 * (Sn + (Sn & 1)) * row_stride(L) + 4 * size_t(L + 1) * np * (np + 1) / 2 + K * (Sn | 1));
 }
 
 // Blocks of a persistent kernel: as many as fit on the device at once (at
@@ -441,9 +517,13 @@ void launch_ps_fwd_fast(const PsArgs & a, const float * C, float * X, __nv_bfloa
 }
 
 void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh, const __nv_bfloat16 * Xl,
-                        const float * row_scale, const float * dX, float * dC, cudaStream_t st) {
+                        const float * row_scale, const float * dX, uint32_t * chunk_map, const uint32_t * present,
+                        float * dC, cudaStream_t st) {
   if (a.n_centers == 0) return;
   if (a.fd.n > kMaxN) throw Error(RGPU_ERR_INVALID_ARGUMENT, "max_radial above 16 is not supported on the fast path");
+  const int nchunk = a.fd.Dg / 4;
+  chunk_map_kernel<<<div_up(nchunk, 256), 256, 0, st>>>(a.fd, chunk_map);
+  RGPU_LAUNCHED();
   constexpr size_t kMaxSmem = 227 * 1024 - 2048;
   const int threads = std::min(tile_config(a.fd.S, a.fd.n, a.fd.L).psb_threads, kBwdThreads);
 #define RGPU_PSB_CASE(LL)                                                                                     \
@@ -455,7 +535,7 @@ void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 *
     RGPU_CUDA(cudaFuncSetAttribute(ps_bwd_f32_kernel<LL>, cudaFuncAttributeMaxDynamicSharedMemorySize,        \
                                    int(smem)));                                                               \
     ps_bwd_f32_kernel<LL><<<persistent_grid(ps_bwd_f32_kernel<LL>, threads, smem, a.n_centers),               \
-                            threads, smem, st>>>(a, C, Xh, Xl, row_scale, dX, dC);                            \
+                            threads, smem, st>>>(a, C, Xh, Xl, row_scale, dX, chunk_map, present, dC);        \
     break;                                                                                                    \
   }
   switch (a.fd.L) {

@@ -98,7 +98,8 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 struct TcPsPlan {
   int T;         // centres per tile
   int ops;       // bytes of the operand tiles
-  int stage;     // bytes of one staging buffer: T x Bp x (hi, lo) BF16
+  int stage;     // bytes of one staging buffer: T x 4 ntile x (hi, lo) BF16
+  int ntile;     // 2 x 2 tiles of one l-block of a row
 };
 
 template <int L>
@@ -115,7 +116,10 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
   __shared__ float nrm_s[kRows];
   const FeatureDims fd = a.fd;
   const int n = fd.n, S = fd.S, Sn = S * n, T = plan.T;
-  const int blk = fd.Bp;  // one packed l-block of a row
+  const int blk = 4 * plan.ntile;  // one l-block of a row in staging (tiles in task order)
+  // task table: row pair i, column pair j and the segment's tiles per l in
+  // .x = i | j << 8 | T << 16, the tile's first column at l = L in .y
+  int2 * tab = reinterpret_cast<int2 *>(ops + plan.ops + 2 * plan.stage);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
@@ -129,6 +133,17 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
   // padding) no epilogue writes
   for (int e = threadIdx.x; e < (plan.ops + 2 * plan.stage) / 16; e += blockDim.x)
     reinterpret_cast<uint4 *>(ops)[e] = make_uint4(0u, 0u, 0u, 0u);
+  for (int r = threadIdx.x; r < plan.ntile; r += blockDim.x) {
+    int j = int((sqrtf(8.f * float(r) + 1.f) - 1.f) * 0.5f);
+    while (j > 0 && j * (j + 1) / 2 > r) --j;
+    while ((j + 1) * (j + 2) / 2 <= r) ++j;
+    const int i = r - j * (j + 1) / 2;
+    int base, lstep;
+    tile_column(fd, i, j, base, lstep);
+    tab[r] = make_int2(int(uint32_t(i) | (uint32_t(j) << 8) | (uint32_t(lstep / 4) << 16)), base);
+  }
+  const int padD = fd.lenD - 4 * (L + 1) * fd.TD, padO = fd.lenO - 4 * (L + 1) * fd.TO;
+  const int nD = fd.G * padD, npad = nD + fd.G * (fd.G - 1) / 2 * padO;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
                  "r"(uint32_t(kTmemCols)));
@@ -189,10 +204,10 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
       ++commits[b];
     };
     if (threadIdx.x == 0) issue(0);
-    // per-thread row: centre t, species a, radial n1
+    // per-thread row: centre t, row my_i = a n + n1 of its Gram block (species a)
     const int r = warp * 32 + lane;
     const int my_t = r / Sn, my_i = r - my_t * Sn;
-    const int my_a = my_i / n, my_n1 = my_i - my_a * n;
+    const int my_a = my_i / n;
     const bool row_ok = my_t < nt;
     const int t_lo = (warp * 32) / Sn, t_hi = std::min((warp * 32 + 31) / Sn, nt - 1);
     float nrm = 0.f;
@@ -232,15 +247,15 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
       }
       tc_fence_before();
       __syncthreads();
-      // the centres' packed l-blocks: contiguous in their rows
-      const int chunks = blk / 8;  // 16-byte chunks of one block
-      for (int e = threadIdx.x; e < 2 * nt * chunks; e += blockDim.x) {
-        const int half = e / (nt * chunks), rem = e - half * (nt * chunks);
-        const int t = rem / chunks, cch = rem - t * chunks;
+      // each staged tile (8 bytes of hi, 8 of lo) to its column of the packed row
+      for (int e = threadIdx.x; e < 2 * nt * plan.ntile; e += blockDim.x) {
+        const int half = e / (nt * plan.ntile), rem = e - half * (nt * plan.ntile);
+        const int t = rem / plan.ntile, r = rem - t * plan.ntile;
         const int64_t row = a.row_of_center[c0 + t];
-        const uint4 * src = reinterpret_cast<const uint4 *>((half ? sl : sh) + t * blk) + cch;
-        __nv_bfloat16 * dstb = (half ? Xl : Xh) + size_t(row) * fd.Dg + size_t(l) * blk;
-        reinterpret_cast<uint4 *>(dstb)[cch] = *src;
+        const int2 te = tab[r];
+        const int col = te.y + 4 * (L - l) * int(uint32_t(te.x) >> 16);
+        const uint2 * src = reinterpret_cast<const uint2 *>((half ? sl : sh) + t * blk + 4 * r);
+        *reinterpret_cast<uint2 *>((half ? Xl : Xh) + size_t(row) * fd.Dg + col) = *src;
       }
     }
     if (!ok) break;
@@ -251,13 +266,25 @@ ps_fwd_tc_kernel(PsArgs a, TcPsPlan plan, const float * __restrict__ C, __nv_bfl
       const float nv = sqrtf(nrm_s[t]);
       row_scale[row] = (a.normalize && nv > 0.f) ? 1.f / nv : 1.f;
     }
-    // padding columns of the rows
-    const int used = (L + 1) * blk, padc = fd.Dg - used;
-    for (int e = threadIdx.x; e < nt * padc; e += blockDim.x) {
-      const int t = e / padc, c = used + (e - t * padc);
+    // the end of every segment after its tiles, in every row of the tile
+    for (int e = threadIdx.x; e < nt * npad; e += blockDim.x) {
+      const int t = e / npad, p = e - t * npad;
+      int d;
+      if (p < nD) {
+        const int A = p / padD;
+        d = segment_offset(fd, A, A) + 4 * (L + 1) * fd.TD + (p - A * padD);
+      } else {
+        int k = (p - nD) / padO, A = 0;
+        const int r = (p - nD) - k * padO;
+        while (k >= fd.G - 1 - A) {
+          k -= fd.G - 1 - A;
+          ++A;
+        }
+        d = segment_offset(fd, A, A + 1 + k) + 4 * (L + 1) * fd.TO + r;
+      }
       const int64_t row = a.row_of_center[c0 + t];
-      Xh[size_t(row) * fd.Dg + c] = __float2bfloat16_rn(0.f);
-      Xl[size_t(row) * fd.Dg + c] = __float2bfloat16_rn(0.f);
+      Xh[size_t(row) * fd.Dg + d] = __float2bfloat16_rn(0.f);
+      Xl[size_t(row) * fd.Dg + d] = __float2bfloat16_rn(0.f);
     }
     __syncthreads();  // nrm_s and the operands are rewritten by the next tile
   }
@@ -284,8 +311,9 @@ bool ps_fwd_tc_supported(const FeatureDims & fd) {
   if (Sn > kRows || fd.n % 4 != 0 || fd.L > kMaxL) return false;
   const int T = kRows / Sn;
   const size_t ops = size_t(op_off(fd.L + 1));
-  const size_t stage = 2 * size_t(T) * fd.Bp * 2 * sizeof(__nv_bfloat16);
-  return ops + stage + 256 <= size_t(227 * 1024 - 4096);
+  const size_t ntile = size_t(Sn / 2) * (Sn / 2 + 1) / 2;
+  const size_t stage = 2 * size_t(T) * 4 * ntile * 2 * sizeof(__nv_bfloat16);
+  return ops + stage + sizeof(int2) * ntile + 256 <= size_t(227 * 1024 - 4096);
 }
 
 void launch_ps_fwd_tc(const PsArgs & a, const float * C, __nv_bfloat16 * Xh, __nv_bfloat16 * Xl, float * row_scale,
@@ -295,8 +323,10 @@ void launch_ps_fwd_tc(const PsArgs & a, const float * C, __nv_bfloat16 * Xh, __n
   TcPsPlan plan;
   plan.T = kRows / (a.fd.S * a.fd.n);
   plan.ops = op_off(a.fd.L + 1);
-  plan.stage = 2 * plan.T * a.fd.Bp * int(sizeof(__nv_bfloat16));  // hi + lo of one l
-  const size_t smem = std::max(kMinSmem, size_t(plan.ops) + 2 * size_t(plan.stage) + 256);
+  plan.ntile = (a.fd.Sn / 2) * (a.fd.Sn / 2 + 1) / 2;
+  plan.stage = 2 * plan.T * 4 * plan.ntile * int(sizeof(__nv_bfloat16));  // hi + lo of one l
+  const size_t smem =
+      std::max(kMinSmem, size_t(plan.ops) + 2 * size_t(plan.stage) + sizeof(int2) * plan.ntile + 256);
   int dev = 0, sms = 0;
   RGPU_CUDA(cudaGetDevice(&dev));
   RGPU_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

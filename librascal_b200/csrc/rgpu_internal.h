@@ -195,9 +195,12 @@ struct FeatureDims {
   int P;      // species pairs S(S+1)/2
   int D;      // P*n*n*(L+1)
   int Dpad;   // D rounded up to 32
-  int Sn;     // S*n: rows of a centre's per-l Gram matrix (packed layout below)
-  int Bp;     // columns of one l-block of the packed layout: 2 ceil(Sn/2)(ceil(Sn/2)+1) rounded up to 8
-  int Dg;     // row length of the packed layout: (L+1) Bp rounded up to 32
+  // packed layout of the FP32 path (below)
+  int Sn;          // S*n: rows of a centre's per-l Gram matrix
+  int G, npg;      // groups of row pairs (S when n is even, else 1) and pairs per group
+  int TD, TO;      // 2 x 2 tiles per l of a diagonal / off-diagonal block of groups
+  int lenD, lenO;  // columns of a diagonal / off-diagonal segment (all l), a multiple of 32
+  int Dg;          // row length: G lenD + G(G-1)/2 lenO
 };
 
 // RadialScaling cutoff parameters (on = 0: plain shifted cosine).
@@ -246,22 +249,45 @@ void launch_expansion_selfgrad_fp64(const ExpansionArgs & a, int64_t c0, int64_t
 // (calculator_spherical_invariants.hh:747-794). The packed layout stores the
 // upper triangle of each G_l in 2 x 2 tiles: tile (i, j), i <= j, holds rows
 // 2i, 2i+1 and columns 2j, 2j+1 as four consecutive columns
-//   l Bp + 4 (j (j + 1) / 2 + i) + (I & 1) + 2 (J & 1),
-// entries with I < J multiplied by sqrt2, and the one entry below the
-// diagonal of a diagonal tile (and any row or column beyond S n) zero. That is
-// the reference's feature itself for a < b. For a = b the reference keeps
-// both p(n1 n2) and p(n2 n1), which are equal, and the packed layout one
-// entry sqrt2 p(n1 n2) (n1 < n2): the sum of squares of a packed row is the
-// reference's |p|^2, and its dot product with a sparse point packed the same
-// way (the two entries folded into (t(n1 n2) + t(n2 n1)) / sqrt2) is the
-// reference's x . t, with S n(n-1)/2 (L+1) fewer columns (less the zeros of
-// the diagonal tiles). A tile is 8 bytes of BF16, so every store of the
-// forward is aligned, and the backward reads a tile with one 16-byte load.
-// The reference's dense order, used by the FP64 path and by every export, is
-// ((key*n + n1)*n + n2)*(L+1) + l (property_block_sparse.hh:911-931).
+// (I & 1) + 2 (J & 1), entries with I < J multiplied by sqrt2, and the one
+// entry below the diagonal of a diagonal tile (and any row or column beyond
+// S n) zero. For a < b that is the reference's feature itself. For a = b
+// the reference keeps both p(n1 n2) and p(n2 n1), which are equal, and the
+// packed layout one entry sqrt2 p(n1 n2) (n1 < n2): the sum of squares of a
+// packed row is the reference's |p|^2, and its dot product with a sparse
+// point packed the same way (the two entries folded into
+// (t(n1 n2) + t(n2 n1)) / sqrt2) is the reference's x . t, with
+// S n(n-1)/2 (L+1) fewer columns.
+//
+// Tiles are ordered by the species of their rows: with n even a row pair
+// lies in one species, and the pairs form G = S groups of npg = n/2; with n
+// odd they form one group. Segment (A, B), A <= B in A-major order, holds
+// the tiles of group A's rows and group B's columns for every l (l slowest,
+// then the tile's column pair, then its row pair; TD = npg(npg+1)/2 tiles per
+// l on the diagonal A = B, TO = npg^2 off it), padded with zero columns to a
+// multiple of 32. A centre without a neighbour of species A has zeros in
+// every segment of A, so the GEMMs skip those column ranges for tiles of
+// rows that all lack A. The reference's dense order, used by the FP64 path
+// and by every export, is ((key*n + n1)*n + n2)*(L+1) + l
+// (property_block_sparse.hh:911-931).
+__host__ __device__ inline int segment_offset(const FeatureDims & fd, int A, int B) {
+  // segments before (A, A): A diagonal ones and A(G-1) - A(A-1)/2 off-diagonal ones
+  int o = A * fd.lenD + (A * (fd.G - 1) - A * (A - 1) / 2) * fd.lenO;
+  if (B > A) o += fd.lenD + (B - A - 1) * fd.lenO;
+  return o;
+}
+// First column of tile (i, j), i <= j (row-pair indices), at l = L, and
+// the column step from one l to the next lower one.
+__host__ __device__ inline void tile_column(const FeatureDims & fd, int i, int j, int & base, int & lstep) {
+  const int A = i / fd.npg, B = j / fd.npg, ii = i - A * fd.npg, jj = j - B * fd.npg;
+  const int t = A < B ? jj * fd.npg + ii : jj * (jj + 1) / 2 + ii;
+  base = segment_offset(fd, A, B) + 4 * t;
+  lstep = 4 * (A < B ? fd.TO : fd.TD);
+}
 inline int packed_column(const FeatureDims & fd, int l, int I, int J) {
-  const int j = J >> 1;
-  return l * fd.Bp + 4 * (j * (j + 1) / 2 + (I >> 1)) + (I & 1) + 2 * (J & 1);
+  int base, lstep;
+  tile_column(fd, I >> 1, J >> 1, base, lstep);
+  return base + (fd.L - l) * lstep + (I & 1) + 2 * (J & 1);
 }
 // Column of (key(a, b), n1, n2, l), a <= b, in the reference's dense order.
 inline int reference_column(const FeatureDims & fd, int a, int n1, int b, int n2, int l) {
@@ -308,9 +334,13 @@ void launch_ps_grad_fp64(const PsArgs & a, const ExpansionArgs & e, int64_t c0, 
 // as dC[i][lm][s*n + n'] (lm = l^2 + m; the (species, radial) index is the
 // fastest so that the centre's 32 consecutive rows store coalesced).
 // x is read back as row_scale * (hi + lo) of the forward's BF16 split.
+// chunk_map: scratch of Dg/4 words (the launch fills it with the slot of
+// every 4-column chunk of a row in the kernel's per-l triangle order and its
+// species pair); present: the centres' species masks (the FP32 expansion's),
+// whose absent pairs are taken as zero whatever dX holds there.
 void launch_ps_bwd_fp32(const PsArgs & a, const float * C, const __nv_bfloat16 * Xh,
-                        const __nv_bfloat16 * Xl, const float * row_scale, const float * dX, float * dC,
-                        cudaStream_t st);
+                        const __nv_bfloat16 * Xl, const float * row_scale, const float * dX, uint32_t * chunk_map,
+                        const uint32_t * present, float * dC, cudaStream_t st);
 
 // ------------------------------------------------------------------ GAP
 struct GapSpecies {
@@ -367,6 +397,14 @@ struct Bf16x3Gemm {
   int zeta;
   float * e_part;
   const float * row_scale;
+  // Species skipping over the packed feature columns (grouped launches):
+  // seg_mode 1 skips the K blocks, 2 the N tiles, whose species pair is
+  // absent from every row of an M-tile (tile_mask[mt]: species present in
+  // the tile's rows); seg_G, seg_LD, seg_LO: groups and segment lengths in
+  // units of 32 columns (FeatureDims G, lenD / 32, lenO / 32).
+  const uint32_t * tile_mask = nullptr;
+  int seg_mode = 0;
+  int seg_G = 0, seg_LD = 0, seg_LO = 0;
 };
 constexpr int kTcTileN = 256;
 void gemm_bf16x3(const Bf16x3Gemm & g, cudaStream_t st);
@@ -467,6 +505,22 @@ void launch_pair_adjoint_fp32(const ExpansionArgs & a, const int32_t * pair_cent
                               double * stress = nullptr);
 
 // ------------------------------------------------------------------ helpers
+// Stable sort of centres by (species, presence mask): rows of one species
+// with the same neighbour species become neighbours, so 128-row GEMM tiles
+// share absent species. Replaces row_of_center / center_of_row.
+void launch_mask_sort(int64_t n, const int32_t * types, const int32_t * center_atom, const int8_t * lut,
+                      const uint32_t * present, int S, int32_t * row_of_center, int32_t * center_of_row, DevBuf & tmp,
+                      cudaStream_t st);
+// Per 128-row tile of each species' rows (species s: rows row0[s] ..
+// row0[s] + rows[s], tiles tile_off[s] .. tile_off[s+1]): the OR of the
+// presence masks of its rows.
+struct TileMaskArgs {
+  static constexpr int kSpecies = 16;  // the largest species count of a dense layout
+  int S;
+  int64_t row0[kSpecies], rows[kSpecies], tile_off[kSpecies + 1];
+};
+void launch_tile_masks(const TileMaskArgs & a, const int32_t * center_of_row, const uint32_t * present, uint32_t * out,
+                       cudaStream_t st);
 void launch_species_sort(int64_t n, const int32_t * types, const int32_t * center_atom,
                          const int8_t * lut, int S, int64_t * species_count /*[S]*/,
                          int32_t * row_of_center, int32_t * center_of_row, DevBuf & tmp,

@@ -265,6 +265,80 @@ __global__ void species_total_kernel(const int64_t * __restrict__ counts, int S,
   out[s] = t;
 }
 
+// ---- stable sort of centres by (species, species-presence mask): LSD
+// passes of 5 bits over key = species << S | mask
+__global__ void mask_key_kernel(int64_t n, const int32_t * __restrict__ types, const int32_t * __restrict__ center_atom,
+                                const int8_t * __restrict__ lut, const uint32_t * __restrict__ present, int S,
+                                uint32_t * __restrict__ key, int32_t * __restrict__ order) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t m = S >= 32 ? present[i] : present[i] & ((1u << S) - 1u);
+  key[i] = (uint32_t(lut[types[center_atom[i]]]) << S) | m;
+  order[i] = int32_t(i);
+}
+
+__global__ void digit_count_kernel(int64_t n, const int32_t * __restrict__ order, const uint32_t * __restrict__ key,
+                                   int shift, int64_t * __restrict__ block_counts /*[32][nb]*/, int nb) {
+  __shared__ int cnt[32];
+  if (threadIdx.x < 32) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t k = int64_t(blockIdx.x) * kSortBlock + threadIdx.x;
+  if (k < n) atomicAdd(&cnt[(key[order[k]] >> shift) & 31u], 1);
+  __syncthreads();
+  if (threadIdx.x < 32) block_counts[int64_t(threadIdx.x) * nb + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Stable: positions keep their order within a digit (the tail of the last
+// block takes digit 31 and sits after every real position, so it never
+// counts before one).
+__global__ void digit_rank_kernel(int64_t n, const int32_t * __restrict__ order_in, const uint32_t * __restrict__ key,
+                                  int shift, const int64_t * __restrict__ block_off /*[32][nb] scanned*/, int nb,
+                                  int32_t * __restrict__ order_out) {
+  __shared__ int wcnt[32][32];  // [warp][digit]
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  wcnt[wid][lane] = 0;
+  __syncthreads();
+  const int64_t k = int64_t(blockIdx.x) * kSortBlock + threadIdx.x;
+  const int32_t c = k < n ? order_in[k] : 0;
+  const int d = k < n ? int((key[c] >> shift) & 31u) : 31;
+  const unsigned same = __match_any_sync(0xffffffffu, d);
+  const int rank_w = __popc(same & lanemask_lt());
+  if ((same & lanemask_lt()) == 0) wcnt[wid][d] = __popc(same);
+  __syncthreads();
+  if (k < n) {
+    int before = 0;
+    for (int w = 0; w < wid; ++w) before += wcnt[w][d];
+    order_out[block_off[int64_t(d) * nb + blockIdx.x] + before + rank_w] = c;
+  }
+}
+
+__global__ void rows_from_order_kernel(int64_t n, const int32_t * __restrict__ order, int32_t * __restrict__ row_of_center,
+                                       int32_t * __restrict__ center_of_row) {
+  const int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const int32_t c = order[k];
+  row_of_center[c] = int32_t(k);
+  center_of_row[k] = c;
+}
+
+static_assert(TileMaskArgs::kSpecies >= kMaxSpecies, "tile masks cover every species");
+
+// One warp per 128-row tile of each species' rows: the OR of its rows'
+// presence masks.
+__global__ void tile_mask_kernel(TileMaskArgs a, const int32_t * __restrict__ center_of_row,
+                                 const uint32_t * __restrict__ present, uint32_t * __restrict__ out) {
+  const int64_t t = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (t >= a.tile_off[a.S]) return;
+  int s = 0;
+  while (t >= a.tile_off[s + 1]) ++s;
+  const int64_t r0 = a.row0[s] + (t - a.tile_off[s]) * 128, r1 = min(r0 + 128, a.row0[s] + a.rows[s]);
+  uint32_t m = 0;
+  for (int64_t r = r0 + lane; r < r1; r += 32) m |= present[center_of_row[r]];
+  m = __reduce_or_sync(0xffffffffu, m);
+  if (lane == 0) out[t] = m;
+}
+
 __global__ void round_tf32_kernel(float * x, int64_t n) {
   int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i < n) x[i] = to_tf32(x[i]);
@@ -288,6 +362,44 @@ void scan_exclusive_i32to64(const int32_t * in, int64_t * out, int64_t n, DevBuf
                             cudaStream_t st) {
   tmp.ensure(scan_tmp_bytes(n));
   scan_impl<int32_t>(in, out, n, tmp, 0, st);
+}
+
+void launch_mask_sort(int64_t n, const int32_t * types, const int32_t * center_atom, const int8_t * lut,
+                      const uint32_t * present, int S, int32_t * row_of_center, int32_t * center_of_row, DevBuf & tmp,
+                      cudaStream_t st) {
+  if (n <= 0) return;
+  const int nb = div_up(n, kSortBlock);
+  const size_t cnt = size_t(32) * nb + 1;
+  const size_t stmp = scan_tmp_bytes(int64_t(32) * nb);
+  const size_t ibytes = (sizeof(int32_t) * size_t(n) + 255) / 256 * 256;
+  tmp.ensure(3 * ibytes + 2 * sizeof(int64_t) * cnt + stmp + 256);
+  char * base = static_cast<char *>(tmp.p);
+  uint32_t * key = reinterpret_cast<uint32_t *>(base);
+  int32_t * ord[2] = {reinterpret_cast<int32_t *>(base + ibytes), reinterpret_cast<int32_t *>(base + 2 * ibytes)};
+  int64_t * counts = reinterpret_cast<int64_t *>(base + 3 * ibytes);
+  int64_t * offs = counts + cnt;
+  const size_t scan_off = 3 * ibytes + 2 * sizeof(int64_t) * cnt;
+  mask_key_kernel<<<div_up(n, 256), 256, 0, st>>>(n, types, center_atom, lut, present, S, key, ord[0]);
+  RGPU_LAUNCHED();
+  const int bits = S + 5;  // species index below 32
+  int cur = 0;
+  for (int shift = 0; shift < bits; shift += 5, cur ^= 1) {
+    digit_count_kernel<<<nb, kSortBlock, 0, st>>>(n, ord[cur], key, shift, counts, nb);
+    RGPU_LAUNCHED();
+    scan_impl<int64_t>(counts, offs, int64_t(32) * nb, tmp, scan_off, st);
+    digit_rank_kernel<<<nb, kSortBlock, 0, st>>>(n, ord[cur], key, shift, offs, nb, ord[cur ^ 1]);
+    RGPU_LAUNCHED();
+  }
+  rows_from_order_kernel<<<div_up(n, 256), 256, 0, st>>>(n, ord[cur], row_of_center, center_of_row);
+  RGPU_LAUNCHED();
+}
+
+void launch_tile_masks(const TileMaskArgs & a, const int32_t * center_of_row, const uint32_t * present, uint32_t * out,
+                       cudaStream_t st) {
+  const int64_t tiles = a.tile_off[a.S];
+  if (tiles <= 0) return;
+  tile_mask_kernel<<<div_up(tiles * 32, 256), 256, 0, st>>>(a, center_of_row, present, out);
+  RGPU_LAUNCHED();
 }
 
 void launch_species_sort(int64_t n, const int32_t * types, const int32_t * center_atom,

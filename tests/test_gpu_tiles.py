@@ -1,7 +1,12 @@
 """Every launch shape the autotuner can choose gives the same FP32 results:
 each candidate of each tile field, on the molecule-cluster shape (5
 species, n 8, l 6) and on the bulk shape (2 species, n 12, l 9), against
-the FP64 oracle at the FP32 bar (1e-4 of the largest value)."""
+the FP64 oracle at the FP32 bar (1e-4 of the largest value). A structure
+energy sum_atoms sum_m alpha_m k^2 (|k| <= 1) can be a small remainder of
+large terms of both signs (the single 300-atom box here: 12 from terms of
+up to 7 000 in total); its bar is then 1e-6 of that total magnitude, the
+size of the rounding of FP32 kernel values k (about 1e-7 relative) summed
+over every (atom, sparse point) term."""
 import numpy as np
 import pytest
 
@@ -19,10 +24,14 @@ def _case(batch, kw, n_sparse):
     sp = rb.SparsePoints(calc)
     sp.add_dense(sps, T, calc.get_keys(species))
     model = rb.GAPModel(calc, sp, alpha, 2)
+    # total magnitude of a structure's energy terms: atoms x sum_m |alpha_m|
+    scale = np.diff(batch["atom_offsets"]).max() * np.abs(alpha).sum()
+    E_ref = (E_ref, scale)
     return model, E_ref, F_ref, (len(species), kw["n"], kw["l"])
 
 
 def _check(model, batch, E_ref, F_ref, shape, cfg):
+    E_ref, scale = E_ref
     old = tune.get_config(shape)
     try:
         tune.set_config(shape, cfg)
@@ -31,7 +40,7 @@ def _check(model, batch, E_ref, F_ref, shape, cfg):
         E, F = model.predict(st, "fp32")
     finally:
         tune.set_config(shape, old)
-    assert np.abs(E - E_ref).max() <= 1e-4 * np.abs(E_ref).max()
+    assert np.abs(E - E_ref).max() <= max(1e-4 * np.abs(E_ref).max(), 1e-6 * scale)
     assert np.abs(F - F_ref).max() <= 1e-4 * np.abs(F_ref).max()
 
 

@@ -2,7 +2,8 @@
 test hook (no GPU).
 
 The FP32 path stores each centre's power-spectrum row as the upper triangles
-of the per-l Gram matrices of its coefficients in 2 x 2 tiles: the two equal
+of the per-l Gram matrices of its coefficients in 2 x 2 tiles, grouped into
+segments by the species of their rows and columns: the two equal
 same-species features p(n1 n2 l) and p(n2 n1 l) of the reference's row
 (calculator_spherical_invariants.hh:747-794) share one column. Packing must
 keep every quantity the GAP path takes from a row: its norm and its dot
@@ -56,10 +57,16 @@ def pack(S, n, L, ref):
 
 
 def test_benchmark_shape_sizes():
-    # 5 species, n 8, l 6: 6 720 reference columns, 7 l-blocks of 210 tiles
-    assert sizes(5, 8, 6) == (6720, 5888)
-    # 2 species, n 12, l 9: 10 l-blocks of 78 tiles
-    assert sizes(2, 12, 9) == (4320, 3136)
+    # 5 species, n 8, l 6: 6 720 reference columns; 5 same-species segments
+    # of 7 x 10 tiles (280 columns, padded to 288) and 10 cross-species
+    # segments of 7 x 16 tiles (448 columns)
+    assert sizes(5, 8, 6) == (6720, 5 * 288 + 10 * 448)
+    # 2 species, n 12, l 9: 2 segments of 10 x 21 tiles (840, padded to 864)
+    # and one of 10 x 36 (1 440)
+    assert sizes(2, 12, 9) == (4320, 2 * 864 + 1440)
+    # odd n: one segment holding the whole triangle (3 x 6 tiles, 72 columns,
+    # padded to 96)
+    assert sizes(2, 3, 2) == (3 * 9 * 3, 96)
 
 
 @pytest.mark.parametrize("S,n,L", [(1, 3, 2), (2, 3, 1), (3, 3, 2), (2, 4, 3), (5, 8, 6)])
