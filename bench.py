@@ -294,7 +294,7 @@ def fma_peaks(lib):
 # workload: the average of the forward and backward launches of one ncu
 # capture of the 2 000-cluster case (32 505 atoms), scaled by atoms to
 # 160 449 atoms.
-GEMM_TRAFFIC_PER_LAUNCH = 0.5 * (1.498e9 + 1.766e9) * 160449 / 32505
+GEMM_TRAFFIC_PER_LAUNCH = 0.5 * (1.233e9 + 1.872e9) * 160449 / 32505
 
 
 def row_stride(L):
@@ -329,6 +329,33 @@ def stage_roofline(stages, nc, n_pairs, n_atoms, S, n, L, Dg, hbm, fp32):
                       frac_hbm=(gbs / hbm) if gbs else None)
     out["peaks"] = dict(hbm_gbs=hbm, fp32_tflops_measured=fp32)
     return out
+def gemm_flops_algorithmic(st, batch, species, msp, n, L):
+    """Flops the two GAP contractions need (forward k = x . t and backward
+    dE/dx = W T, 2 flops per multiply-add each): per row, the sparse points
+    of its species times the power-spectrum entries it can hold, the
+    upper triangles of the per-l Gram blocks of the species pairs present
+    among its neighbours (n(n+1)/2 per l for a same-species pair, n^2 for
+    two species). The GEMMs skip what no row of a 128-row tile holds, so
+    they issue at least this."""
+    nl = st.neighbour_list()
+    sidx = {int(z): i for i, z in enumerate(species)}
+    lut = np.zeros(int(max(species)) + 1, np.int64)
+    for z, i in sidx.items():
+        lut[z] = i
+    po = nl["pair_offsets"]
+    bits = np.left_shift(1, lut[batch["numbers"][nl["j"]]])
+    mask = np.bitwise_or.reduceat(bits, po[:-1])
+    present = np.array([[(m >> a) & 1 for a in range(len(species))] for m in range(1 << len(species))], bool)
+    L1 = L + 1
+    per_mask = np.zeros(1 << len(species))
+    for m in range(1 << len(species)):
+        k = present[m].sum()
+        per_mask[m] = L1 * (k * n * (n + 1) // 2 + k * (k - 1) // 2 * n * n)
+    centre_species = lut[batch["numbers"][nl["center_atom"]]]
+    m_row = np.asarray(msp)[centre_species]
+    return float(4.0 * np.sum(m_row * per_mask[mask]))
+
+
 TRAINING_METRIC = "GAP training K_NM rows (energy + position gradients) atoms/s on 1 B200, FP64"
 FP64_NOMINAL_TFLOPS = 37.0  # B200 nominal FP64 (CUDA cores), used only if the measurement fails
 
@@ -730,17 +757,15 @@ def run_gap(args):
     counts = np.array([np.sum(batch["numbers"] == s) for s in species])
     msp = np.array([int(np.sum(np.asarray(sp.species) == s)) for s in species])
     S, n, L = len(species), hypers["max_radial"], hypers["max_angular"]
-    # the FP32 path's rows hold the upper triangles of the per-l Gram
-    # matrices (one entry per symmetric pair of same-species entries), in
-    # 2 x 2 tiles grouped into species-pair segments of 32-column multiples:
-    # Dp values, Dg columns with padding
+    # the FP32 path's rows: the upper triangles of the per-l Gram matrices in
+    # 2 x 2 tiles grouped into species-pair segments of 32-column multiples,
+    # Dg columns in all
     Sn = S * n
-    Dp = (L + 1) * Sn * (Sn + 1) // 2
     G, npg = (S, n // 2) if n % 2 == 0 else (1, (Sn + 1) // 2)
     lenD = (4 * (L + 1) * npg * (npg + 1) // 2 + 31) // 32 * 32
     lenO = (4 * (L + 1) * npg * npg + 31) // 32 * 32
     Dg = G * lenD + G * (G - 1) // 2 * lenO
-    gemm_flops = 4.0 * float(np.sum(counts * msp)) * Dp  # forward + backward
+    gemm_flops = gemm_flops_algorithmic(st, batch, species, msp, n, L)  # forward + backward
     gemm_ms = stages[4] + stages[5]
     bf16_peak, hbm_peak, peak_kind = peaks()
     achieved = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else None
