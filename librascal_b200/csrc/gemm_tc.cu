@@ -59,6 +59,10 @@ struct Smem {
   static constexpr int B_BYTES = BN * BK * 2;
   static constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int TOTAL = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+  // the grouped kernel adds the FP32 epilogue's staging: per epilogue warp
+  // two 32 x 32 boxes of 4 KB (128-byte swizzle, 1024-byte aligned)
+  static constexpr int STAGING = 4 * 2 * 4096;
+  static constexpr int TOTAL_GROUPED = TOTAL + STAGING;
 };
 
 __device__ __forceinline__ float powz(float v, int z) {
@@ -290,6 +294,7 @@ struct SegWalk {
 
 struct TcGroupedArgs {
   CUtensorMap a_hi[kMaxGroups], a_lo[kMaxGroups], b_hi[kMaxGroups], b_lo[kMaxGroups];
+  CUtensorMap c_map[kMaxGroups];  // FP32 output (epilogue 0): 32 x 32 boxes, 128-byte swizzle
   TcGroup grp[kMaxGroups];
   int n_groups;
   int epilogue;
@@ -321,7 +326,8 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char * base = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  uint64_t * full = reinterpret_cast<uint64_t *>(base + STAGES * SM::STAGE_BYTES);
+  float * staging = reinterpret_cast<float *>(base + STAGES * SM::STAGE_BYTES);  // [4 warps][2][32][32]
+  uint64_t * full = reinterpret_cast<uint64_t *>(base + STAGES * SM::STAGE_BYTES + SM::STAGING);
   uint64_t * empty = full + STAGES;
   uint64_t * tfull = empty + STAGES;  // [2] accumulator buffer written
   uint64_t * tempty = tfull + 2;      // [2] accumulator buffer read out
@@ -445,6 +451,8 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
     }
   } else {
     const int q = warp & 3;  // TMEM lane quadrant of this warp
+    float * stg = staging + q * 2048;  // this warp's two 32 x 32 boxes
+    int sb = 0;                        // box to fill next
     int i = 0;
     for (int64_t t = blockIdx.x; t < p.n_tiles; t += gridDim.x) {
       const int g = find_group(p, t);
@@ -467,16 +475,23 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(b * BN + c0), v);
         const int64_t col = n0 + c0;
         if (p.epilogue == 0) {
-          if (row >= G.M || col >= G.N) continue;
-          float * out = G.C + row * G.ldc + col;
-          if (col + 32 <= G.N) {
+          // the warp's 32 rows x 32 columns through shared memory to a TMA
+          // store, which clips rows >= M and columns >= N
+          if (col >= G.N) continue;  // uniform over the warp
+          if (lane == 0) bulk_wait_read<1>();  // the store that read this box last is done with it
+          __syncwarp();
+          float * box = stg + sb * 1024;
 #pragma unroll
-            for (int k = 0; k < 32; k += 4)
-              *reinterpret_cast<float4 *>(out + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
-          } else {
-            for (int k = 0; k < 32; ++k)
-              if (col + k < G.N) out[k] = v[k];
+          for (int c = 0; c < 8; ++c)  // 16-byte chunk c of row `lane` at chunk c ^ (lane % 8): 128-byte swizzle
+            *reinterpret_cast<float4 *>(box + lane * 32 + 4 * (c ^ (lane & 7))) =
+                make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+          fence_async_smem();
+          __syncwarp();
+          if (lane == 0) {
+            tma_store_2d(&p.c_map[g], box, int(col), int(m0 + q * 32));
+            bulk_commit();
           }
+          sb ^= 1;
         } else {
           if (col >= G.ldw) continue;  // uniform over the warp: ldw is a multiple of 32
           // lane j holds alpha of column col + j; every lane takes them all by shuffles
@@ -519,6 +534,8 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
       if (lane == 0) mbar_arrive(&tempty[b]);
       ++i;
     }
+    if (lane == 0) bulk_wait<0>();  // every TMA store of this warp has completed
+    __syncwarp();
   }
   tc_fence_before();
   __syncthreads();
@@ -549,6 +566,25 @@ EncodeFn encode_fn() {
 // 2D bf16 tensor map over a row-major [rows x cols] matrix with row stride
 // ld elements; box = box_rows x 64 columns, 128-byte swizzle, zero fill
 // outside the matrix.
+// 2D FP32 tensor map for TMA stores of 32 x 32 boxes into a row-major
+// [rows x cols] matrix with row stride ld elements (128-byte swizzle: the
+// box's 16-byte chunk c of row r sits at chunk c ^ (r % 8) in shared memory).
+CUtensorMap make_store_map_f32(const float * ptr, int64_t rows, int64_t cols, int64_t ld) {
+  if ((reinterpret_cast<uintptr_t>(ptr) & 15) != 0 || (ld * 4) % 16 != 0)
+    throw Error(RGPU_ERR_INVALID_ARGUMENT, "tensor map: base or stride not 16-byte aligned");
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  cuuint64_t dims[2] = {cuuint64_t(cols), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(ld * 4)};
+  cuuint32_t box[2] = {32, 32};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(ptr), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(RGPU_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string(int(r)) + ")");
+  return m;
+}
+
 CUtensorMap make_map(const __nv_bfloat16 * ptr, int64_t rows, int64_t cols, int64_t ld, int box_rows,
                      int box_k = kBK) {
   if ((reinterpret_cast<uintptr_t>(ptr) & 15) != 0 || (ld * 2) % 16 != 0)
@@ -693,6 +729,7 @@ void grouped_launch(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
     p.a_lo[ng] = make_map(g.A_lo, g.M, g.K, g.lda, kBM, BK);
     p.b_hi[ng] = make_map(g.B_hi, g.N, g.K, g.ldb, BN, BK);
     p.b_lo[ng] = make_map(g.B_lo, g.N, g.K, g.ldb, BN, BK);
+    if (g.epilogue == 0) p.c_map[ng] = make_store_map_f32(g.C, g.M, g.N, g.ldc);
     TcGroup & G = p.grp[ng];
     G.M = g.M;
     G.N = g.N;
@@ -733,7 +770,7 @@ void grouped_launch(const Bf16x3Gemm * gs, int n, cudaStream_t st) {
   int dev = 0, sms = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   cuda_check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
-  const size_t smem = Smem<BN, STAGES, BK>::TOTAL;
+  const size_t smem = Smem<BN, STAGES, BK>::TOTAL_GROUPED;
   cuda_check(cudaFuncSetAttribute(gemm_tc_grouped_kernel<BN, STAGES, BK>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
              "cudaFuncSetAttribute(gemm_tc_grouped)");
