@@ -272,10 +272,11 @@ __global__ void chunk_map_kernel(FeatureDims fd, uint32_t * __restrict__ map) {
 // Contraction tasks are (row pair 2ip, 2ip+1; 4-wide column group g of the
 // padded coefficient rows) with g fastest, so the lanes of a half-warp share
 // their rows (one broadcast 16-byte load per tile, uniform trip counts) and
-// read consecutive 16-byte chunks of a coefficient row. The centre's dE/dc
-// rows are staged in shared memory with an odd row stride and stored
-// coalesced. The next centre's coefficients are copied in with cp.async, and
-// its x and dE/dx rows prefetched into L2, while this one is worked on.
+// read consecutive 16-byte chunks of a coefficient row; each task stores its
+// two rows of dE/dc as 8-byte pairs. The chunk map is copied into shared
+// memory once per block. The next centre's coefficients are copied in with
+// cp.async, and its x and dE/dx rows prefetched into L2, while this one is
+// worked on.
 template <int L>
 __global__ void __launch_bounds__(kBwdThreads, 4)
 ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * __restrict__ Xh,
@@ -285,12 +286,12 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
   constexpr int L1 = L + 1, RS = row_stride(L), K = L1 * L1;
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
-  const int Sn = fd.Sn, OS = Sn | 1;
+  const int Sn = fd.Sn;
   const int NP = (Sn + 1) >> 1, NT = NP * (NP + 1) / 2;
   const int tile = Sn * RS, tileP = (Sn + (Sn & 1)) * RS;  // a coefficient tile; its buffer
   float * Cb = smf;                // two coefficient buffers [Sn rounded up to even][RS]
   float * Ts = Cb + 2 * tileP;     // G: L1 triangles of NT tiles
-  float * Os = Ts + 4 * L1 * NT;   // dE/dc of the centre: [K][OS]
+  uint32_t * smap = reinterpret_cast<uint32_t *>(Ts + 4 * L1 * NT);  // the chunk map
   __shared__ float red[32];
   // column groups of the contraction: the 4-wide chunks of the padded
   // coefficient row in order (group g covers columns 4g .. 4g+3, of block
@@ -306,6 +307,7 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
   // the row after an odd S n's last row stays zero in both buffers
   for (int e = tile + threadIdx.x; e < tileP; e += blockDim.x) Cb[e] = Cb[tileP + e] = 0.f;
   const int nq = fd.Dg >> 2;  // 4-column chunks of the row (one tile each)
+  for (int c = threadIdx.x; c < nq; c += blockDim.x) smap[c] = chunk_map[c];
   float4 * T4 = reinterpret_cast<float4 *>(Ts);
   auto prefetch = [&](int64_t c, float * dst) {
     const float4 * src = reinterpret_cast<const float4 *>(C + size_t(c) * tile);
@@ -340,7 +342,7 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
     float dot = 0.f;
 #pragma unroll 4
     for (int c = threadIdx.x; c < nq; c += blockDim.x) {
-      const uint32_t e = __ldg(chunk_map + c);
+      const uint32_t e = smap[c];
       if (e == kNoChunk) continue;
       if (!live(e)) {
         T4[e & 0xFFFFFFu] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -364,7 +366,7 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
       // each thread projects the chunks it stored
 #pragma unroll 4
       for (int c = threadIdx.x; c < nq; c += blockDim.x) {
-        const uint32_t e = __ldg(chunk_map + c);
+        const uint32_t e = smap[c];
         if (!live(e)) continue;
         const int d = int(e & 0xFFFFFFu);
         const uint2 hv = __ldcs(xh + c), lv = __ldcs(xl + c);
@@ -428,18 +430,21 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
         if (m0 + e < M) {
-          float * o = Os + (l * l + m0 + e) * OS + i0;
-          o[0] = v0[e] * sc;
-          if (i0 + 1 < Sn) o[1] = v1[e] * sc;
+          float * o = dC + (size_t(ci) * K + (l * l + m0 + e)) * Sn + i0;
+          if (i0 + 1 < Sn) {
+            if ((Sn & 1) == 0)  // 8-byte aligned pair
+              *reinterpret_cast<float2 *>(o) = make_float2(v0[e] * sc, v1[e] * sc);
+            else {
+              o[0] = v0[e] * sc;
+              o[1] = v1[e] * sc;
+            }
+          } else {
+            o[0] = v0[e] * sc;
+          }
         }
       }
     }
-    __syncthreads();
-    // rows lm of the centre's dE/dc, one warp per row (consecutive lanes:
-    // consecutive (species, radial) entries)
-    float * out = dC + size_t(ci) * Sn * K;
-    for (int lm = threadIdx.x >> 5; lm < K; lm += blockDim.x >> 5)
-      for (int i = threadIdx.x & 31; i < Sn; i += 32) out[lm * Sn + i] = Os[lm * OS + i];
+    __syncthreads();  // the triangles and this coefficient buffer are read no more
   }
   cp_async_wait<0>();
 }
@@ -452,11 +457,12 @@ size_t fwd_smem(const FeatureDims & fd) {
 }
 
 // Shared memory of the backward: two coefficient buffers, the per-l
-// triangles of G and the staged dE/dc rows.
+// triangles of G and the chunk map.
 template <int L>
 size_t bwd_smem(const FeatureDims & fd) {
-  const size_t Sn = size_t(fd.Sn), K = size_t(L + 1) * (L + 1), np = (Sn + 1) / 2;
-  return sizeof(float) * (2 * (Sn + (Sn & 1)) * row_stride(L) + 4 * size_t(L + 1) * np * (np + 1) / 2 + K * (Sn | 1));
+  const size_t Sn = size_t(fd.Sn), np = (Sn + 1) / 2;
+  return sizeof(float) * (2 * (Sn + (Sn & 1)) * row_stride(L) + 4 * size_t(L + 1) * np * (np + 1) / 2) +
+         sizeof(uint32_t) * size_t(fd.Dg / 4);
 }
 
 // Blocks of a persistent kernel: as many as fit on the device at once (at
