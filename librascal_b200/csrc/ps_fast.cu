@@ -271,7 +271,8 @@ __global__ void chunk_map_kernel(FeatureDims fd, uint32_t * __restrict__ map) {
 //
 // Contraction tasks are (row pair 2ip, 2ip+1; 4-wide column group g of the
 // padded coefficient rows) with g fastest, so the lanes of a half-warp share
-// their rows (one broadcast 16-byte load per tile, uniform trip counts) and
+// their rows (one broadcast 16-byte load per tile, uniform trip counts and
+// the same skips of the species the centre lacks) and
 // read consecutive 16-byte chunks of a coefficient row; each task stores its
 // two rows of dE/dc as 8-byte pairs. The chunk map is copied into shared
 // memory once per block. The next centre's coefficients are copied in with
@@ -286,7 +287,7 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
   constexpr int L1 = L + 1, RS = row_stride(L), K = L1 * L1;
   extern __shared__ __align__(16) float smf[];
   const FeatureDims fd = a.fd;
-  const int Sn = fd.Sn;
+  const int Sn = fd.Sn, npg = fd.npg;
   const int NP = (Sn + 1) >> 1, NT = NP * (NP + 1) / 2;
   const int tile = Sn * RS, tileP = (Sn + (Sn & 1)) * RS;  // a coefficient tile; its buffer
   float * Cb = smf;                // two coefficient buffers [Sn rounded up to even][RS]
@@ -387,6 +388,10 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
     // diagonal tile, then (ip, j) for j > ip
     for (int t = threadIdx.x; t < kG * NP; t += blockDim.x) {
       const int ip = t / kG, g = t - ip * kG;
+      // rows of a species the centre has no neighbour of: their dE/dc is
+      // never read (no pair of that species), so the task is skipped
+      const int B = ip / npg;
+      if (!((pm >> B) & 1u)) continue;
       const int l = grp_l[g];
       const float4 * Tl = T4 + l * NT;
       const int i0 = 2 * ip;
@@ -405,24 +410,36 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
         a1.z += h10 * c0.z + h11 * c1.z;
         a1.w += h10 * c0.w + h11 * c1.w;
       };
+      const float * cb = Cp + 4 * g;
+      // j < ip: tiles (j, ip), transposed, one run per group A <= B; groups the
+      // centre lacks hold zero tiles and zero coefficients and are skipped
       const float4 * tp = Tl + ip * (ip + 1) / 2;  // tile (0, ip)
-      const float * cj = Cp + 4 * g;
+      for (int A = 0; A <= B; ++A) {
+        const int j0 = A * npg, j1 = min(j0 + npg, ip);
+        if (j1 <= j0 || !((pm >> A) & 1u)) continue;
+        const float * cj = cb + 2 * j0 * RS;
 #pragma unroll 2
-      for (int j = 0; j < ip; ++j, cj += 2 * RS) {
-        const float4 v = tp[j];  // (2j, i0), (2j+1, i0), (2j, i0+1), (2j+1, i0+1)
-        acc(v.x, v.z, v.y, v.w, cj);
+        for (int j = j0; j < j1; ++j, cj += 2 * RS) {
+          const float4 v = tp[j];  // (2j, i0), (2j+1, i0), (2j, i0+1), (2j+1, i0+1)
+          acc(v.x, v.z, v.y, v.w, cj);
+        }
       }
       {
         const float4 v = tp[ip];  // (i0, i0), zero, (i0, i0+1), (i0+1, i0+1)
-        acc(kSqrt2f * v.x, v.z, v.z, kSqrt2f * v.w, cj);
-        cj += 2 * RS;
+        acc(kSqrt2f * v.x, v.z, v.z, kSqrt2f * v.w, cb + i0 * RS);
       }
-      const float4 * tq = Tl + (ip + 1) * (ip + 2) / 2 + ip;  // tile (ip, ip + 1)
+      // j > ip: tiles (ip, j), one run per group A >= B
+      for (int A = B; A < fd.G; ++A) {
+        const int j0 = max(A * npg, ip + 1), j1 = min((A + 1) * npg, NP);
+        if (j1 <= j0 || !((pm >> A) & 1u)) continue;
+        const float4 * tq = Tl + j0 * (j0 + 1) / 2 + ip;  // tile (ip, j0)
+        const float * cj = cb + 2 * j0 * RS;
 #pragma unroll 2
-      for (int j = ip + 1; j < NP; ++j, cj += 2 * RS) {
-        const float4 v = *tq;  // (i0, 2j), (i0+1, 2j), (i0, 2j+1), (i0+1, 2j+1)
-        acc(v.x, v.y, v.z, v.w, cj);
-        tq += j + 1;
+        for (int j = j0; j < j1; ++j, cj += 2 * RS) {
+          const float4 v = *tq;  // (i0, 2j), (i0+1, 2j), (i0, 2j+1), (i0+1, 2j+1)
+          acc(v.x, v.y, v.z, v.w, cj);
+          tq += j + 1;
+        }
       }
       const int M = 2 * l + 1, m0 = 4 * g - offp_rt(l);
       const float sc = rsqrtf(float(M)) * kSqrt2f;
