@@ -12,7 +12,8 @@ import pytest
 
 import librascal_b200 as rb
 from librascal_b200 import synthetic, tune
-from test_gpu_parity import gap_setup, soap
+from oracle import oracle as O
+from test_gpu_parity import gap_setup, oracle_calc, soap
 
 pytestmark = pytest.mark.gpu
 
@@ -78,3 +79,23 @@ def test_tensor_core_power_spectrum_forward(which):
         batch, kw = synthetic.bulk_box(n_atoms=301, seed=63), dict(rc=6.0, n=12, l=9, sigma=0.5)
     model, E_ref, F_ref, shape = _case(batch, kw, 20)
     _check(model, batch, E_ref, F_ref, shape, dict(tune.DEFAULT, psf_tc=1))
+
+
+@pytest.mark.parametrize("species,n,l", [((1, 6, 8), 5, 3), ((1, 8), 7, 4), ((1, 6, 7, 8), 3, 5)])
+def test_odd_radial_single_group(species, n, l):
+    """Odd max_radial: every (species, n) channel shares one group of
+    ceil(S n / 2) channel pairs, whose last pair is half padding when S n is
+    odd (S n = 15, 14, 12 here). Features exported into the
+    reference's column order and GAP energies and forces against the FP64
+    oracle."""
+    batch = synthetic.triclinic_cells(n_struct=3, n_min=30, n_max=44, species=species, seed=71)
+    kw = dict(rc=5.0, n=n, l=l, sigma=0.4)
+    calc = soap(**kw)
+    al = calc.transform(rb.AtomsList(rb.StructureSet(batch)), precision="fp32")
+    sp = np.unique(batch["numbers"])
+    X = al.get_features(calc, keys=calc.get_keys(sp))
+    Xo = O.Run(oracle_calc(**kw), batch, sp).power_spectrum()
+    assert X.shape == Xo.shape
+    assert np.abs(X - Xo).max() <= 1e-5 * np.abs(Xo).max()
+    model, E_ref, F_ref, shape = _case(batch, kw, 20)
+    _check(model, batch, E_ref, F_ref, shape, dict(tune.DEFAULT))
