@@ -129,8 +129,10 @@ pair_adjoint_kernel(ExpansionArgs a, const int32_t * __restrict__ pair_center, i
               for (int qq = 0; qq < NV / 4; ++qq) {
                 if (4 * qq < n) {
                   const float4 ev = __ldg(E4 + qq);
-                  A += ev.x * pl[4 * qq] + ev.y * pl[4 * qq + 1] + ev.z * pl[4 * qq + 2] + ev.w * pl[4 * qq + 3];
-                  B += ev.x * rl[4 * qq] + ev.y * rl[4 * qq + 1] + ev.z * rl[4 * qq + 2] + ev.w * rl[4 * qq + 3];
+                  A = fmaf(ev.w, pl[4 * qq + 3],
+                           fmaf(ev.z, pl[4 * qq + 2], fmaf(ev.y, pl[4 * qq + 1], fmaf(ev.x, pl[4 * qq], A))));
+                  B = fmaf(ev.w, rl[4 * qq + 3],
+                           fmaf(ev.z, rl[4 * qq + 2], fmaf(ev.y, rl[4 * qq + 1], fmaf(ev.x, rl[4 * qq], B))));
                 }
               }
             } else {

@@ -80,10 +80,11 @@ __device__ __forceinline__ float fwd_tile(const float * Cp, int Sn, int i, int j
 #pragma unroll
   for (int q = 0; q < Q; ++q) {
     const float4 x0 = a0[q], x1 = a1[q], y0 = b0[q], y1 = b1[q];
-    u00 += x0.x * y0.x + x0.y * y0.y + x0.z * y0.z + x0.w * y0.w;
-    u10 += x1.x * y0.x + x1.y * y0.y + x1.z * y0.z + x1.w * y0.w;
-    u01 += x0.x * y1.x + x0.y * y1.y + x0.z * y1.z + x0.w * y1.w;
-    u11 += x1.x * y1.x + x1.y * y1.y + x1.z * y1.z + x1.w * y1.w;
+    // chained FMAs into the accumulators (one FFMA per product)
+    u00 = fmaf(x0.x, y0.x, fmaf(x0.y, y0.y, fmaf(x0.z, y0.z, fmaf(x0.w, y0.w, u00))));
+    u10 = fmaf(x1.x, y0.x, fmaf(x1.y, y0.y, fmaf(x1.z, y0.z, fmaf(x1.w, y0.w, u10))));
+    u01 = fmaf(x0.x, y1.x, fmaf(x0.y, y1.y, fmaf(x0.z, y1.z, fmaf(x0.w, y1.w, u01))));
+    u11 = fmaf(x1.x, y1.x, fmaf(x1.y, y1.y, fmaf(x1.z, y1.z, fmaf(x1.w, y1.w, u11))));
   }
   // v_rc: row I0 + r, column J0 + c
   float v00 = sw ? u10 : u00, v10 = sw ? u00 : u10, v01 = sw ? u11 : u01, v11 = sw ? u01 : u11;
@@ -401,14 +402,14 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
       auto acc = [&](float h00, float h10, float h01, float h11, const float * cj) {
         const float4 c0 = *reinterpret_cast<const float4 *>(cj);
         const float4 c1 = *reinterpret_cast<const float4 *>(cj + RS);
-        a0.x += h00 * c0.x + h01 * c1.x;
-        a0.y += h00 * c0.y + h01 * c1.y;
-        a0.z += h00 * c0.z + h01 * c1.z;
-        a0.w += h00 * c0.w + h01 * c1.w;
-        a1.x += h10 * c0.x + h11 * c1.x;
-        a1.y += h10 * c0.y + h11 * c1.y;
-        a1.z += h10 * c0.z + h11 * c1.z;
-        a1.w += h10 * c0.w + h11 * c1.w;
+        a0.x = fmaf(h01, c1.x, fmaf(h00, c0.x, a0.x));
+        a0.y = fmaf(h01, c1.y, fmaf(h00, c0.y, a0.y));
+        a0.z = fmaf(h01, c1.z, fmaf(h00, c0.z, a0.z));
+        a0.w = fmaf(h01, c1.w, fmaf(h00, c0.w, a0.w));
+        a1.x = fmaf(h11, c1.x, fmaf(h10, c0.x, a1.x));
+        a1.y = fmaf(h11, c1.y, fmaf(h10, c0.y, a1.y));
+        a1.z = fmaf(h11, c1.z, fmaf(h10, c0.z, a1.z));
+        a1.w = fmaf(h11, c1.w, fmaf(h10, c0.w, a1.w));
       };
       const float * cb = Cp + 4 * g;
       // j < ip: tiles (j, ip), transposed, one run per group A <= B; groups the
