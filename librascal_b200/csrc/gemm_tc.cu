@@ -305,13 +305,35 @@ struct TcGroupedArgs {
   SegGeom seg;
 };
 
-// Whether N-mode skipping drops tile (mt, nt) of group G (every role asks).
+// The 32-column units of tile (mt, nt) that are computed: [u0, u0 + nu).
+// The tile's BN / 32 units are cut after the last one holding a column the
+// epilogue writes (< N; < ldw for the GAP forward, whose W rows are zero up
+// to ldw), and under N-mode skipping to the run from its first to its last
+// needed unit; nu = 0 drops the tile. The MMA then runs N = 32 nu wide on
+// B rows loaded from the span's first column. Every role asks, so all agree.
+struct TileSpan {
+  int u0, nu;
+};
 template <int BN>
-__device__ __forceinline__ bool skip_tile(const TcGroupedArgs & p, const TcGroup & G, int64_t mt, int64_t nt) {
-  if (p.seg.mode != 2 || !G.tile_mask) return false;
-  SegWalk w;
-  w.start(p.seg, G.tile_mask[mt]);
-  return !w.any(int(nt * (BN / 32)), BN / 32);
+__device__ __forceinline__ TileSpan tile_span(const TcGroupedArgs & p, const TcGroup & G, int64_t mt, int64_t nt) {
+  const int64_t ext = (p.epilogue == 1 && G.ldw > G.N) ? G.ldw : G.N;
+  const int64_t ue = (ext + 31) / 32;
+  int u0 = int(nt) * (BN / 32);
+  int u1 = int(ue < u0 + BN / 32 ? ue : int64_t(u0 + BN / 32));
+  if (p.seg.mode == 2 && G.tile_mask) {
+    SegWalk w;
+    w.start(p.seg, G.tile_mask[mt]);
+    int first = u1, last = u0 - 1;
+    for (int u = u0; u < u1; ++u)
+      if (w.need(u)) {
+        first = min(first, u);
+        last = u;
+      }
+    if (last < first) return {u0, 0};
+    u0 = first;
+    u1 = last + 1;
+  }
+  return {u0, u1 - u0};
 }
 
 __device__ __forceinline__ int find_group(const TcGroupedArgs & p, int64_t t) {
@@ -366,8 +388,9 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         const int g = find_group(p, t);
         const TcGroup & G = p.grp[g];
         const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
-        if (skip_tile<BN>(p, G, mt, nt)) continue;
-        const int m0 = int(mt * kBM), n0 = int(nt * BN);
+        const TileSpan sp = tile_span<BN>(p, G, mt, nt);
+        if (sp.nu == 0) continue;
+        const int m0 = int(mt * kBM), n0 = 32 * sp.u0;
         const int nk = int((G.K + BK - 1) / BK);
         const bool kskip = p.seg.mode == 1 && G.tile_mask;
         SegWalk w;
@@ -385,6 +408,8 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
           const int kx = kb * BK;
           tma_load_2d(st, &p.a_hi[g], &full[s], kx, m0);
           tma_load_2d(st + SM::A_BYTES, &p.a_lo[g], &full[s], kx, m0);
+          // B as one box of BN rows from the span's first column (rows past
+          // the span or past N are loaded or zero-filled but not multiplied)
           tma_load_2d(st + 2 * SM::A_BYTES, &p.b_hi[g], &full[s], kx, n0);
           tma_load_2d(st + 2 * SM::A_BYTES + SM::B_BYTES, &p.b_lo[g], &full[s], kx, n0);
           ++it;
@@ -397,7 +422,6 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      constexpr uint32_t idesc = make_idesc(kBM, BN);
       uint32_t it = 0;
       int i = 0;
       bool ok = true;
@@ -405,7 +429,9 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
         const int g = find_group(p, t);
         const TcGroup & G = p.grp[g];
         const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
-        if (skip_tile<BN>(p, G, mt, nt)) continue;
+        const TileSpan sp = tile_span<BN>(p, G, mt, nt);
+        if (sp.nu == 0) continue;
+        const uint32_t idesc = make_idesc(kBM, 32 * sp.nu);
         const int nk = int((G.K + BK - 1) / BK);
         const int b = i & 1;
         const uint32_t use = uint32_t(i >> 1);
@@ -458,8 +484,9 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
       const int g = find_group(p, t);
       const TcGroup & G = p.grp[g];
       const int64_t local = t - G.tile0, mt = local / G.n_tiles, nt = local - mt * G.n_tiles;
-      if (skip_tile<BN>(p, G, mt, nt)) continue;
-      const int64_t m0 = mt * kBM, n0 = nt * BN;
+      const TileSpan sp = tile_span<BN>(p, G, mt, nt);
+      if (sp.nu == 0) continue;
+      const int64_t m0 = mt * kBM, n0 = 32 * int64_t(sp.u0);
       const int b = i & 1;
       const uint32_t use = uint32_t(i >> 1);
       const bool ok = __all_sync(0xffffffffu, mbar_wait(&tfull[b], use & 1u, status, 3));
@@ -470,7 +497,7 @@ __global__ void __launch_bounds__(kThreads, 1) gemm_tc_grouped_kernel(const __gr
       float e_acc = 0.f;
       const float zf = float(p.zeta);
       const int zm1 = p.zeta - 1;
-      for (int c0 = 0; c0 < BN; c0 += 32) {
+      for (int c0 = 0; c0 < 32 * sp.nu; c0 += 32) {
         float v[32];
         tmem_ld32(tmem + (uint32_t(q * 32) << 16) + uint32_t(b * BN + c0), v);
         const int64_t col = n0 + c0;
