@@ -542,6 +542,7 @@ void compute_features(rgpu_calculator * c, rgpu_structures * s, int precision, b
       s->Xh.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dg + 64);
       s->Xl.ensure(sizeof(uint16_t) * size_t(nc) * fd.Dg + 64);
       s->xscale32.ensure(sizeof(float) * (nc + 1));
+      pa.present = s->present.as<uint32_t>();
       launch_ps_fwd_fast(pa, s->C32.as<float>(), need_x32 ? s->X32.as<float>() : nullptr,
                          s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(), s->xscale32.as<float>(), s->st);
     }
@@ -1570,6 +1571,7 @@ static void graph_enqueue(rgpu_gap_model * m, rgpu_structures * s, bool stress, 
   pa.row_of_center = s->row_of_center.as<int32_t>();
   launch_expansion_fp32(ea, s->C32.as<float>(), s->present.as<uint32_t>(), st);
   sort_rows_by_mask(s);
+  pa.present = s->present.as<uint32_t>();
   launch_ps_fwd_fast(pa, s->C32.as<float>(), nullptr, s->Xh.as<__nv_bfloat16>(), s->Xl.as<__nv_bfloat16>(),
                      s->xscale32.as<float>(), st);
   RGPU_CUDA(cudaMemsetAsync(s->E_d.p, 0, sizeof(double) * s->n_struct, st));

@@ -56,88 +56,84 @@ __device__ __forceinline__ void prefetch_l2(const void * p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// One 2 x 2 tile (i, j), i <= j, of the packed l-block: G_l over rows
-// 2i, 2i+1 and columns 2j, 2j+1, scaled by lf (sqrt2 lf off the diagonal),
-// the entry below the diagonal of a diagonal tile and rows or columns beyond
-// S n zero, stored as 4 consecutive columns (8 bytes of BF16 hi, 8 of lo,
-// 16 of FP32 when X is given). Returns the tile's sum of squares.
-template <int L, int l>
-__device__ __forceinline__ float fwd_tile(const float * Cp, int Sn, int i, int j, float * __restrict__ X,
-                                          __nv_bfloat16 * __restrict__ hr, __nv_bfloat16 * __restrict__ lr) {
-  constexpr int RS = row_stride(L), Q = pad4(2 * l + 1) / 4, O = offp(l);
-  const float lf = rsqrtf(float(2 * l + 1)), lf2 = lf * kSqrt2f;
-  const int I0 = 2 * i, J0 = 2 * j;
-  const bool i1 = I0 + 1 < Sn, j1 = J0 + 1 < Sn;
-  // Lanes with consecutive i read rows 2i apart; taking row 2i + 1 first when
-  // bit 2 of i is set spreads the 8 lanes of a 16-byte load phase over 8
-  // different bank groups (the row stride is an odd number of 16-byte units).
-  const int sw = (i >> 2) & 1 & int(i1);
-  const float4 * a0 = reinterpret_cast<const float4 *>(Cp + (I0 + sw) * RS + O);
-  const float4 * a1 = reinterpret_cast<const float4 *>(Cp + (i1 ? I0 + 1 - sw : I0) * RS + O);
-  const float4 * b0 = reinterpret_cast<const float4 *>(Cp + J0 * RS + O);
-  const float4 * b1 = reinterpret_cast<const float4 *>(Cp + (j1 ? J0 + 1 : J0) * RS + O);
-  float u00 = 0.f, u10 = 0.f, u01 = 0.f, u11 = 0.f;  // u_rc: row a_r, column J0 + c
-#pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    const float4 x0 = a0[q], x1 = a1[q], y0 = b0[q], y1 = b1[q];
-    // chained FMAs into the accumulators (one FFMA per product)
-    u00 = fmaf(x0.x, y0.x, fmaf(x0.y, y0.y, fmaf(x0.z, y0.z, fmaf(x0.w, y0.w, u00))));
-    u10 = fmaf(x1.x, y0.x, fmaf(x1.y, y0.y, fmaf(x1.z, y0.z, fmaf(x1.w, y0.w, u10))));
-    u01 = fmaf(x0.x, y1.x, fmaf(x0.y, y1.y, fmaf(x0.z, y1.z, fmaf(x0.w, y1.w, u01))));
-    u11 = fmaf(x1.x, y1.x, fmaf(x1.y, y1.y, fmaf(x1.z, y1.z, fmaf(x1.w, y1.w, u11))));
-  }
-  // v_rc: row I0 + r, column J0 + c
-  float v00 = sw ? u10 : u00, v10 = sw ? u00 : u10, v01 = sw ? u11 : u01, v11 = sw ? u01 : u11;
-  const bool diag = i == j;
-  v00 *= diag ? lf : lf2;
-  v10 = (diag || !i1) ? 0.f : v10 * lf2;
-  v01 = j1 ? v01 * lf2 : 0.f;
-  v11 = (i1 && j1) ? v11 * (diag ? lf : lf2) : 0.f;
-  const __nv_bfloat162 h0 = __floats2bfloat162_rn(v00, v10), h1 = __floats2bfloat162_rn(v01, v11);
-  const float2 f0 = __bfloat1622float2(h0), f1 = __bfloat1622float2(h1);
-  const __nv_bfloat162 l0 = __floats2bfloat162_rn(v00 - f0.x, v10 - f0.y);
-  const __nv_bfloat162 l1 = __floats2bfloat162_rn(v01 - f1.x, v11 - f1.y);
-  uint2 hw, lw;
-  hw.x = *reinterpret_cast<const uint32_t *>(&h0);
-  hw.y = *reinterpret_cast<const uint32_t *>(&h1);
-  lw.x = *reinterpret_cast<const uint32_t *>(&l0);
-  lw.y = *reinterpret_cast<const uint32_t *>(&l1);
-  *reinterpret_cast<uint2 *>(hr) = hw;
-  *reinterpret_cast<uint2 *>(lr) = lw;
-  if (X) *reinterpret_cast<float4 *>(X) = make_float4(v00, v10, v01, v11);
-  return v00 * v00 + v10 * v10 + v01 * v01 + v11 * v11;
-}
+// One task of the forward: tile (i, j), i <= j, of every l-block, i.e. G_l
+// over rows 2i, 2i+1 and columns 2j, 2j+1. Row pointers are at column 0 of
+// the centre's coefficients; a1 / b1 repeat a0 / b0 when row 2i+1 / 2j+1 is
+// beyond S n. Lanes with consecutive i read rows 2i apart; taking row 2i + 1
+// first (sw) when bit 2 of i is set spreads the 8 lanes of a 16-byte load
+// phase over 8 different bank groups (the row stride is an odd number of
+// 16-byte units). A tile of a species pair the centre has no neighbour of
+// (live false) holds zeros and reads no coefficients.
+struct FwdTask {
+  const float * a0;
+  const float * a1;
+  const float * b0;
+  const float * b1;
+  int base, T;  // column of the tile at l = L; tiles per l of its segment
+  bool sw, diag, i1, j1, live;
+};
 
-// Every tile of l-block l of the row (task r: row pair i, column pair j and
-// T, the tiles per l of its segment, in tab[r].x = i | j << 8 | T << 16; its
-// first column at l = L in tab[r].y), then the blocks above l; returns their
-// sum of squares.
+// Tile k of l-blocks l .. L: scaled by lf (sqrt2 lf off the diagonal), the
+// entry below the diagonal of a diagonal tile and rows or columns beyond
+// S n zero, stored as 4 consecutive columns at base + 4 (L - l) T (8 bytes
+// of BF16 hi, 8 of lo, 16 of FP32 when X is given). Returns the sum of
+// squares.
 template <int L, int l>
-__device__ __forceinline__ float fwd_blocks(const float * Cp, int Sn, int nt, const int2 * tab, float * X,
-                                            __nv_bfloat16 * hr, __nv_bfloat16 * lr) {
+__device__ __forceinline__ float fwd_task(const FwdTask & k, float * __restrict__ X, __nv_bfloat16 * __restrict__ hr,
+                                          __nv_bfloat16 * __restrict__ lr) {
   if constexpr (l > L) {
     return 0.f;
   } else {
-    float ss = 0.f;
-    for (int r = threadIdx.x; r < nt; r += blockDim.x) {
-      const int2 e = tab[r];
-      const uint32_t ij = uint32_t(e.x);
-      const int o = e.y + 4 * (L - l) * int(ij >> 16);
-      ss += fwd_tile<L, l>(Cp, Sn, int(ij & 0xFFu), int((ij >> 8) & 0xFFu), X ? X + o : nullptr, hr + o, lr + o);
+    constexpr int Q = pad4(2 * l + 1) / 4, O = offp(l);
+    const float lf = rsqrtf(float(2 * l + 1)), lf2 = lf * kSqrt2f;
+    float u00 = 0.f, u10 = 0.f, u01 = 0.f, u11 = 0.f;  // u_rc: row a_r, column J0 + c
+    if (k.live) {
+#pragma unroll
+      for (int q = 0; q < Q; ++q) {
+        const float4 x0 = *reinterpret_cast<const float4 *>(k.a0 + O + 4 * q);
+        const float4 x1 = *reinterpret_cast<const float4 *>(k.a1 + O + 4 * q);
+        const float4 y0 = *reinterpret_cast<const float4 *>(k.b0 + O + 4 * q);
+        const float4 y1 = *reinterpret_cast<const float4 *>(k.b1 + O + 4 * q);
+        // chained FMAs into the accumulators (one FFMA per product)
+        u00 = fmaf(x0.x, y0.x, fmaf(x0.y, y0.y, fmaf(x0.z, y0.z, fmaf(x0.w, y0.w, u00))));
+        u10 = fmaf(x1.x, y0.x, fmaf(x1.y, y0.y, fmaf(x1.z, y0.z, fmaf(x1.w, y0.w, u10))));
+        u01 = fmaf(x0.x, y1.x, fmaf(x0.y, y1.y, fmaf(x0.z, y1.z, fmaf(x0.w, y1.w, u01))));
+        u11 = fmaf(x1.x, y1.x, fmaf(x1.y, y1.y, fmaf(x1.z, y1.z, fmaf(x1.w, y1.w, u11))));
+      }
     }
-    return ss + fwd_blocks<L, l + 1>(Cp, Sn, nt, tab, X, hr, lr);
+    // v_rc: row I0 + r, column J0 + c
+    float v00 = k.sw ? u10 : u00, v10 = k.sw ? u00 : u10, v01 = k.sw ? u11 : u01, v11 = k.sw ? u01 : u11;
+    v00 *= k.diag ? lf : lf2;
+    v10 = (k.diag || !k.i1) ? 0.f : v10 * lf2;
+    v01 = k.j1 ? v01 * lf2 : 0.f;
+    v11 = (k.i1 && k.j1) ? v11 * (k.diag ? lf : lf2) : 0.f;
+    const __nv_bfloat162 h0 = __floats2bfloat162_rn(v00, v10), h1 = __floats2bfloat162_rn(v01, v11);
+    const float2 f0 = __bfloat1622float2(h0), f1 = __bfloat1622float2(h1);
+    const __nv_bfloat162 l0 = __floats2bfloat162_rn(v00 - f0.x, v10 - f0.y);
+    const __nv_bfloat162 l1 = __floats2bfloat162_rn(v01 - f1.x, v11 - f1.y);
+    uint2 hw, lw;
+    hw.x = *reinterpret_cast<const uint32_t *>(&h0);
+    hw.y = *reinterpret_cast<const uint32_t *>(&h1);
+    lw.x = *reinterpret_cast<const uint32_t *>(&l0);
+    lw.y = *reinterpret_cast<const uint32_t *>(&l1);
+    const int o = k.base + 4 * (L - l) * k.T;
+    *reinterpret_cast<uint2 *>(hr + o) = hw;
+    *reinterpret_cast<uint2 *>(lr + o) = lw;
+    if (X) *reinterpret_cast<float4 *>(X + o) = make_float4(v00, v10, v01, v11);
+    const float ss = v00 * v00 + v10 * v10 + v01 * v01 + v11 * v11;
+    return ss + fwd_task<L, l + 1>(k, X, hr, lr);
   }
 }
 
 // p of a centre's row in the packed layout as a BF16 hi/lo split (and in
-// FP32 when X is given), one 2 x 2 tile per task straight to HBM, the
-// segments' padding set to zero, and the row's scale 1/|p| (1 without
-// normalisation); the packed values keep |p|. The block walks the l-blocks
-// in turn (l a compile-time constant in each loop); consecutive lanes take
+// FP32 when X is given), one 2 x 2 tile of every l-block per task straight
+// to HBM, the segments' padding set to zero, and the row's scale 1/|p| (1
+// without normalisation); the packed values keep |p|. Consecutive lanes take
 // consecutive tiles (mostly of one column pair, whose coefficient rows they
-// then read as broadcasts). Persistent: each block loops over centres,
-// prefetching the next centre's coefficient tile with cp.async while it
-// works on the current one.
+// then read as broadcasts); tiles of species pairs the centre lacks are
+// written as zeros. Persistent: each block loops over centres, prefetching
+// the next centre's coefficient tile with cp.async while it works on the
+// current one.
 template <int L>
 __global__ void __launch_bounds__(kThreads)
 ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X,
@@ -158,7 +154,8 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
     const int i = t - j * (j + 1) / 2;
     int base, lstep;
     tile_column(fd, i, j, base, lstep);
-    tab[t] = make_int2(int(uint32_t(i) | (uint32_t(j) << 8) | (uint32_t(lstep / 4) << 16)), base);
+    const uint32_t A = uint32_t(i / fd.npg), B = uint32_t(j / fd.npg);  // species groups
+    tab[t] = make_int2(int(uint32_t(i) | (uint32_t(j) << 8) | (A << 16) | (B << 21)), base);
   }
   // zero columns: the end of every segment after its tiles
   const int padD = fd.lenD - 4 * L1 * fd.TD, padO = fd.lenO - 4 * L1 * fd.TO;
@@ -182,7 +179,27 @@ ps_fwd_f32_kernel(PsArgs a, const float * __restrict__ C, float * __restrict__ X
     float * Xr = X ? X + roff : nullptr;
     __nv_bfloat16 * hr = Xh + roff;
     __nv_bfloat16 * lr = Xl + roff;
-    float ss = fwd_blocks<L, 0>(Cp, Sn, nt, tab, Xr, hr, lr);
+    const uint32_t pm = (fd.G > 1 && a.present) ? a.present[ci] : 0xFFFFFFFFu;
+    float ss = 0.f;
+    for (int r = threadIdx.x; r < nt; r += blockDim.x) {
+      const int2 e = tab[r];
+      const uint32_t x = uint32_t(e.x);
+      const int i = int(x & 0xFFu), j = int((x >> 8) & 0xFFu), A = int((x >> 16) & 31u), B = int((x >> 21) & 31u);
+      FwdTask k;
+      const int I0 = 2 * i, J0 = 2 * j;
+      k.i1 = I0 + 1 < Sn;
+      k.j1 = J0 + 1 < Sn;
+      k.sw = ((i >> 2) & 1) && k.i1;
+      k.a0 = Cp + (I0 + int(k.sw)) * RS;
+      k.a1 = Cp + (k.i1 ? I0 + 1 - int(k.sw) : I0) * RS;
+      k.b0 = Cp + J0 * RS;
+      k.b1 = Cp + (k.j1 ? J0 + 1 : J0) * RS;
+      k.diag = i == j;
+      k.live = ((pm >> A) & (pm >> B) & 1u) != 0u;
+      k.base = e.y;
+      k.T = A == B ? fd.TD : fd.TO;
+      ss += fwd_task<L, 0>(k, Xr, hr, lr);
+    }
     for (int e = threadIdx.x; e < npad; e += blockDim.x) {
       int d;
       if (e < nD) {

@@ -305,6 +305,9 @@ struct PsArgs {
   int64_t n_centers;
   bool normalize;
   const int32_t * row_of_center;  // output row for each centre (species-sorted)
+  // FP32 forward: the centres' species masks (the FP32 expansion's); tiles of
+  // pairs a centre lacks are written as zeros. Null: every pair computed.
+  const uint32_t * present = nullptr;
 };
 // X rows (normalised) and inverse norms.
 void launch_ps_fwd_fp64(const PsArgs & a, const double * C, double * X, double * inv_norm,
