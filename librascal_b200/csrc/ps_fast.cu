@@ -274,10 +274,10 @@ __global__ void chunk_map_kernel(FeatureDims fd, uint32_t * __restrict__ map) {
 }
 
 // Per centre: the projected gradient G = (g - x (x.g)) / |p| of the packed
-// row (x as BF16 hi + lo, g = dE/dx) is formed in shared memory in two
-// passes (the first stores g and reduces x.g, the second, an L2 re-read of
-// x, projects in place), each 16-byte chunk (one 2 x 2 tile) going to its
-// slot of the per-l triangles (chunk_map). A chunk of a species pair the
+// row (x as BF16 hi + lo, g = dE/dx) is formed in shared memory: g arrives
+// by cp.async, each 16-byte chunk (one 2 x 2 tile) at its slot of the per-l
+// triangles (chunk_map), then two passes over x (L2 reads) reduce x.g and
+// project in place. A chunk of a species pair the
 // centre has no neighbour of is neither read nor trusted (x is zero there,
 // and the GAP backward leaves such columns unwritten when no row of the GEMM
 // tile holds the pair): its slot is set to zero. Then dE/dc = lf_l H_l c_l with the
@@ -310,7 +310,8 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
   const int tile = Sn * RS, tileP = (Sn + (Sn & 1)) * RS;  // a coefficient tile; its buffer
   float * Cb = smf;                // two coefficient buffers [Sn rounded up to even][RS]
   float * Ts = Cb + 2 * tileP;     // G: L1 triangles of NT tiles
-  uint32_t * smap = reinterpret_cast<uint32_t *>(Ts + 4 * L1 * NT);  // the chunk map
+  const int zslot = L1 * NT;       // a zero tile after the triangles
+  uint32_t * smap = reinterpret_cast<uint32_t *>(Ts + 4 * (zslot + 1));  // the chunk map
   __shared__ float red[32];
   // column groups of the contraction: the 4-wide chunks of the padded
   // coefficient row in order (group g covers columns 4g .. 4g+3, of block
@@ -328,6 +329,7 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
   const int nq = fd.Dg >> 2;  // 4-column chunks of the row (one tile each)
   for (int c = threadIdx.x; c < nq; c += blockDim.x) smap[c] = chunk_map[c];
   float4 * T4 = reinterpret_cast<float4 *>(Ts);
+  if (threadIdx.x == 0) T4[zslot] = make_float4(0.f, 0.f, 0.f, 0.f);
   auto prefetch = [&](int64_t c, float * dst) {
     const float4 * src = reinterpret_cast<const float4 *>(C + size_t(c) * tile);
     for (int e = threadIdx.x; e < tile / 4; e += blockDim.x) cp_async16(dst + 4 * e, src + e);
@@ -337,6 +339,27 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
   cp_async_commit();
   // persistent: the tables above serve every centre of this block
   for (int buf = 0; ci < a.n_centers; ci += gridDim.x, buf ^= 1) {
+    const float * Cp = Cb + buf * tileP;
+    const int64_t row = a.row_of_center[ci];
+    const uint2 * xh = reinterpret_cast<const uint2 *>(Xh + size_t(row) * fd.Dg);
+    const uint2 * xl = reinterpret_cast<const uint2 *>(Xl + size_t(row) * fd.Dg);
+    const float4 * g4 = reinterpret_cast<const float4 *>(dX + size_t(row) * fd.Dg);
+    const float rs = row_scale[row];  // x = rs * p; G = rs * (g - x (x.g))
+    const uint32_t pm = fd.G > 1 ? present[ci] : 0xFFFFFFFFu;  // species with neighbours (the groups)
+    auto live = [&](uint32_t e) {
+      return e != kNoChunk && ((pm >> ((e >> 24) & 15u)) & 1u) && ((pm >> (e >> 28)) & 1u);
+    };
+    // g into its slots by asynchronous copies (all in flight at once); the
+    // slots of absent pairs are zeroed
+    for (int c = threadIdx.x; c < nq; c += blockDim.x) {
+      const uint32_t e = smap[c];
+      if (e == kNoChunk) continue;
+      if (live(e))
+        cp_async16(T4 + (e & 0xFFFFFFu), g4 + c);
+      else
+        T4[e & 0xFFFFFFu] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    cp_async_commit();
     const int64_t next = ci + gridDim.x;
     if (next < a.n_centers) {
       prefetch(next, Cb + (buf ^ 1) * tileP);
@@ -348,47 +371,34 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
       }
     }
     cp_async_commit();
-    const float * Cp = Cb + buf * tileP;
-    const int64_t row = a.row_of_center[ci];
-    const uint2 * xh = reinterpret_cast<const uint2 *>(Xh + size_t(row) * fd.Dg);
-    const uint2 * xl = reinterpret_cast<const uint2 *>(Xl + size_t(row) * fd.Dg);
-    const float4 * g4 = reinterpret_cast<const float4 *>(dX + size_t(row) * fd.Dg);
-    const float rs = row_scale[row];  // x = rs * p; G = rs * (g - x (x.g))
-    const uint32_t pm = fd.G > 1 ? present[ci] : 0xFFFFFFFFu;  // species with neighbours (the groups)
-    auto live = [&](uint32_t e) {
-      return e != kNoChunk && ((pm >> ((e >> 24) & 15u)) & 1u) && ((pm >> (e >> 28)) & 1u);
-    };
-    float dot = 0.f;
-#pragma unroll 4
-    for (int c = threadIdx.x; c < nq; c += blockDim.x) {
-      const uint32_t e = smap[c];
-      if (e == kNoChunk) continue;
-      if (!live(e)) {
-        T4[e & 0xFFFFFFu] = make_float4(0.f, 0.f, 0.f, 0.f);
-        continue;
-      }
-      const float4 gq = __ldcs(g4 + c);
-      T4[e & 0xFFFFFFu] = gq;
-      if (a.normalize) {
-        const uint2 hv = xh[c], lv = xl[c];
-        const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
-        const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
-        dot += (__bfloat162float(hb[0]) + __bfloat162float(lb[0])) * gq.x;
-        dot += (__bfloat162float(hb[1]) + __bfloat162float(lb[1])) * gq.y;
-        dot += (__bfloat162float(hb[2]) + __bfloat162float(lb[2])) * gq.z;
-        dot += (__bfloat162float(hb[3]) + __bfloat162float(lb[3])) * gq.w;
-      }
-    }
+    cp_async_wait<1>();  // g and this centre's coefficients have landed ...
+    __syncthreads();     // ... for every thread
     if (a.normalize) {
-      dot = block_sum_f(dot, red) * rs;  // x is zero in the chunks left out
-      const float k = rs * dot;
-      // each thread projects the chunks it stored
+      // x.g, then G = rs (g - x (x.g)) in place; x is read twice from L2,
+      // by loads that wait on nothing (a chunk without a slot reads the zero
+      // tile; the slots of absent pairs hold zero)
+      float dot = 0.f;
 #pragma unroll 4
       for (int c = threadIdx.x; c < nq; c += blockDim.x) {
         const uint32_t e = smap[c];
+        const uint2 hv = xh[c], lv = xl[c];
+        const float4 t = T4[e == kNoChunk ? zslot : int(e & 0xFFFFFFu)];
+        const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
+        const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
+        dot = fmaf(__bfloat162float(hb[0]) + __bfloat162float(lb[0]), t.x, dot);
+        dot = fmaf(__bfloat162float(hb[1]) + __bfloat162float(lb[1]), t.y, dot);
+        dot = fmaf(__bfloat162float(hb[2]) + __bfloat162float(lb[2]), t.z, dot);
+        dot = fmaf(__bfloat162float(hb[3]) + __bfloat162float(lb[3]), t.w, dot);
+      }
+      dot = block_sum_f(dot, red) * rs;
+      const float k = rs * dot;
+      // each thread projects the chunks it read
+#pragma unroll 4
+      for (int c = threadIdx.x; c < nq; c += blockDim.x) {
+        const uint32_t e = smap[c];
+        const uint2 hv = __ldcs(xh + c), lv = __ldcs(xl + c);
         if (!live(e)) continue;
         const int d = int(e & 0xFFFFFFu);
-        const uint2 hv = __ldcs(xh + c), lv = __ldcs(xl + c);
         const __nv_bfloat16 * hb = reinterpret_cast<const __nv_bfloat16 *>(&hv);
         const __nv_bfloat16 * lb = reinterpret_cast<const __nv_bfloat16 *>(&lv);
         float4 t = T4[d];
@@ -398,9 +408,9 @@ ps_bwd_f32_kernel(PsArgs a, const float * __restrict__ C, const __nv_bfloat16 * 
         t.w = (t.w - (__bfloat162float(hb[3]) + __bfloat162float(lb[3])) * k) * rs;
         T4[d] = t;
       }
+      __syncthreads();  // G is complete
     }
-    cp_async_wait<1>();  // this centre's coefficients have landed ...
-    __syncthreads();     // ... for every thread, and G is complete
+
     // dE/dc_(i l m) = lf_l sqrt2 (sum_j G(i j) c_(j l m) + (sqrt2 - 1) G(i i) c_(i l m)),
     // over the tiles of row pair ip: (j, ip) for j < ip (transposed), the
     // diagonal tile, then (ip, j) for j > ip
@@ -496,7 +506,7 @@ size_t fwd_smem(const FeatureDims & fd) {
 template <int L>
 size_t bwd_smem(const FeatureDims & fd) {
   const size_t Sn = size_t(fd.Sn), np = (Sn + 1) / 2;
-  return sizeof(float) * (2 * (Sn + (Sn & 1)) * row_stride(L) + 4 * size_t(L + 1) * np * (np + 1) / 2) +
+  return sizeof(float) * (2 * (Sn + (Sn & 1)) * row_stride(L) + 4 * (size_t(L + 1) * np * (np + 1) / 2 + 1)) +
          sizeof(uint32_t) * size_t(fd.Dg / 4);
 }
 
