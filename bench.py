@@ -294,7 +294,7 @@ def fma_peaks(lib):
 # workload: the average of the forward and backward launches of one ncu
 # capture of the 2 000-cluster case (32 505 atoms), scaled by atoms to
 # 160 449 atoms.
-GEMM_TRAFFIC_PER_LAUNCH = 0.5 * (1.210e9 + 2.167e9) * 160449 / 32505
+GEMM_TRAFFIC_PER_LAUNCH = 0.5 * (1.280e9 + 1.925e9) * 160449 / 32505
 
 
 def row_stride(L):
