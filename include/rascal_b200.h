@@ -416,8 +416,7 @@ rgpu_status rgpu_debug_packed_layout(int32_t S, int32_t max_radial, int32_t max_
  * return RGPU_ERR_CAPACITY before any pointer is touched.
  * The first call on each device does the setup (the address lookup of the
  * static arrays, kept for the life of the process; a cudaDeviceReset after
- * it is not supported) and should precede any stream capture. The work is
- * ordered on `stream` (a cudaStream_t or NULL), and the call synchronises
+ * it is not supported). The work is ordered on `stream` (a cudaStream_t or NULL), and the call synchronises
  * that stream before it returns, to read the GEMM's status word. Calls that
  * overlap in time share the scratch and race, so callers serialise them. */
 rgpu_status rgpu_gap_energies_noalloc(int64_t M, int64_t N, int64_t K,

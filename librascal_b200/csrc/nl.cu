@@ -356,46 +356,74 @@ __global__ void nl_gather_kernel(int64_t n_centers, GatherCtx c, int64_t * __res
     }
     base += 1;
   }
-  for (int dx = 0; dx < 3; ++dx) {
-    for (int dy = 0; dy < 3; ++dy) {
-      int64_t lin = (int64_t(b[0] + dx - 1) * g.nboxes[1] + (b[1] + dy - 1)) * g.nboxes[2] + (b[2] - 1);
-      int64_t lo = c.box_ptr[c.box_base[s] + lin];
-      int64_t hi = c.box_ptr[c.box_base[s] + lin + 3];
-      for (int64_t k0 = lo; k0 < hi; k0 += 32) {
-        int64_t k = k0 + lane;
-        bool ok = false;
-        double v[3] = {0., 0., 0.};
-        double d2 = 0.;
-        int64_t sj = -1;
-        if (k < hi) {
-          sj = c.sorted[k];
-          v[0] = c.sorted_x[3 * k + 0] - xi[0];
-          v[1] = c.sorted_x[3 * k + 1] - xi[1];
-          v[2] = c.sorted_x[3 * k + 2] - xi[2];
-          d2 = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
-          ok = (sj != site) && (d2 <= c.rc2);
-        }
-        unsigned m = __ballot_sync(0xffffffffu, ok);
-        if (MODE == 1 && ok && base + out + __popc(m & lanemask_lt()) < c.pair_cap) {
-          int64_t p = base + out + __popc(m & lanemask_lt());
-          pair_j[p] = site_real[sj];
-          pair_shift[3 * p + 0] = site_shift[3 * sj + 0];
-          pair_shift[3 * p + 1] = site_shift[3 * sj + 1];
-          pair_shift[3 * p + 2] = site_shift[3 * sj + 2];
-          double dist = sqrt(d2);
-          pair_dist[p] = dist;
-          if (d2 > 0.) {
-            pair_dir[3 * p + 0] = v[0] / dist;
-            pair_dir[3 * p + 1] = v[1] / dist;
-            pair_dir[3 * p + 2] = v[2] / dist;
-          } else {
-            pair_dir[3 * p + 0] = v[0];
-            pair_dir[3 * p + 1] = v[1];
-            pair_dir[3 * p + 2] = v[2];
-          }
-        }
-        out += __popc(m);
+  // The stencil's 9 box rows (dx, dy; 3 boxes along z each) are runs of the
+  // box-sorted sites; lanes 0..8 read one run's bounds each, all at once.
+  int64_t run_lo = 0, run_len = 0;
+  if (lane < 9) {
+    const int dx = lane / 3, dy = lane - 3 * (lane / 3);
+    const int64_t lin = (int64_t(b[0] + dx - 1) * g.nboxes[1] + (b[1] + dy - 1)) * g.nboxes[2] + (b[2] - 1);
+    run_lo = c.box_ptr[c.box_base[s] + lin];
+    run_len = c.box_ptr[c.box_base[s] + lin + 3] - run_lo;
+  }
+  // candidate k (valid: has one) of this lane: its pair, if within the
+  // cutoff, takes the next slot in lane order
+  auto visit = [&](bool valid, int64_t k) {
+    bool ok = false;
+    double v[3] = {0., 0., 0.};
+    double d2 = 0.;
+    int64_t sj = -1;
+    if (valid) {
+      sj = c.sorted[k];
+      v[0] = c.sorted_x[3 * k + 0] - xi[0];
+      v[1] = c.sorted_x[3 * k + 1] - xi[1];
+      v[2] = c.sorted_x[3 * k + 2] - xi[2];
+      d2 = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2];
+      ok = (sj != site) && (d2 <= c.rc2);
+    }
+    unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (MODE == 1 && ok && base + out + __popc(m & lanemask_lt()) < c.pair_cap) {
+      int64_t p = base + out + __popc(m & lanemask_lt());
+      pair_j[p] = site_real[sj];
+      pair_shift[3 * p + 0] = site_shift[3 * sj + 0];
+      pair_shift[3 * p + 1] = site_shift[3 * sj + 1];
+      pair_shift[3 * p + 2] = site_shift[3 * sj + 2];
+      double dist = sqrt(d2);
+      pair_dist[p] = dist;
+      if (d2 > 0.) {
+        pair_dir[3 * p + 0] = v[0] / dist;
+        pair_dir[3 * p + 1] = v[1] / dist;
+        pair_dir[3 * p + 2] = v[2] / dist;
+      } else {
+        pair_dir[3 * p + 0] = v[0];
+        pair_dir[3 * p + 1] = v[1];
+        pair_dir[3 * p + 2] = v[2];
       }
+    }
+    out += __popc(m);
+  };
+  int64_t run_end = run_len;  // inclusive scan of the run lengths over lanes 0..8
+#pragma unroll
+  for (int off = 1; off < 16; off <<= 1) {
+    const int64_t t = __shfl_up_sync(0xffffffffu, run_end, off);
+    if (lane >= off) run_end += t;
+  }
+  const int64_t total = __shfl_sync(0xffffffffu, run_end, 8);
+  if (total <= 32) {
+    // one step over the 9 runs concatenated (same order as row by row), so
+    // that no candidate load waits on another row's
+    const int64_t run_start = run_end - run_len;
+    int64_t k = 0;  // this lane's candidate in the sorted sites
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+      const int64_t st = __shfl_sync(0xffffffffu, run_start, r), en = __shfl_sync(0xffffffffu, run_end, r),
+                    lo = __shfl_sync(0xffffffffu, run_lo, r);
+      if (lane >= st && lane < en) k = lo + (lane - st);
+    }
+    visit(lane < total, k);
+  } else {
+    for (int r = 0; r < 9; ++r) {  // row by row, 32 candidates per step
+      const int64_t lo = __shfl_sync(0xffffffffu, run_lo, r), hi = lo + __shfl_sync(0xffffffffu, run_len, r);
+      for (int64_t k0 = lo; k0 < hi; k0 += 32) visit(k0 + lane < hi, k0 + lane);
     }
   }
   if (MODE == 0 && lane == 0) count[ci] = out + 1;

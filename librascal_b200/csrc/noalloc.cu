@@ -5,15 +5,17 @@
 // epilogue (gemm_tc.cu) in its energies-only form. Every scratch buffer (the
 // BF16 hi/lo splits of A and B and the per-tile energy partials) is carved
 // out of one file-scope device array, and the bounded-wait status word is a
-// second one, so a call never allocates device memory.
+// second one, so a call never allocates device memory. It is for callers
+// that must not allocate or free device memory inside a call, such as an MD
+// engine's force callback running beside the engine's own kernels:
+// cudaMalloc and cudaFree synchronise the whole device and would stall them.
 //
 // Setup: the first call on a device (with that device current) looks the
 // two arrays up with cudaGetSymbolAddress and keeps their addresses for the
-// life of the process; it should come before any stream capture. A
-// cudaDeviceReset after that first call is not supported: the kept
-// addresses would belong to the destroyed context. Concurrency: all calls
-// share the one array, so calls that overlap in time (from several host
-// threads or streams) race; callers serialise them.
+// life of the process. A cudaDeviceReset after that first call is not
+// supported: the kept addresses would belong to the destroyed context.
+// Concurrency: all calls share the one array, so calls that overlap in time
+// (from several host threads or streams) race; callers serialise them.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
